@@ -1,0 +1,385 @@
+// capi.cu -- C ABI: context, per-view PatchMatch call, NCC queries.
+//
+// dpe_pm_run replaces DPE::CudaSpaceInitialization + SetDataPassHelperInCuda + RunPatchMatch
+// (DPE.cpp:1071-1252, DPE.cu:3130-3262).  The context owns a grow-only device arena (replacing
+// the process-wide GpuWorkspace, DPE.cpp:775-837), one stream and timing events.
+#include <cub/cub.cuh>
+
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "ctx.h"
+#include "pm_kernels.cuh"
+
+using namespace dpe;
+
+// ------------------------------------------------------------------ host helpers
+namespace {
+
+// Relative pose of source s with respect to the reference, with the float operation order of
+// ComputeHomography (DPE.cu:459-485).
+void relative_pose(const dpe_camera &rc, const dpe_camera &sc, float Rrel[9], float trel[3]) {
+  float rC[3], sC[3], Cr[3];
+  for (int k = 0; k < 3; ++k) {
+    rC[k] = -(rc.R[k] * rc.t[0] + rc.R[3 + k] * rc.t[1] + rc.R[6 + k] * rc.t[2]);
+    sC[k] = -(sc.R[k] * sc.t[0] + sc.R[3 + k] * sc.t[1] + sc.R[6 + k] * sc.t[2]);
+  }
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b)
+      Rrel[3 * a + b] = sc.R[3 * a] * rc.R[3 * b] + sc.R[3 * a + 1] * rc.R[3 * b + 1] + sc.R[3 * a + 2] * rc.R[3 * b + 2];
+  for (int k = 0; k < 3; ++k) Cr[k] = rC[k] - sC[k];
+  for (int a = 0; a < 3; ++a) trel[a] = sc.R[3 * a] * Cr[0] + sc.R[3 * a + 1] * Cr[1] + sc.R[3 * a + 2] * Cr[2];
+}
+
+int check_problem(const dpe_problem *p) {
+  if (!p) return DPE_ERR_INVALID_ARGUMENT;
+  if (p->width < 16 || p->height < 16 || p->width > 32767 || p->height > 32767) return DPE_ERR_INVALID_ARGUMENT;
+  if (p->num_images < 2 || p->num_images > DPE_MAX_IMAGES) return DPE_ERR_INVALID_ARGUMENT;
+  if (p->memory != DPE_MEM_HOST && p->memory != DPE_MEM_DEVICE) return DPE_ERR_INVALID_ARGUMENT;
+  for (int i = 0; i < p->num_images; ++i) {
+    if (!p->images[i]) return DPE_ERR_INVALID_ARGUMENT;
+    if (p->params.geom_consistency && !p->depths[i]) return DPE_ERR_INVALID_ARGUMENT;
+  }
+  const dpe_params &P = p->params;
+  if (P.state < DPE_FIRST_INIT || P.state > DPE_REFINE_ITER) return DPE_ERR_INVALID_ARGUMENT;
+  if (P.state != DPE_FIRST_INIT && !p->plane_in) return DPE_ERR_INVALID_ARGUMENT;
+  if (P.use_APD && !p->weak_in) return DPE_ERR_INVALID_ARGUMENT;
+  if ((P.use_edge || P.use_limit) && (!p->edge || !p->edge_low_res || p->low_width <= 0 || p->low_height <= 0))
+    return DPE_ERR_INVALID_ARGUMENT;
+  if (P.use_label && !p->label) return DPE_ERR_INVALID_ARGUMENT;
+  if (P.strong_radius < 0 || P.strong_increment <= 0 || P.weak_increment <= 0 || P.weak_radius < 0)
+    return DPE_ERR_INVALID_ARGUMENT;
+  if ((2 * P.strong_radius) / P.strong_increment + 1 > kMaxWin) return DPE_ERR_INVALID_ARGUMENT;
+  if (P.rotate_time < 1 || P.rotate_time > 4 || P.top_k < 0 || P.max_iterations < 0) return DPE_ERR_INVALID_ARGUMENT;
+  return DPE_OK;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ context
+extern "C" const char *dpe_status_string(int s) {
+  switch (s) {
+    case DPE_OK: return "ok";
+    case DPE_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case DPE_ERR_CUDA: return "CUDA runtime error";
+    case DPE_ERR_OUT_OF_MEMORY: return "device out of memory";
+    case DPE_ERR_CAPACITY: return "output capacity too small";
+    case DPE_ERR_NO_DEVICE: return "no usable CUDA device";
+    case DPE_ERR_DEVICE_TIMEOUT: return "device-side wait timed out";
+    default: return "unknown status";
+  }
+}
+
+extern "C" void dpe_params_default(dpe_params *p) {
+  if (!p) return;
+  std::memset(p, 0, sizeof(*p));
+  p->max_iterations = 3;
+  p->num_images = 5;
+  p->sigma_spatial = 5.0f;
+  p->sigma_color = 3.0f;
+  p->top_k = 4;
+  p->depth_min = 0.0f;
+  p->depth_max = 1.0f;
+  p->geom_consistency = 0;
+  p->strong_radius = 5;
+  p->strong_increment = 2;
+  p->weak_radius = 5;
+  p->weak_increment = 5;
+  p->use_APD = 1;
+  p->use_edge = 1;
+  p->use_limit = 1;
+  p->use_label = 1;
+  p->use_radius = 1;
+  p->high_res_img = 1;
+  p->max_scale_size = 1;
+  p->scale_size = 1;
+  p->weak_peak_radius = 2;
+  p->rotate_time = 4;
+  p->ransac_threshold = 0.005f;
+  p->geom_factor = 0.2f;
+  p->state = DPE_FIRST_INIT;
+}
+
+extern "C" int dpe_ctx_create(int device, const dpe_limits *limits, dpe_ctx **out) {
+  if (!out) return DPE_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) {
+    cudaGetLastError();
+    return DPE_ERR_NO_DEVICE;
+  }
+  dpe_ctx *c = new dpe_ctx();
+  c->device = device;
+  if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess) {
+    cudaGetLastError();
+    delete c;
+    return DPE_ERR_CUDA;
+  }
+  (void)limits;
+  *out = c;
+  return DPE_OK;
+}
+
+extern "C" int dpe_ctx_destroy(dpe_ctx *c) {
+  if (!c) return DPE_OK;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  c->arena.release();
+  cudaEventDestroy(c->ev0);
+  cudaEventDestroy(c->ev1);
+  cudaStreamDestroy(c->stream);
+  delete c;
+  return DPE_OK;
+}
+
+// ------------------------------------------------------------------ dpe_pm_run
+namespace {
+
+dim3 full_grid(int W, int H) { return dim3((W + 15) / 16, (H + 7) / 8); }
+const dim3 kFullBlock(16, 8);
+dim3 half_grid(int W, int H) { return dim3((W + 31) / 32, ((H + 1) / 2 + 3) / 4); }
+const dim3 kHalfBlock(32, 4);
+
+}  // namespace
+
+extern "C" int dpe_pm_run(dpe_ctx *ctx, const dpe_problem *p, dpe_pm_out *out) {
+  if (!ctx || !out) return DPE_ERR_INVALID_ARGUMENT;
+  int st = check_problem(p);
+  if (st) return st;
+  if (!out->plane || !out->weak || !out->selected_views) return DPE_ERR_INVALID_ARGUMENT;
+  DPE_TRY(cudaSetDevice(ctx->device));
+  cudaStream_t s = ctx->stream;
+  const int W = p->width, H = p->height, N = p->num_images;
+  const size_t L = (size_t)W * H;
+  const size_t PL = (size_t)(W + 2) * (H + 2);
+  const bool host = p->memory == DPE_MEM_HOST;
+  const cudaMemcpyKind h2d = host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+  Arena &A = ctx->arena;
+
+  PMArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.W = W; a.H = H; a.N = N; a.pad_w = W + 2;
+  a.P = p->params;
+  a.P.num_images = N;
+  for (int i = 0; i < N; ++i) a.cam[i] = p->cameras[i];
+  for (int i = 1; i < N; ++i) relative_pose(a.cam[0], a.cam[i], a.Rrel[i], a.trel[i]);
+  a.key[0] = (uint32_t)p->seed;
+  a.key[1] = (uint32_t)(p->seed >> 32);
+
+  // ---- device buffers
+  float *img_pad = A.get<float>("img_pad", PL * N);
+  float *stage = A.get<float>("img_stage", L * N);
+  a.plane = A.get<float4>("plane", L);
+  a.plane_snap = A.get<float4>("plane_snap", L);
+  a.fit_plane = A.get<float4>("fit_plane", L);
+  a.cost = A.get<float>("cost", L);
+  a.cost_snap = A.get<float>("cost_snap", L);
+  a.complexity = A.get<float>("complexity", L);
+  a.views = A.get<uint32_t>("views", L);
+  a.rng_ctr = A.get<uint32_t>("rng_ctr", L);
+  a.vweight = A.get<uint4>("vweight", L);
+  a.weak = A.get<uint8_t>("weak", L);
+  a.reliable = A.get<uint8_t>("reliable", L);
+  a.nmap = A.get<int32_t>("nmap", L);
+  a.radius = A.get<int32_t>("radius", L);
+  int *weak_flag = A.get<int32_t>("weak_flag", L);
+  a.neigh = A.get<short2>("neigh", L * kNeighbours);
+  a.lab_bound = A.get<short2>("lab_bound", L * 8);
+  a.edge_neigh = A.get<short2>("edge_neigh", L * 8);
+  a.nearest = A.get<short2>("nearest", L);
+  if (!A.ok()) return DPE_ERR_OUT_OF_MEMORY;
+
+  const float4 *plane_in = nullptr;
+  const uint32_t *views_in = nullptr;
+  const uint8_t *weak_in = nullptr;
+  if (host) {
+    if (a.P.state != DPE_FIRST_INIT) {
+      float4 *d = A.get<float4>("plane_in", L);
+      if (!d) return DPE_ERR_OUT_OF_MEMORY;
+      DPE_TRY(cudaMemcpyAsync(d, p->plane_in, L * sizeof(float4), h2d, s));
+      plane_in = d;
+      if (p->selected_views_in) {
+        uint32_t *dv = A.get<uint32_t>("views_in", L);
+        if (!dv) return DPE_ERR_OUT_OF_MEMORY;
+        DPE_TRY(cudaMemcpyAsync(dv, p->selected_views_in, L * 4, h2d, s));
+        views_in = dv;
+      }
+    }
+    if (a.P.use_APD) {
+      uint8_t *dw = A.get<uint8_t>("weak_in", L);
+      if (!dw) return DPE_ERR_OUT_OF_MEMORY;
+      DPE_TRY(cudaMemcpyAsync(dw, p->weak_in, L, h2d, s));
+      weak_in = dw;
+    }
+  } else {
+    plane_in = reinterpret_cast<const float4 *>(p->plane_in);
+    views_in = p->selected_views_in;
+    weak_in = p->weak_in;
+  }
+  if (a.P.use_edge || a.P.use_limit) {
+    const size_t LL = (size_t)p->low_width * p->low_height;
+    a.lowW = p->low_width; a.lowH = p->low_height;
+    if (host) {
+      uint8_t *de = A.get<uint8_t>("edge", L), *dl = A.get<uint8_t>("edge_low", LL);
+      if (!de || !dl) return DPE_ERR_OUT_OF_MEMORY;
+      DPE_TRY(cudaMemcpyAsync(de, p->edge, L, h2d, s));
+      DPE_TRY(cudaMemcpyAsync(dl, p->edge_low_res, LL, h2d, s));
+      a.edge = de; a.edge_low = dl;
+    } else {
+      a.edge = p->edge; a.edge_low = p->edge_low_res;
+    }
+  }
+  if (a.P.use_label) {
+    if (host) {
+      int32_t *dl = A.get<int32_t>("label", L);
+      if (!dl) return DPE_ERR_OUT_OF_MEMORY;
+      DPE_TRY(cudaMemcpyAsync(dl, p->label, L * 4, h2d, s));
+      a.label = dl;
+    } else {
+      a.label = p->label;
+    }
+  }
+  if (a.P.geom_consistency) {
+    float *dd = host ? A.get<float>("depths", L * N) : nullptr;
+    if (host && !dd) return DPE_ERR_OUT_OF_MEMORY;
+    for (int i = 0; i < N; ++i) {
+      if (host) {
+        DPE_TRY(cudaMemcpyAsync(dd + L * i, p->depths[i], L * 4, h2d, s));
+        a.dep[i] = dd + L * i;
+      } else {
+        a.dep[i] = p->depths[i];
+      }
+    }
+  }
+  for (int i = 0; i < N; ++i) {
+    const float *src = p->images[i];
+    if (host) {
+      DPE_TRY(cudaMemcpyAsync(stage + L * i, p->images[i], L * 4, h2d, s));
+      src = stage + L * i;
+    }
+    a.img[i] = img_pad + PL * i;
+    k_pad_image<<<dim3((W + 2 + 31) / 32, (H + 2 + 7) / 8), dim3(32, 8), 0, s>>>(src, img_pad + PL * i, W, H);
+  }
+  unsigned long long *counters = A.get<unsigned long long>("counters", 2);
+  if (!counters) return DPE_ERR_OUT_OF_MEMORY;
+  a.counters = ctx->count_evals ? counters : nullptr;
+  if (ctx->count_evals) DPE_TRY(cudaMemsetAsync(counters, 0, 16, s));
+
+  // ---- kernel sequence (DPE.cu:3157-3234)
+  DPE_TRY(cudaEventRecord(ctx->ev0, s));
+  const dim3 fg = full_grid(W, H), hg = half_grid(W, H);
+  k_init_state<<<fg, kFullBlock, 0, s>>>(a, plane_in, views_in, weak_in, weak_flag);
+  if (a.P.use_APD) {
+    size_t tmp_bytes = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, weak_flag, a.nmap, (int)L, s);
+    void *tmp = A.get<uint8_t>("scan_tmp", tmp_bytes + 16);
+    if (!tmp) return DPE_ERR_OUT_OF_MEMORY;
+    DPE_TRY(cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, weak_flag, a.nmap, (int)L, s));
+  } else {
+    DPE_TRY(cudaMemsetAsync(a.nmap, 0, L * 4, s));
+  }
+  k_gen_edge_inform<<<fg, kFullBlock, 0, s>>>(a);
+  k_find_nearest_strong<<<fg, kFullBlock, 0, s>>>(a);
+  k_gen_neighbours<<<fg, kFullBlock, 0, s>>>(a);
+  k_neighbour_update<<<fg, kFullBlock, 0, s>>>(a);
+  k_random_init<<<fg, kFullBlock, 0, s>>>(a);
+  for (int it = 0; it < a.P.max_iterations; ++it) {
+    for (int parity = 0; parity < 2; ++parity) {
+      if (a.P.use_edge) {
+        DPE_TRY(cudaMemcpyAsync(a.plane_snap, a.plane, L * sizeof(float4), cudaMemcpyDeviceToDevice, s));
+        DPE_TRY(cudaMemcpyAsync(a.cost_snap, a.cost, L * 4, cudaMemcpyDeviceToDevice, s));
+      }
+      k_strong_update<<<hg, kHalfBlock, 0, s>>>(a, it, parity);
+    }
+    k_ransac_fit_plane<<<fg, kFullBlock, 0, s>>>(a);
+    if (a.P.use_APD)
+      for (int parity = 0; parity < 2; ++parity) k_weak_update<<<hg, kHalfBlock, 0, s>>>(a, it, parity);
+  }
+  k_get_depth_normal<<<fg, kFullBlock, 0, s>>>(a);
+  for (int parity = 0; parity < 2; ++parity) k_filter_strong<<<hg, kHalfBlock, 0, s>>>(a, parity);
+  k_depth_to_weak<<<fg, kFullBlock, 0, s>>>(a, a.weak);
+  k_local_refine<<<fg, kFullBlock, 0, s>>>(a);
+  DPE_TRY(cudaGetLastError());
+  DPE_TRY(cudaEventRecord(ctx->ev1, s));
+
+  // ---- outputs (DPE.cu:3258-3260)
+  const cudaMemcpyKind d2o = host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+  DPE_TRY(cudaMemcpyAsync(out->plane, a.plane, L * sizeof(float4), d2o, s));
+  DPE_TRY(cudaMemcpyAsync(out->weak, a.weak, L, d2o, s));
+  DPE_TRY(cudaMemcpyAsync(out->selected_views, a.views, L * 4, d2o, s));
+  if (out->costs) DPE_TRY(cudaMemcpyAsync(out->costs, a.cost, L * 4, d2o, s));
+  unsigned long long cnt[2] = {0, 0};
+  if (ctx->count_evals) DPE_TRY(cudaMemcpyAsync(cnt, counters, 16, cudaMemcpyDeviceToHost, s));
+  DPE_TRY(cudaStreamSynchronize(s));
+  float ms = 0.f;
+  DPE_TRY(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+  out->gpu_ms = ms;
+  out->strong_ncc_evals = cnt[0];
+  out->weak_ncc_evals = cnt[1];
+  return DPE_OK;
+}
+
+// ------------------------------------------------------------------ dpe_ncc_eval
+namespace {
+__global__ void k_ncc_queries(const __grid_constant__ PMArgs a, int64_t n, const int32_t *px, const int32_t *py,
+                              const int32_t *src, const float4 *pl, float *out) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  RefWindow rw;
+  build_ref_window(a, px[k], py[k], rw);
+  out[k] = ncc_strong(a, px[k], py[k], src[k], pl[k], rw);
+}
+}  // namespace
+
+extern "C" int dpe_ncc_eval(dpe_ctx *ctx, const dpe_ncc_query *q, float *costs_out) {
+  if (!ctx || !q || !costs_out || q->count < 0) return DPE_ERR_INVALID_ARGUMENT;
+  if (q->num_images < 2 || q->num_images > DPE_MAX_IMAGES || q->width < 16 || q->height < 16) return DPE_ERR_INVALID_ARGUMENT;
+  if ((2 * q->params.strong_radius) / q->params.strong_increment + 1 > kMaxWin) return DPE_ERR_INVALID_ARGUMENT;
+  const int W = q->width, H = q->height, N = q->num_images;
+  for (int64_t k = 0; k < q->count; ++k)
+    if (q->src[k] < 1 || q->src[k] >= N || q->px[k] < 0 || q->px[k] >= W || q->py[k] < 0 || q->py[k] >= H)
+      return DPE_ERR_INVALID_ARGUMENT;
+  if (q->count == 0) return DPE_OK;
+  DPE_TRY(cudaSetDevice(ctx->device));
+  cudaStream_t s = ctx->stream;
+  const size_t L = (size_t)W * H, PL = (size_t)(W + 2) * (H + 2);
+  Arena &A = ctx->arena;
+  PMArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.W = W; a.H = H; a.N = N; a.pad_w = W + 2;
+  a.P = q->params;
+  a.P.num_images = N;
+  for (int i = 0; i < N; ++i) a.cam[i] = q->cameras[i];
+  for (int i = 1; i < N; ++i) relative_pose(a.cam[0], a.cam[i], a.Rrel[i], a.trel[i]);
+  float *img_pad = A.get<float>("img_pad", PL * N);
+  float *stage = A.get<float>("img_stage", L * N);
+  const int64_t n = q->count;
+  int32_t *dpx = A.get<int32_t>("q_px", n), *dpy = A.get<int32_t>("q_py", n), *dsrc = A.get<int32_t>("q_src", n);
+  float4 *dpl = A.get<float4>("q_plane", n);
+  float *dout = A.get<float>("q_out", n);
+  if (!A.ok()) return DPE_ERR_OUT_OF_MEMORY;
+  for (int i = 0; i < N; ++i) {
+    DPE_TRY(cudaMemcpyAsync(stage + L * i, q->images[i], L * 4, cudaMemcpyHostToDevice, s));
+    a.img[i] = img_pad + PL * i;
+    k_pad_image<<<dim3((W + 2 + 31) / 32, (H + 2 + 7) / 8), dim3(32, 8), 0, s>>>(stage + L * i, img_pad + PL * i, W, H);
+  }
+  DPE_TRY(cudaMemcpyAsync(dpx, q->px, n * 4, cudaMemcpyHostToDevice, s));
+  DPE_TRY(cudaMemcpyAsync(dpy, q->py, n * 4, cudaMemcpyHostToDevice, s));
+  DPE_TRY(cudaMemcpyAsync(dsrc, q->src, n * 4, cudaMemcpyHostToDevice, s));
+  DPE_TRY(cudaMemcpyAsync(dpl, q->plane, n * 16, cudaMemcpyHostToDevice, s));
+  k_ncc_queries<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(a, n, dpx, dpy, dsrc, dpl, dout);
+  DPE_TRY(cudaGetLastError());
+  DPE_TRY(cudaMemcpyAsync(costs_out, dout, n * 4, cudaMemcpyDeviceToHost, s));
+  DPE_TRY(cudaStreamSynchronize(s));
+  return DPE_OK;
+}
+
+// Statistics switch: count NCC evaluations in dpe_pm_run (adds device atomics; off by default).
+extern "C" int dpe_ctx_set_eval_counting(dpe_ctx *ctx, int on) {
+  if (!ctx) return DPE_ERR_INVALID_ARGUMENT;
+  ctx->count_evals = on != 0;
+  return DPE_OK;
+}

@@ -1,0 +1,72 @@
+// ctx.h -- the dpe_ctx object behind the C ABI: device, stream, events and a device arena.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <map>
+#include <string>
+
+#include "../../include/dpe_b200.h"
+
+// Return DPE_ERR_CUDA (or DPE_ERR_OUT_OF_MEMORY) from the enclosing ABI function when a CUDA call
+// fails; the reference exits the process instead (CudaSafeCall, DPE.cpp:646-679).
+#define DPE_TRY(call)                                                              \
+  do {                                                                             \
+    cudaError_t dpe_err_ = (call);                                                 \
+    if (dpe_err_ != cudaSuccess) {                                                 \
+      cudaGetLastError();                                                          \
+      return dpe_err_ == cudaErrorMemoryAllocation ? DPE_ERR_OUT_OF_MEMORY : DPE_ERR_CUDA; \
+    }                                                                              \
+  } while (0)
+
+// Named grow-only device buffers, reused across calls (the reference's GpuWorkspace pools
+// best-fit blocks per call; here each role keeps one buffer that only grows).
+class Arena {
+ public:
+  template <class T> T *get(const char *name, size_t count) {
+    const size_t bytes = count * sizeof(T) + 256;
+    Slot &s = slots_[name];
+    if (s.bytes < bytes) {
+      if (s.ptr) cudaFree(s.ptr);
+      s.ptr = nullptr;
+      s.bytes = 0;
+      if (cudaMalloc(&s.ptr, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        s.ptr = nullptr;
+        failed_ = true;
+        return nullptr;
+      }
+      s.bytes = bytes;
+      reserved_ += bytes;
+    }
+    return static_cast<T *>(s.ptr);
+  }
+  bool ok() {
+    const bool r = !failed_;
+    failed_ = false;
+    return r;
+  }
+  void release() {
+    for (auto &kv : slots_)
+      if (kv.second.ptr) cudaFree(kv.second.ptr);
+    slots_.clear();
+  }
+  size_t reserved() const { return reserved_; }
+
+ private:
+  struct Slot {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+  };
+  std::map<std::string, Slot> slots_;
+  bool failed_ = false;
+  size_t reserved_ = 0;
+};
+
+struct dpe_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  bool count_evals = false;
+  Arena arena;
+};

@@ -1,0 +1,423 @@
+// dpe_device.cuh -- device-side building blocks of the sm_100a PatchMatch kernels.
+//
+// Geometry and cost functions restate the reference's device helpers (DPE.cu:9-957) in FP32
+// without fast-math; the per-pixel reference window of the strong NCC is hoisted out of the
+// hypothesis loop (weights and reference moments do not depend on the plane).
+#pragma once
+
+#include <cfloat>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/dpe_b200.h"
+
+namespace dpe {
+
+constexpr int kMaxImages = DPE_MAX_IMAGES;
+constexpr int kMaxSrc = DPE_MAX_IMAGES - 1;
+constexpr int kNeighbours = DPE_NEIGHBOUR_NUM;
+constexpr int kMaxWin = 6;  // taps per window side for radius 5 / step 2 (DPE.cu:728-737)
+
+// All per-call read-only data, passed by value as a __grid_constant__ kernel parameter.
+struct PMArgs {
+  int W, H, N, lowW, lowH, pad_w;  // pad_w = W + 2 (images carry a 1-texel clamp border)
+  dpe_params P;
+  dpe_camera cam[kMaxImages];
+  float Rrel[kMaxImages][9];  // source rotation relative to the reference (DPE.cu:471-479)
+  float trel[kMaxImages][3];  // source translation relative to the reference (DPE.cu:480-485)
+  uint32_t key[2];
+  const float *img[kMaxImages];  // padded (W+2)*(H+2) float images
+  const float *dep[kMaxImages];  // W*H depth maps (geom consistency)
+  // state
+  float4 *plane;
+  float4 *plane_snap;
+  float4 *fit_plane;
+  float *cost;
+  float *cost_snap;
+  float *complexity;
+  uint32_t *views;
+  uint32_t *rng_ctr;
+  uint4 *vweight;          // 32 4-bit sample counts per pixel
+  uint8_t *weak;
+  uint8_t *reliable;
+  const uint8_t *edge;
+  const uint8_t *edge_low;
+  const int32_t *label;
+  int32_t *nmap;
+  int32_t *radius;
+  short2 *neigh;
+  short2 *lab_bound;
+  short2 *edge_neigh;
+  short2 *nearest;
+  unsigned long long *counters;  // [0] strong NCC evals, [1] weak NCC evals (stats builds)
+};
+
+// ------------------------------------------------------------------ OpenCV MIN/MAX semantics
+template <class A, class B> __device__ __forceinline__ auto cvmin(A a, B b) -> decltype(a + b) { return a > b ? b : a; }
+template <class A, class B> __device__ __forceinline__ auto cvmax(A a, B b) -> decltype(a + b) { return a < b ? b : a; }
+
+__device__ __forceinline__ int isSet(uint32_t v, int n) { return (v >> n) & 1; }
+__device__ __forceinline__ void setBit(uint32_t *v, int n) { *v |= (1u << n); }
+__device__ __forceinline__ void unSetBit(uint32_t *v, int n) { *v &= (0xFFFFFFFEu << n); }
+
+// ------------------------------------------------------------------ Philox4x32-10
+// Salmon et al., SC'11.  Draw n of pixel p is word 0 of philox({n, p, 0x5EED, 0}, key).
+__device__ __forceinline__ uint32_t philox_word0(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0,
+                                                 uint32_t k1) {
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    if (r > 0) { k0 += 0x9E3779B9u; k1 += 0xBB67AE85u; }
+    const uint32_t lo0 = 0xD2511F53u * c0, hi0 = __umulhi(0xD2511F53u, c0);
+    const uint32_t lo1 = 0xCD9E8D57u * c2, hi1 = __umulhi(0xCD9E8D57u, c2);
+    const uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
+    c0 = n0; c1 = lo1; c2 = n2; c3 = lo0;
+  }
+  return c0;
+}
+__device__ __forceinline__ void philox4(const uint32_t ci[4], const uint32_t ki[2], uint32_t out[4]) {
+  uint32_t c0 = ci[0], c1 = ci[1], c2 = ci[2], c3 = ci[3], k0 = ki[0], k1 = ki[1];
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    if (r > 0) { k0 += 0x9E3779B9u; k1 += 0xBB67AE85u; }
+    const uint32_t lo0 = 0xD2511F53u * c0, hi0 = __umulhi(0xD2511F53u, c0);
+    const uint32_t lo1 = 0xCD9E8D57u * c2, hi1 = __umulhi(0xCD9E8D57u, c2);
+    const uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
+    c0 = n0; c1 = lo1; c2 = n2; c3 = lo0;
+  }
+  out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+
+// Per-pixel random stream; the counter lives in a register and is written back by the owner.
+struct Rng {
+  uint32_t k0, k1, pixel, ctr;
+  __device__ __forceinline__ uint32_t u32() { return philox_word0(ctr++, pixel, 0x5EEDu, 0u, k0, k1); }
+  __device__ __forceinline__ float uniform() { return (float)((u32() >> 8) + 1u) * (1.0f / 16777216.0f); }
+};
+__device__ __forceinline__ Rng make_rng(const PMArgs &a, int center) {
+  return Rng{a.key[0], a.key[1], (uint32_t)center, a.rng_ctr[center]};
+}
+
+// ------------------------------------------------------------------ image access
+__device__ __forceinline__ float texel(const PMArgs &a, int im, int x, int y) {
+  x = min(max(x, 0), a.W - 1);
+  y = min(max(y, 0), a.H - 1);
+  return __ldg(a.img[im] + (size_t)(y + 1) * a.pad_w + (x + 1));
+}
+// tex2D(x+0.5, y+0.5) with linear filtering and clamp-to-edge addressing, exact FP32 weights.
+// The padded border makes the four reads branch-free for x0 in [-1, W-1].
+__device__ __forceinline__ float bilinear(const float *__restrict__ img, int pad_w, int W, int H, float x, float y) {
+  const float xc = fminf(fmaxf(x, -1.0f), (float)(W - 1));
+  const float yc = fminf(fmaxf(y, -1.0f), (float)(H - 1));
+  const float fx = floorf(xc), fy = floorf(yc);
+  const float ax = xc - fx, ay = yc - fy;
+  const float *p = img + (size_t)((int)fy + 1) * pad_w + ((int)fx + 1);
+  const float v00 = __ldg(p), v10 = __ldg(p + 1), v01 = __ldg(p + pad_w), v11 = __ldg(p + pad_w + 1);
+  const float top = (1.0f - ax) * v00 + ax * v10;
+  const float bot = (1.0f - ax) * v01 + ax * v11;
+  return (1.0f - ay) * top + ay * bot;
+}
+
+// ------------------------------------------------------------------ geometry (DPE.cu:313-546)
+__device__ __forceinline__ void point3d(const dpe_camera &c, int x, int y, float depth, float X[3]) {
+  X[0] = depth * ((float)x - c.K[2]) / c.K[0];
+  X[1] = depth * ((float)y - c.K[5]) / c.K[4];
+  X[2] = depth;
+}
+__device__ __forceinline__ float4 view_direction(const dpe_camera &c, int x, int y, float depth) {
+  float X[3];
+  point3d(c, x, y, depth, X);
+  const float norm = sqrtf(X[0] * X[0] + X[1] * X[1] + X[2] * X[2]);
+  return make_float4(X[0] / norm, X[1] / norm, X[2] / norm, 0.0f);
+}
+__device__ __forceinline__ float dist_to_origin(const dpe_camera &c, int x, int y, float depth, float4 n) {
+  float X[3];
+  point3d(c, x, y, depth, X);
+  return -(n.x * X[0] + n.y * X[1] + n.z * X[2]);
+}
+__device__ __forceinline__ float depth_from_plane(const dpe_camera &c, float4 pl, int x, int y) {
+  return -pl.w * c.K[0] /
+         (((float)x - c.K[2]) * pl.x + (c.K[0] / c.K[4]) * ((float)y - c.K[5]) * pl.y + c.K[0] * pl.z);
+}
+__device__ __forceinline__ float4 normal_to_world(const dpe_camera &c, float4 p) {
+  return make_float4(c.R[0] * p.x + c.R[3] * p.y + c.R[6] * p.z, c.R[1] * p.x + c.R[4] * p.y + c.R[7] * p.z,
+                     c.R[2] * p.x + c.R[5] * p.y + c.R[8] * p.z, p.w);
+}
+__device__ __forceinline__ float4 normal_to_ref(const dpe_camera &c, float4 p) {
+  return make_float4(c.R[0] * p.x + c.R[1] * p.y + c.R[2] * p.z, c.R[3] * p.x + c.R[4] * p.y + c.R[5] * p.z,
+                     c.R[6] * p.x + c.R[7] * p.y + c.R[8] * p.z, p.w);
+}
+__device__ __forceinline__ void normalize3(float4 *v) {
+  const float inv = 1.0f / sqrtf(v->x * v->x + v->y * v->y + v->z * v->z);
+  v->x *= inv; v->y *= inv; v->z *= inv;
+}
+__device__ __forceinline__ void normalize3(float3 *v) {
+  const float inv = 1.0f / sqrtf(v->x * v->x + v->y * v->y + v->z * v->z);
+  v->x *= inv; v->y *= inv; v->z *= inv;
+}
+__device__ __forceinline__ void normalize2(float2 *v) {
+  const float inv = 1.0f / sqrtf(v->x * v->x + v->y * v->y);
+  v->x *= inv; v->y *= inv;
+}
+
+// Marsaglia sphere point facing the camera (DPE.cu:365-391); rejection capped at 64 tries.
+__device__ __forceinline__ float4 random_normal(const dpe_camera &c, int x, int y, Rng &rng, float depth) {
+  float q1 = 1.0f, q2 = 1.0f, s = 2.0f;
+  for (int tries = 0; s >= 1.0f && tries < 64; ++tries) {
+    q1 = 2.0f * rng.uniform() - 1.0f;
+    q2 = 2.0f * rng.uniform() - 1.0f;
+    s = q1 * q1 + q2 * q2;
+  }
+  const float sq = sqrtf(fmaxf(1.0f - s, 0.0f));
+  float4 n = make_float4(2.0f * q1 * sq, 2.0f * q2 * sq, 1.0f - 2.0f * s, 0.0f);
+  const float4 v = view_direction(c, x, y, depth);
+  if (n.x * v.x + n.y * v.y + n.z * v.z > 0.0f) { n.x = -n.x; n.y = -n.y; n.z = -n.z; }
+  normalize3(&n);
+  return n;
+}
+
+// Euler-angle perturbation (DPE.cu:393-428)
+__device__ __forceinline__ float4 perturbed_normal(const dpe_camera &c, int x, int y, float4 n, Rng &rng, float pert) {
+  const float4 v = view_direction(c, x, y, 1.0f);
+  const float a1 = (rng.uniform() - 0.5f) * pert;
+  const float a2 = (rng.uniform() - 0.5f) * pert;
+  const float a3 = (rng.uniform() - 0.5f) * pert;
+  float s1, s2, s3, c1, c2, c3;
+  sincosf(a1, &s1, &c1);
+  sincosf(a2, &s2, &c2);
+  sincosf(a3, &s3, &c3);
+  const float R0 = c2 * c3, R1 = c3 * s1 * s2 - c1 * s3, R2 = s1 * s3 + c1 * c3 * s2;
+  const float R3 = c2 * s3, R4 = c1 * c3 + s1 * s2 * s3, R5 = c1 * s2 * s3 - c3 * s1;
+  const float R6 = -s2, R7 = c2 * s1, R8 = c1 * c2;
+  float4 r = make_float4(R0 * n.x + R1 * n.y + R2 * n.z, R3 * n.x + R4 * n.y + R5 * n.z, R6 * n.x + R7 * n.y + R8 * n.z, n.w);
+  if (r.x * v.x + r.y * v.y + r.z * v.z >= 0.0f) r = n;
+  normalize3(&r);
+  return r;
+}
+
+// Homography of a reference-camera plane into source `s` (DPE.cu:457-517), using the relative
+// pose precomputed on the host with the reference's float operation order.
+__device__ __forceinline__ void homography(const PMArgs &a, int s, float4 pl, float H[9]) {
+  const dpe_camera &rc = a.cam[0];
+  const dpe_camera &sc = a.cam[s];
+  const float n[3] = {pl.x, pl.y, pl.z};
+  float G[9];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) G[3 * i + j] = a.Rrel[s][3 * i + j] - a.trel[s][i] * n[j] / pl.w;
+  float T[9];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    T[3 * i] = G[3 * i] / rc.K[0];
+    T[3 * i + 1] = G[3 * i + 1] / rc.K[4];
+    T[3 * i + 2] = -G[3 * i] * rc.K[2] / rc.K[0] - G[3 * i + 1] * rc.K[5] / rc.K[4] + G[3 * i + 2];
+  }
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    H[j] = sc.K[0] * T[j] + sc.K[2] * T[6 + j];
+    H[3 + j] = sc.K[4] * T[3 + j] + sc.K[5] * T[6 + j];
+    H[6 + j] = sc.K[8] * T[6 + j];
+  }
+}
+__device__ __forceinline__ float2 project(const float H[9], int x, int y) {
+  const float fx = (float)x, fy = (float)y;
+  const float X = H[0] * fx + H[1] * fy + H[2];
+  const float Y = H[3] * fx + H[4] * fy + H[5];
+  const float Z = H[6] * fx + H[7] * fy + H[8];
+  return make_float2(X / Z, Y / Z);
+}
+
+__device__ __forceinline__ float bilateral_weight(float dx, float dy, float pix, float center, float ss, float sc) {
+  const float spatial = sqrtf(dx * dx + dy * dy);
+  const float color = fabsf(pix - center);
+  return expf(-spatial / (2.0f * ss * ss) - color / (2.0f * sc * sc));
+}
+
+// ------------------------------------------------------------------ strong NCC
+// Hypothesis-invariant part of the strong window of one pixel: per tap the bilateral weight w and
+// w*r, plus the normalised reference moments.
+struct RefWindow {
+  float w[kMaxWin * kMaxWin];
+  float wr[kMaxWin * kMaxWin];
+  float inv_wsum, mean_r, var_r;
+  int taps_side;
+};
+
+__device__ __forceinline__ void build_ref_window(const PMArgs &a, int px, int py, RefWindow &rw) {
+  const int r = a.P.strong_radius, inc = a.P.strong_increment;
+  const float center = texel(a, 0, px, py);
+  float sw = 0.f, swr = 0.f, swrr = 0.f;
+  int k = 0, side = 0;
+  for (int i = -r; i <= r; i += inc, ++side) {
+    for (int j = -r; j <= r; j += inc) {
+      const float rp = texel(a, 0, px + i, py + j);
+      const float w = bilateral_weight((float)i, (float)j, rp, center, a.P.sigma_spatial, a.P.sigma_color);
+      rw.w[k] = w;
+      rw.wr[k] = w * rp;
+      sw += w; swr += w * rp; swrr += w * rp * rp;
+      ++k;
+    }
+  }
+  rw.taps_side = side;
+  rw.inv_wsum = 1.0f / sw;
+  rw.mean_r = swr * rw.inv_wsum;
+  rw.var_r = swrr * rw.inv_wsum - rw.mean_r * rw.mean_r;
+}
+
+// ComputeBilateralNCCOld (DPE.cu:696-782) with the reference window precomputed.
+__device__ __forceinline__ float ncc_strong(const PMArgs &a, int px, int py, int s, float4 pl, const RefWindow &rw) {
+  float H[9];
+  homography(a, s, pl, H);
+  const float2 pt = project(H, px, py);
+  const dpe_camera &sc = a.cam[s];
+  if (pt.x >= sc.width || pt.x < 0.0f || pt.y >= sc.height || pt.y < 0.0f) return 2.0f;
+  if (a.counters) atomicAdd(&a.counters[0], 1ull);
+  const int r = a.P.strong_radius, inc = a.P.strong_increment;
+  const float *__restrict__ img = a.img[s];
+  float s_s = 0.f, s_ss = 0.f, s_rs = 0.f;
+  int k = 0;
+  for (int i = -r; i <= r; i += inc) {
+    const float x = (float)(px + i);
+    // column x is fixed while y walks the window: the projective numerators are affine in y
+    const float bx = H[0] * x + H[2], by = H[3] * x + H[5], bz = H[6] * x + H[8];
+    for (int j = -r; j <= r; j += inc) {
+      const float y = (float)(py + j);
+      const float X = H[1] * y + bx, Y = H[4] * y + by, Z = H[7] * y + bz;
+      const float iz = 1.0f / Z;
+      const float sv = bilinear(img, a.pad_w, a.W, a.H, X * iz, Y * iz);
+      const float ws = rw.w[k] * sv;
+      s_s += ws;
+      s_ss += ws * sv;
+      s_rs += rw.wr[k] * sv;
+      ++k;
+    }
+  }
+  const float m_s = s_s * rw.inv_wsum;
+  const float var_s = s_ss * rw.inv_wsum - m_s * m_s;
+  if (rw.var_r < 1e-5f || var_s < 1e-5f) return 2.0f;
+  const float cov = s_rs * rw.inv_wsum - rw.mean_r * m_s;
+  return fmaxf(0.0f, fminf(2.0f, 1.0f - cov / sqrtf(rw.var_r * var_s)));
+}
+
+// Window NCC with the window built on the fly (deformable weak window, DPE.cu:628-672).
+__device__ __forceinline__ float window_ncc(const PMArgs &a, const float H[9], int s, int cx, int cy, int radius, int inc,
+                                            float ref_center) {
+  const float *__restrict__ img = a.img[s];
+  float s_r = 0, s_rr = 0, s_s = 0, s_ss = 0, s_rs = 0, s_w = 0;
+  for (int i = -radius; i <= radius; i += inc) {
+    float r_r = 0, r_rr = 0, r_s = 0, r_ss = 0, r_rs = 0, r_w = 0;
+    for (int j = -radius; j <= radius; j += inc) {
+      const int rx = cx + i, ry = cy + j;
+      const float rp = texel(a, 0, rx, ry);
+      const float2 sp = project(H, rx, ry);
+      const float sv = bilinear(img, a.pad_w, a.W, a.H, sp.x, sp.y);
+      const float w = bilateral_weight((float)i, (float)j, rp, ref_center, a.P.sigma_spatial, a.P.sigma_color);
+      r_r += w * rp; r_rr += w * rp * rp; r_s += w * sv; r_ss += w * sv * sv; r_rs += w * rp * sv; r_w += w;
+    }
+    s_r += r_r; s_rr += r_rr; s_s += r_s; s_ss += r_ss; s_rs += r_rs; s_w += r_w;
+  }
+  const float inv = 1.0f / s_w;
+  s_r *= inv; s_rr *= inv; s_s *= inv; s_ss *= inv; s_rs *= inv;
+  const float var_r = s_rr - s_r * s_r;
+  const float var_s = s_ss - s_s * s_s;
+  if (var_r < 1e-5f || var_s < 1e-5f) return 2.0f;
+  const float cov = s_rs - s_r * s_s;
+  return fmaxf(0.0f, fminf(2.0f, 1.0f - cov / sqrtf(var_r * var_s)));
+}
+
+__device__ __forceinline__ short2 neighbour(const PMArgs &a, int center, int k) {
+  return a.neigh[(size_t)a.nmap[center] * kNeighbours + k];
+}
+
+// ComputeBilateralNCCNew (DPE.cu:561-694)
+__device__ __forceinline__ float ncc_weak(const PMArgs &a, int px, int py, int s, float4 pl) {
+  float H[9];
+  homography(a, s, pl, H);
+  const float2 pt = project(H, px, py);
+  const dpe_camera &sc = a.cam[s];
+  if (pt.x >= sc.width || pt.x < 0.0f || pt.y >= sc.height || pt.y < 0.0f) return 2.0f;
+  if (a.counters) atomicAdd(&a.counters[1], 1ull);
+  const int center = px + py * a.W;
+  const float ref_center = texel(a, 0, px, py);
+  float center_cost = 0.0f, strong_cost = 0.0f;
+  int strong_count = 0;
+  for (int k = 0; k < kNeighbours; ++k) {
+    const short2 nb = neighbour(a, center, k);
+    if (nb.x == -1 || nb.y == -1) continue;
+    const float2 np = project(H, nb.x, nb.y);
+    if (np.x < 0 || np.y < 0 || np.x >= a.W || np.y >= a.H) {
+      if (k != 0) {
+        const long idx = (long)nb.x + (long)nb.y * a.W;
+        const uint32_t v = (idx >= 0 && idx < (long)a.W * a.H) ? a.views[idx] : 0u;
+        if (isSet(v, s - 1)) { strong_cost += 2.0f; strong_count++; }
+        continue;
+      }
+      return 2.0f;
+    }
+    int radius = k == 0 ? a.P.strong_radius : a.P.weak_radius;
+    int inc = k == 0 ? a.P.strong_increment : a.P.weak_increment;
+    if (a.P.use_radius && k == 0) {
+      radius = a.radius[center];
+      inc = cvmax(2, (int)(2.0 * radius / 5.0));
+    }
+    const float t = window_ncc(a, H, s, nb.x, nb.y, radius, inc, ref_center);
+    if (k == 0) center_cost = t;
+    else { strong_cost += t; strong_count++; }
+  }
+  if (strong_count == 0) return center_cost;
+  strong_cost /= strong_count;
+  strong_cost = cvmin(strong_cost, 2.0f);
+  return (float)(0.25 * center_cost + 0.75 * strong_cost);
+}
+
+// ComputeGeomConsistencyCost (DPE.cu:919-957)
+__device__ __forceinline__ float3 point_world(float x, float y, float depth, const dpe_camera &c) {
+  const float px = depth * (x - c.K[2]) / c.K[0];
+  const float py = depth * (y - c.K[5]) / c.K[4];
+  const float pz = depth;
+  const float tx = c.R[0] * px + c.R[3] * py + c.R[6] * pz;
+  const float ty = c.R[1] * px + c.R[4] * py + c.R[7] * pz;
+  const float tz = c.R[2] * px + c.R[5] * py + c.R[8] * pz;
+  return make_float3(tx + c.c[0], ty + c.c[1], tz + c.c[2]);
+}
+__device__ __forceinline__ void project_camera(float3 X, const dpe_camera &c, float2 &pt, float &depth) {
+  const float tx = c.R[0] * X.x + c.R[1] * X.y + c.R[2] * X.z + c.t[0];
+  const float ty = c.R[3] * X.x + c.R[4] * X.y + c.R[5] * X.z + c.t[1];
+  const float tz = c.R[6] * X.x + c.R[7] * X.y + c.R[8] * X.z + c.t[2];
+  depth = c.K[6] * tx + c.K[7] * ty + c.K[8] * tz;
+  pt.x = (c.K[0] * tx + c.K[1] * ty + c.K[2] * tz) / depth;
+  pt.y = (c.K[3] * tx + c.K[4] * ty + c.K[5] * tz) / depth;
+}
+__device__ __forceinline__ float geom_cost(const PMArgs &a, int px, int py, int s, float4 pl) {
+  const dpe_camera &rc = a.cam[0], &sc = a.cam[s];
+  const float depth = depth_from_plane(rc, pl, px, py);
+  const float3 fw = point_world((float)px, (float)py, depth, rc);
+  float2 sp;
+  float sd;
+  project_camera(fw, sc, sp, sd);
+  int ix = (int)sp.x, iy = (int)sp.y;  // cvt.rzi: truncation, NaN -> 0
+  ix = min(max(ix, 0), a.W - 1);
+  iy = min(max(iy, 0), a.H - 1);
+  const float src_depth = __ldg(a.dep[s] + (size_t)iy * a.W + ix);
+  if (src_depth == 0.0f) return 3.0f;
+  const float3 sw = point_world(sp.x, sp.y, src_depth, sc);
+  float2 bp;
+  float rd;
+  project_camera(sw, rc, bp, rd);
+  const float dx = (float)px - bp.x, dy = (float)py - bp.y;
+  return fminf(3.0f, sqrtf(dx * dx + dy * dy));
+}
+
+// ------------------------------------------------------------------ packed view weights
+__device__ __forceinline__ void store_vweight(uint4 *dst, const uint8_t *vw) {
+  uint32_t w[4] = {0, 0, 0, 0};
+#pragma unroll
+  for (int i = 0; i < 32; ++i) w[i >> 3] |= (uint32_t)(vw[i] & 0xF) << (4 * (i & 7));
+  *dst = make_uint4(w[0], w[1], w[2], w[3]);
+}
+__device__ __forceinline__ int vweight_at(const uint4 &p, int i) {
+  const uint32_t w = (i >> 3) == 0 ? p.x : (i >> 3) == 1 ? p.y : (i >> 3) == 2 ? p.z : p.w;
+  return (w >> (4 * (i & 7))) & 0xF;
+}
+
+}  // namespace dpe

@@ -1,0 +1,1202 @@
+// pm_kernels.cuh -- the per-view PatchMatch kernels (one thread per pixel of a pass).
+//
+// Kernel order and per-pixel semantics follow DPE::RunPatchMatch (DPE.cu:3130-3262).  B200
+// design points: all per-call constants (cameras, relative poses, params, pointers) travel in one
+// __grid_constant__ parameter block; state is structure-of-arrays; view weights are packed as
+// 4-bit counts (16 B per pixel instead of 32); the strong NCC's reference window is built once
+// per thread and reused by every hypothesis and source view; the same-colour race of the
+// edge-aware update is removed by reading candidates from a pre-pass snapshot.
+#pragma once
+
+#include "dpe_device.cuh"
+
+namespace dpe {
+
+__device__ __constant__ const int kDir[8][2] = {{0, -1}, {0, 1}, {-1, 0}, {1, 0}, {-1, -1}, {1, 1}, {-1, 1}, {1, -1}};
+
+// pixel of colour `parity` ((x + y) % 2) handled by this thread of a half-height grid
+__device__ __forceinline__ bool colour_pixel(const PMArgs &a, int parity, int *px, int *py) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int yy = blockIdx.y * blockDim.y + threadIdx.y;
+  const int y = 2 * yy + ((x + parity) & 1);
+  *px = x; *py = y;
+  return x < a.W && y < a.H;
+}
+__device__ __forceinline__ bool full_pixel(const PMArgs &a, int *px, int *py) {
+  *px = blockIdx.x * blockDim.x + threadIdx.x;
+  *py = blockIdx.y * blockDim.y + threadIdx.y;
+  return *px < a.W && *py < a.H;
+}
+
+// ------------------------------------------------------------------ setup
+__global__ void k_pad_image(const float *__restrict__ src, float *__restrict__ dst, int W, int H) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x - 1;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y - 1;
+  if (x > W || y > H) return;
+  const int sx = min(max(x, 0), W - 1), sy = min(max(y, 0), H - 1);
+  dst[(size_t)(y + 1) * (W + 2) + (x + 1)] = src[(size_t)sy * W + sx];
+}
+
+__global__ void k_init_state(const __grid_constant__ PMArgs a, const float4 *plane_in, const uint32_t *views_in,
+                             const uint8_t *weak_in, int *weak_flag) {
+  int px, py;
+  if (!full_pixel(a, &px, &py)) return;
+  const int c = px + py * a.W;
+  a.plane[c] = (a.P.state != DPE_FIRST_INIT && plane_in) ? plane_in[c] : make_float4(0, 0, 0, 0);
+  a.views[c] = (a.P.state != DPE_FIRST_INIT && views_in) ? views_in[c] : 0u;
+  const uint8_t wk = a.P.use_APD ? weak_in[c] : (uint8_t)DPE_STRONG;
+  a.weak[c] = wk;
+  weak_flag[c] = (a.P.use_APD && wk == DPE_WEAK) ? 1 : 0;
+  a.rng_ctr[c] = 0u;
+  a.radius[c] = a.P.strong_radius;
+  a.fit_plane[c] = make_float4(0, 0, 0, 0);
+  a.reliable[c] = 0;
+  a.complexity[c] = 0.0f;
+  a.vweight[c] = make_uint4(0, 0, 0, 0);
+  a.cost[c] = 0.0f;
+}
+
+// ------------------------------------------------------------------ GenEdgeInform (DPE.cu:2487-2595)
+__global__ void k_gen_edge_inform(const __grid_constant__ PMArgs a) {
+  int px, py;
+  if (!full_pixel(a, &px, &py)) return;
+  const int W = a.W, H = a.H, center = px + py * W;
+  if (a.P.use_edge) {
+    short2 *en = &a.edge_neigh[(size_t)center * 8];
+    for (int i = 0; i < 8; ++i) {
+      short2 found = make_short2(-1, -1);
+      const int dx = kDir[i][0], dy = kDir[i][1];
+      int nx = px + dx, ny = py + dy;
+      while (nx >= 0 && nx < W && ny >= 0 && ny < H) {
+        if (a.edge[nx + ny * W]) { found = make_short2(nx, ny); break; }
+        nx += dx; ny += dy;
+      }
+      en[i] = found;
+    }
+    const int r = a.P.strong_radius;
+    int edge_pix = 0, tot_pix = 0, bound_pix = 0;
+    for (int i = -r; i <= r; ++i)
+      for (int j = -r; j <= r; ++j) {
+        const int nx = px + i, ny = py + j;
+        if (nx < 0 || nx >= W || ny < 0 || ny >= H) continue;
+        if (a.edge[ny * W + nx]) edge_pix++;
+        if (a.P.use_label && a.label[ny * W + nx] == 0) bound_pix++;
+        tot_pix++;
+      }
+    float density = 1.0f * edge_pix / tot_pix;
+    if (a.P.use_label) density = cvmax(density, bound_pix / tot_pix);  // integer division (quirk Q6)
+    a.complexity[center] = (float)(1.0f / (1.0f + exp(-25.0 * (density - 0.35))));
+  }
+  if (a.P.use_label && a.weak[center] == DPE_WEAK) {
+    const int cl = a.label[center];
+    if (cl > 0) {
+      short2 *lb = &a.lab_bound[(size_t)a.nmap[center] * 8];
+      for (int i = 0; i < 8; ++i) {
+        const int dx = kDir[i][0], dy = kDir[i][1];
+        int nx = px + dx, ny = py + dy, lx = -1, ly = -1;
+        while (nx >= 0 && nx < W && ny >= 0 && ny < H) {
+          const int nl = a.label[nx + ny * W];
+          if (nl == cl) { lx = nx; ly = ny; }
+          else if (nl == -1) break;
+          nx += dx; ny += dy;
+        }
+        lb[i] = make_short2(lx, ly);
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------------ FindNearestStrongPoint (DPE.cu:2859-2893)
+__global__ void k_find_nearest_strong(const __grid_constant__ PMArgs a) {
+  int px, py;
+  if (!full_pixel(a, &px, &py)) return;
+  const int W = a.W, H = a.H, center = px + py * W;
+  short2 res = make_short2(-1, -1);
+  if (a.weak[center] == DPE_WEAK) {
+    for (int r = 1; r <= 100; ++r) {
+      bool found = false;
+      for (int x = -r; x <= r && !found; ++x) {
+        const int nx = px + x;
+        const bool edge_col = (x == -r || x == r);
+        // inner loop over y: full column on the ring's left/right edges, else only y = -r and y = r
+        for (int y = -r; y <= r; y += edge_col ? 1 : 2 * r) {
+          const int ny = py + y;
+          if (nx < 0 || ny < 0 || nx >= W || ny >= H) continue;
+          if (a.weak[nx + ny * W] == DPE_STRONG) { res = make_short2(nx, ny); found = true; break; }
+        }
+      }
+      if (found) break;
+    }
+  }
+  a.nearest[center] = res;
+}
+
+// ------------------------------------------------------------------ geometry helpers for GenNeighbours
+__device__ __forceinline__ uint8_t edge_at(const PMArgs &a, long idx) {
+  return (idx >= 0 && idx < (long)a.W * a.H) ? a.edge[idx] : (uint8_t)0;
+}
+__device__ __forceinline__ uint8_t edge_low_at(const PMArgs &a, long idx) {
+  return (idx >= 0 && idx < (long)a.lowW * a.lowH) ? a.edge_low[idx] : (uint8_t)0;
+}
+
+// BresenhamLine (DPE.cu:162-248); out-of-image linear indices read 0.
+__device__ bool bresenham(const PMArgs &a, int ax, int ay, int bx, int by) {
+  if (edge_at(a, (long)ax + (long)ay * a.W) || edge_at(a, (long)bx + (long)by * a.W)) return false;
+  const float scale_x = 1.0f * a.lowW / (float)a.W;
+  const float scale_y = 1.0f * a.lowH / (float)a.H;
+  const int h = a.lowH, w = a.lowW;
+  const int max_step = a.P.high_res_img ? (int)round(cvmax(h, w) / 60.0) : cvmax(h, w);
+  for (int pass = 0; pass < 2; ++pass) {
+    const int fx = pass == 0 ? bx : ax, fy = pass == 0 ? by : ay;
+    const int tx = pass == 0 ? ax : bx, ty = pass == 0 ? ay : by;
+    int x0 = (int)cvmin(roundf(fx * scale_x), (float)(w - 1));
+    int y0 = (int)cvmin(roundf(fy * scale_y), (float)(h - 1));
+    const int x1 = (int)cvmin(roundf(tx * scale_x), (float)(w - 1));
+    const int y1 = (int)cvmin(roundf(ty * scale_y), (float)(h - 1));
+    const int dx = abs(x1 - x0), sx = x0 < x1 ? 1 : -1;
+    const int dy = abs(y1 - y0), sy = y0 < y1 ? 1 : -1;
+    int err = (dx > dy ? dx : dy) / 2;
+    int step = 0;
+    bool tagx = true, tagy = true;
+    while (tagx || tagy) {
+      if (x0 == x1) tagx = false;
+      if (y0 == y1) tagy = false;
+      const int e2 = err;
+      if (e2 > -dx) { err -= dy; x0 += sx; }
+      if (e2 < dy) { err += dx; y0 += sy; }
+      if (edge_low_at(a, (long)x0 + (long)y0 * w)) return true;
+      step += 1;
+      if (step >= max_step) break;
+    }
+  }
+  return false;
+}
+
+// PointinTriangle (DPE.cu:139-160)
+__device__ __forceinline__ bool point_in_triangle(short2 A, short2 B, short2 C, int px, int py) {
+  const float2 AB = make_float2(B.x - A.x, B.y - A.y), BC = make_float2(C.x - B.x, C.y - B.y), CA = make_float2(A.x - C.x, A.y - C.y);
+  const float ab = sqrtf(AB.x * AB.x + AB.y * AB.y), bc = sqrtf(BC.x * BC.x + BC.y * BC.y), ca = sqrtf(CA.x * CA.x + CA.y * CA.y);
+  if (ab <= 2 || bc <= 2 || ca <= 2) return false;
+  if (!(ab + bc > ca && bc + ca > ab && ab + ca > bc)) return false;
+  const float2 PA = make_float2(A.x - px, A.y - py), PB = make_float2(B.x - px, B.y - py), PC = make_float2(C.x - px, C.y - py);
+  const float t1 = PA.x * PB.y - PA.y * PB.x, t2 = PB.x * PC.y - PB.y * PC.x, t3 = PC.x * PA.y - PC.y * PA.x;
+  return t1 * t2 >= 0 && t1 * t3 >= 0;
+}
+
+__device__ __forceinline__ void sort_small(float *d, int n) {
+  for (int i = 1; i < n; ++i) {
+    const float t = d[i];
+    int j;
+    for (j = i; j >= 1 && t < d[j - 1]; j--) d[j] = d[j - 1];
+    d[j] = t;
+  }
+}
+
+// ------------------------------------------------------------------ GenNeighbours (DPE.cu:2107-2467)
+__global__ void __launch_bounds__(128) k_gen_neighbours(const __grid_constant__ PMArgs a) {
+  int px, py;
+  if (!full_pixel(a, &px, &py)) return;
+  const int W = a.W, H = a.H, center = px + py * W;
+  if (a.weak[center] != DPE_WEAK) return;
+  constexpr int kMaxPts = 64;
+  const int margin = 6;
+  const float depth_diff = a.P.depth_max - a.P.depth_min;
+  const dpe_camera &cam = a.cam[0];
+  Rng rng = make_rng(a, center);
+  short2 *nbs = &a.neigh[(size_t)a.nmap[center] * kNeighbours];
+  nbs[0] = make_short2(px, py);
+  for (int i = 1; i < kNeighbours; ++i) nbs[i] = make_short2(-1, -1);
+  short2 pts[kMaxPts];
+  uint64_t valid = 0;
+  int odi = -1, npts = 0;
+  const int rt = a.P.rotate_time;
+  const float angle = 45.0f / rt;
+  const float cos_a = (float)cos(angle * 3.14159265358979323846 / 180.f);
+  const float sin_a = (float)sin(angle * 3.14159265358979323846 / 180.f);
+  const float thr = (float)cos((angle / 2.0f) * 3.14159265358979323846 / 180.0f);
+  const int shift_range = cvmax((int)(tan((angle / 2.0f) * 3.14159265358979323846 / 180.0f) * 20), 1);
+  const float ransac_thr = a.P.ransac_threshold * depth_diff;
+  bool edge_limit = false;
+  if (a.P.use_limit) {
+    edge_limit = true;
+    if (a.P.use_edge) {
+      const float cv = a.complexity[center];
+      const float rp = rng.uniform() - FLT_EPSILON;
+      if (rp < cv) edge_limit = false;
+      else a.complexity[center] = cvmax(0.99f, cv);
+    }
+  }
+  for (int odx = -1; odx <= 1; ++odx)
+    for (int ody = -1; ody <= 1; ++ody) {
+      if (odx == 0 && ody == 0) continue;
+      float2 od = make_float2((float)odx, (float)ody);
+      normalize2(&od);
+      odi++;
+      for (int ri = 0; ri < rt; ++ri) {
+        const int di = odi * 4 + ri;
+        for (int radius = 2; radius <= 4096; radius = cvmin(radius * 2, radius + 25)) {
+          const float2 tp = make_float2(px + od.x * radius, py + od.y * radius);
+          if (tp.x < 0 || tp.y < 0 || tp.x >= W || tp.y >= H) break;
+          for (int k = 0; k < 4; ++k) {
+            uint32_t sgn = (rng.u32() % 2 == 0) ? 1u : 0xFFFFFFFFu;
+            const int rxs = (int)((sgn * rng.u32()) % (uint32_t)shift_range);
+            sgn = (rng.u32() % 2 == 0) ? 1u : 0xFFFFFFFFu;
+            const int rys = (int)((sgn * rng.u32()) % (uint32_t)shift_range);
+            float2 dir = make_float2(od.x * 20 + rxs, od.y * 20 + rys);
+            normalize2(&dir);
+            short2 nb = make_short2((short)(int)(px + dir.x * radius), (short)(int)(py + dir.y * radius));
+            if (nb.x < margin || nb.y < margin || nb.x >= W - margin || nb.y >= H - margin) continue;
+            int nbc = nb.x + nb.y * W;
+            if (a.weak[nbc] != DPE_STRONG) {
+              nb = a.nearest[nbc];
+              if (nb.x == -1 || nb.y == -1) continue;
+              nbc = nb.x + nb.y * W;
+            }
+            float2 td = make_float2((float)(nb.x - px), (float)(nb.y - py));
+            normalize2(&td);
+            const float ca = td.x * od.x + td.y * od.y;
+            if (ca > thr && (!edge_limit || !bresenham(a, px, py, nb.x, nb.y))) {
+              pts[di] = nb; valid |= 1ull << di; npts++;
+              break;
+            }
+          }
+          if ((valid >> di) & 1ull) break;
+        }
+        float2 rd = make_float2(od.x * cos_a - od.y * sin_a, od.x * sin_a + od.y * cos_a);
+        normalize2(&rd);
+        od = rd;
+      }
+    }
+  int ext = 31;
+  if (a.P.use_label && a.label[center] > 0) {
+    const short2 *lb = &a.lab_bound[(size_t)a.nmap[center] * 8];
+    float bd[8];
+    int ds[8];
+    for (int i = 0; i < 8; ++i) {
+      const short2 b = lb[i];
+      float dist = 0.0f;
+      if (b.x != -1 && b.y != -1) {
+        const double ddx = (double)(px - b.x), ddy = (double)(py - b.y);
+        dist = (float)sqrt(ddx * ddx + ddy * ddy);
+        if (i >= 4) dist = (float)(dist / sqrt(2.0));
+      }
+      bd[i] = dist;
+      if (i % 2 == 1) {
+        const float od2 = bd[i - 1];
+        const int step = cvmin(1, cvmax(2 * rt - 1, (int)(2 * rt * dist / (dist + od2))));  // quirk Q5
+        ds[i - 1] = 2 * rt - step;
+        ds[i] = step;
+      }
+    }
+    for (int i = 0; i < 8; ++i) {
+      const float dist = bd[i];
+      const int gap = ds[i] + 1;
+      const int step_len = cvmax(1, (int)floor(1.0 * dist / gap));
+      for (int s = 1; s <= ds[i]; ++s) {
+        short2 nb = make_short2((short)(px + s * step_len * kDir[i][0]), (short)(py + s * step_len * kDir[i][1]));
+        if (nb.x < margin || nb.y < margin || nb.x >= W - margin || nb.y >= H - margin) continue;
+        int nbc = nb.x + nb.y * W;
+        if (a.weak[nbc] != DPE_STRONG) {
+          nb = a.nearest[nbc];
+          if (nb.x == -1 || nb.y == -1) continue;
+          nbc = nb.x + nb.y * W;
+        }
+        if (a.label[nbc] != 0 && a.label[nbc] != a.label[center]) continue;
+        ext++;
+        pts[ext] = nb; valid |= 1ull << ext; npts++;
+      }
+    }
+  }
+  if (npts <= 3) { a.reliable[center] = 0; a.rng_ctr[center] = rng.ctr; return; }
+
+  short2 sv[kMaxPts];
+  float3 sv3[kMaxPts], svn[kMaxPts];
+  int vc = 0;
+  float X[3];
+  point3d(cam, px, py, a.plane[center].w, X);
+  const float cwz = X[2];
+  for (int i = 0; i < kMaxPts; ++i) {
+    if ((valid >> i) & 1ull) {
+      const short2 sp = pts[i];
+      const int spc = sp.x + sp.y * W;
+      const float4 spl = a.plane[spc];
+      sv[vc] = sp;
+      point3d(cam, sp.x, sp.y, spl.w, X);
+      sv3[vc] = make_float3(X[0], X[1], X[2]);
+      const float4 n4 = normal_to_ref(cam, spl);
+      svn[vc] = make_float3(n4.x, n4.y, n4.z);
+      vc++;
+    }
+  }
+  float4 best = make_float4(0, 0, 0, 0);
+  bool has_valid = false;
+  {
+    int iteration = 50, max_iter = a.P.high_res_img ? 200 : 125, max_count = 3;
+    float min_cost = FLT_MAX;
+    float residuals[kMaxPts];
+    for (int i = 0; i < kMaxPts; ++i) residuals[i] = 0.0f;
+    float tthr = ransac_thr;
+    bool has_consist = false;
+    bool must_tri = (a.P.use_label && a.label[center] > 0 && edge_limit) ? false : true;
+    while (iteration > 0 && max_iter > 0) {
+      max_iter--;
+      const int ia = (int)(rng.u32() % (uint32_t)vc);
+      const int ib = (int)(rng.u32() % (uint32_t)vc);
+      const int ic = (int)(rng.u32() % (uint32_t)vc);
+      if (ia == ib || ib == ic || ia == ic) continue;
+      if (must_tri && !point_in_triangle(sv[ia], sv[ib], sv[ic], px, py)) continue;
+      if (edge_limit) {
+        if (bresenham(a, sv[ia].x, sv[ia].y, sv[ib].x, sv[ib].y) || bresenham(a, sv[ib].x, sv[ib].y, sv[ic].x, sv[ic].y) ||
+            bresenham(a, sv[ic].x, sv[ic].y, sv[ia].x, sv[ia].y))
+          continue;
+      }
+      bool nc = false;
+      if (a.P.geom_consistency && edge_limit) {
+        const float3 AN = svn[ia], BN = svn[ib], CN = svn[ic];
+        nc = true;
+        if ((double)(AN.x * BN.x + AN.y * BN.y + AN.z * BN.z) < 0.8660254 ||
+            (double)(AN.x * CN.x + AN.y * CN.y + AN.z * CN.z) < 0.8660254 ||
+            (double)(BN.x * CN.x + BN.y * CN.y + BN.z * CN.z) < 0.8660254)
+          nc = false;
+        if (has_consist && !nc) continue;
+      }
+      iteration--;
+      const float3 A = sv3[ia], B = sv3[ib], C = sv3[ic];
+      const float3 AC = make_float3(A.x - C.x, A.y - C.y, A.z - C.z), BC = make_float3(B.x - C.x, B.y - C.y, B.z - C.z);
+      float4 cr;
+      cr.x = AC.y * BC.z - BC.y * AC.z;
+      cr.y = -(AC.x * BC.z - BC.x * AC.z);
+      cr.z = AC.x * BC.y - BC.x * AC.y;
+      if ((cr.x == 0 && cr.y == 0 && cr.z == 0) || isnan(cr.x) || isnan(cr.y) || isnan(cr.z)) continue;
+      normalize3(&cr);
+      cr.w = -(cr.x * A.x + cr.y * A.y + cr.z * A.z);
+      int tcount = 0;
+      float sdist = 0.0f;
+      for (int s = 0; s < vc; ++s) {
+        const float fx = (sv[s].x - cam.K[2]) / cam.K[0];
+        const float fy = (sv[s].y - cam.K[5]) / cam.K[4];
+        const float fd = -cr.w / (cr.x * fx + cr.y * fy + cr.z);
+        const float dist = fabsf(fd - sv3[s].z);
+        residuals[s] = dist;
+        if (dist < tthr) { tcount++; sdist += dist; }
+      }
+      if (tcount < 6) continue;
+      const float fx = (px - cam.K[2]) / cam.K[0], fy = (py - cam.K[5]) / cam.K[4];
+      if (tcount > max_count) {
+        if (!must_tri && point_in_triangle(sv[ia], sv[ib], sv[ic], px, py)) must_tri = true;
+        if (!has_consist && nc) has_consist = true;
+        const float fd = -cr.w / (cr.x * fx + cr.y * fy + cr.z);
+        const float cd = fabsf(fd - cwz);
+        best = cr; max_count = tcount; sdist /= tcount; min_cost = cd; has_valid = true;
+        if (tthr > (a.P.high_res_img ? 0.05 : 0.005)) {
+          sort_small(residuals, vc);
+          if (tthr < residuals[kNeighbours]) continue;
+          tthr = (float)(residuals[kNeighbours] - 1e-6);
+          tcount = 0;
+          for (int s = 0; s < vc; ++s) {
+            if (residuals[s] < tthr) tcount++;
+            else break;
+          }
+          max_count = tcount;
+        }
+      } else if (tcount == max_count) {
+        if (!must_tri && point_in_triangle(sv[ia], sv[ib], sv[ic], px, py)) must_tri = true;
+        const float fd = -cr.w / (cr.x * fx + cr.y * fy + cr.z);
+        const float cd = fabsf(fd - cwz);
+        if (cd < min_cost) { best = cr; max_count = tcount; sdist /= tcount; min_cost = cd; }
+      }
+    }
+  }
+  a.rng_ctr[center] = rng.ctr;
+  if (!has_valid) { a.reliable[center] = 0; return; }
+  float weight[kMaxPts];
+  for (int i = 0; i < vc; ++i) {
+    const float fx = (sv[i].x - cam.K[2]) / cam.K[0];
+    const float fy = (sv[i].y - cam.K[5]) / cam.K[4];
+    const float fd = -best.w / (best.x * fx + best.y * fy + best.z);
+    const float dist = fabsf(fd - sv3[i].z);
+    if (dist >= ransac_thr) { sv[i] = make_short2(-1, -1); weight[i] = FLT_MAX; continue; }
+    weight[i] = dist;
+  }
+  for (int i = 1; i < vc; ++i) {
+    const short2 tp = sv[i];
+    const float tw = weight[i];
+    int j;
+    for (j = i; j >= 1 && tw < weight[j - 1]; j--) { sv[j] = sv[j - 1]; weight[j] = weight[j - 1]; }
+    sv[j] = tp; weight[j] = tw;
+  }
+  for (int i = 1; i < kNeighbours; ++i) nbs[i] = (i - 1 < vc) ? sv[i - 1] : make_short2(-1, -1);
+  a.reliable[center] = 1;
+}
+
+__global__ void k_neighbour_update(const __grid_constant__ PMArgs a) {
+  int px, py;
+  if (!full_pixel(a, &px, &py)) return;
+  const int c = px + py * a.W;
+  if (a.weak[c] == DPE_WEAK && a.reliable[c] != 1) a.weak[c] = DPE_UNKNOWN;
+}
+
+// ------------------------------------------------------------------ RandomInitialization (DPE.cu:1039-1067, 784-861)
+__global__ void __launch_bounds__(128) k_random_init(const __grid_constant__ PMArgs a) {
+  int px, py;
+  if (!full_pixel(a, &px, &py)) return;
+  const int center = px + py * a.W;
+  const dpe_camera &rc = a.cam[0];
+  RefWindow rw;
+  build_ref_window(a, px, py, rw);
+  const int n = a.N - 1;
+  if (a.P.state == DPE_FIRST_INIT) {
+    Rng rng = make_rng(a, center);
+    const float depth = rng.uniform() * (a.P.depth_max - a.P.depth_min) + a.P.depth_min;
+    float4 pl = random_normal(rc, px, py, rng, depth);
+    pl.w = dist_to_origin(rc, px, py, depth, pl);
+    a.rng_ctr[center] = rng.ctr;
+    a.plane[center] = pl;
+    float cv[kMaxSrc], srt[kMaxSrc];
+    int valid = 0;
+    for (int i = 0; i < n; ++i) {
+      const float v = ncc_strong(a, px, py, i + 1, pl, rw);
+      cv[i] = v; srt[i] = v;
+      if (v < 2.0f) valid++;
+    }
+    sort_small(srt, n);
+    uint32_t views = 0;
+    float cost = 2.0f;
+    const int k = min(valid, a.P.top_k);
+    if (k > 0) {
+      float c = 0.0f;
+      for (int i = 0; i < k; ++i) c += srt[i];
+      const float thr = srt[k - 1];
+      for (int i = 0; i < n; ++i)
+        if (cv[i] <= thr) setBit(&views, i);
+      cost = c / k;
+    }
+    a.views[center] = views;
+    a.cost[center] = cost;
+  } else {
+    float4 pl = normal_to_ref(rc, a.plane[center]);
+    const float depth = pl.w;
+    pl.w = dist_to_origin(rc, px, py, depth, pl);
+    a.plane[center] = pl;
+    uint32_t views = a.views[center];
+    int cnt = 0;
+    float cost = 0.0f;
+    for (int i = 1; i < a.N; ++i) {
+      if (isSet(views, i - 1)) {
+        const float v = ncc_strong(a, px, py, i, pl, rw);
+        if (v < 2.0f) { cnt++; cost += v; }
+        else unSetBit(&views, i - 1);
+      }
+    }
+    a.views[center] = views;
+    a.cost[center] = cnt == 0 ? 2.0f : cost / cnt;
+  }
+}
+
+// ------------------------------------------------------------------ shared pieces of the propagation kernels
+// Multi-hypothesis joint view selection (DPE.cu:1551-1619 / 1714-1783).
+__device__ __forceinline__ float sample_views(const PMArgs &a, Rng &rng, int iter, const float (*cost_array)[kMaxSrc],
+                                              const float *priors, uint8_t *vw, uint32_t *temp_sel) {
+  const int n = a.N - 1;
+  for (int i = 0; i < 32; ++i) vw[i] = 0;
+  float probs[kMaxSrc];
+  const float thr = (float)(0.8 * (double)expf((float)(iter * iter) / (-90.0f)));
+  const float base = expf(thr * thr / (-0.32f));
+  for (int i = 0; i < n; ++i) {
+    float count = 0;
+    int count_false = 0;
+    float tmpw = 0;
+    for (int j = 0; j < 8; ++j) {
+      const float v = cost_array[j][i];
+      if (v < thr) { tmpw += expf(v * v / (-0.18f)); count++; }
+      if (v > 1.2f) count_false++;
+    }
+    float p = 0.0f;
+    if (count > 2 && count_false < 3) p = tmpw / count;
+    else if (count_false < 3) p = base;
+    probs[i] = p * priors[i];
+  }
+  float sum = 0.0f;
+  for (int i = 0; i < n; ++i) sum += probs[i];
+  const float inv = 1.0f / sum;
+  float cum = 0.0f;
+  for (int i = 0; i < n; ++i) { cum += probs[i] * inv; probs[i] = cum; }
+  for (int s = 0; s < 15; ++s) {
+    const float r = rng.uniform() - FLT_EPSILON;
+    for (int id = 0; id < n; ++id)
+      if (probs[id] > r) { vw[id] += 1; break; }
+  }
+  uint32_t sel = 0;
+  float wn = 0;
+  for (int i = 0; i < n; ++i)
+    if (vw[i] > 0) { setBit(&sel, i); wn += vw[i]; }
+  *temp_sel = sel;
+  return wn;
+}
+
+__device__ __forceinline__ int find_min_cost_index(const float *c, int n) {
+  float m = c[0];
+  int idx = 0;
+  for (int i = 1; i < n; ++i)
+    if (c[i] <= m) { m = c[i]; idx = i; }
+  return idx;
+}
+
+// ------------------------------------------------------------------ strong update (DPE.cu:1218-1670, 1069-1122)
+__global__ void __launch_bounds__(128) k_strong_update(const __grid_constant__ PMArgs a, int iter, int parity) {
+  int px, py;
+  if (!colour_pixel(a, parity, &px, &py)) return;
+  const int W = a.W, H = a.H, n = a.N - 1;
+  const int center = py * W + px;
+  if (a.weak[center] == DPE_WEAK) return;
+  const dpe_camera &rc = a.cam[0];
+  RefWindow rw;
+  build_ref_window(a, px, py, rw);
+  float cost_array[8][kMaxSrc];
+  for (int d = 0; d < 8; ++d)
+    for (int j = 0; j < n; ++j) cost_array[d][j] = 0.0f;
+  cost_array[0][0] = 2.0f;  // `= {2.0f}` initialises only the first element (quirk Q2)
+  bool flag[8] = {false, false, false, false, false, false, false, false};
+  int positions[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  const float4 *cand_plane = a.P.use_edge ? a.plane_snap : a.plane;
+  const float *cand_cost = a.P.use_edge ? a.cost_snap : a.cost;
+
+  if (a.P.use_edge) {
+    const short2 *en = &a.edge_neigh[(size_t)center * 8];
+    const float max_edge_dist = cvmax(H, W) / 30.0f;
+    const int min_step = 2;
+    const bool on_edge = a.edge[center] != 0;
+    for (int d = 0; d < 8; ++d) {
+      const int dx = kDir[d][0], dy = kDir[d][1];
+      const int sx = cvmax(1, 5 - 2 * iter) * dx, sy = cvmax(1, 5 - 2 * iter) * dy;
+      const short2 e = en[d];
+      const double ex = (double)(e.x - px), ey = (double)(e.y - py);
+      float dist = (float)sqrt(ex * ex + ey * ey);
+      if (d >= 4) dist = (float)(dist / sqrt(2.0));
+      if (on_edge) dist = 11 * min_step;
+      else if (e.x == -1 || e.y == -1 || dist > max_edge_dist) {
+        dist = max_edge_dist;
+        if (d >= 4) dist = (float)(dist / sqrt(2.0));
+      }
+      const int step_num = cvmin(cvmax(11, (int)(1.0f * dist / min_step)), 22);
+      int step_len = cvmax((int)(1.0f * dist / step_num), min_step);
+      if (d < 4 && step_len % 2 == 1) step_len -= 1;
+      float mc = FLT_MAX;
+      int mp = -1;
+      int fx = 0, fy = 0;
+      if (d > 4) { if (d % 2) fx = dx; else fy = dy; }
+      for (int s = 0; s < step_num; ++s) {
+        const int tx = px + sx + s * step_len * dx + fx, ty = py + sy + s * step_len * dy + fy;
+        if (!(tx >= 0 && ty >= 0 && tx < W && ty < H)) continue;
+        const int tc = tx + ty * W;
+        const float cc = cand_cost[tc];
+        if (mc > cc) { mp = tc; mc = cc; }
+      }
+      if (mc < FLT_MAX) {
+        flag[d] = true;
+        positions[d] = mp;
+        const float4 cp = cand_plane[mp];
+        for (int j = 0; j < n; ++j) cost_array[d][j] = ncc_strong(a, px, py, j + 1, cp, rw);
+      }
+    }
+    if (!on_edge) {
+      const float good_thr = 0.8f * expf((float)(iter * iter) / (-90.0f));
+      for (int d = 0; d < 8; ++d) {
+        const int dx = kDir[d][0], dy = kDir[d][1];
+        const int sx = cvmax(1, 5 - 2 * iter) * dx, sy = cvmax(1, 5 - 2 * iter) * dy;
+        const bool had = flag[d];
+        float mc = FLT_MAX;
+        int mp = -1;
+        int fx = 0, fy = 0;
+        if (d > 4) { if (d % 2) fx = dx; else fy = dy; }
+        for (int s = 0; s < 11; ++s) {
+          const int tx = px + sx + s * min_step * dx + fx, ty = py + sy + s * min_step * dy + fy;
+          if (!(tx >= 0 && ty >= 0 && tx < W && ty < H)) continue;
+          const int tc = tx + ty * W;
+          const float cc = cand_cost[tc];
+          if (mc > cc) { mp = tc; mc = cc; }
+        }
+        if (mc < FLT_MAX) {
+          flag[d] = true;
+          float tca[kMaxSrc];
+          const float4 cp = cand_plane[mp];
+          for (int j = 0; j < n; ++j) tca[j] = ncc_strong(a, px, py, j + 1, cp, rw);
+          int g0 = 0, g1 = 0, b0 = 0, b1 = 0;
+          for (int j = 0; j < n; ++j) {
+            if (cost_array[d][j] < good_thr) g0++;
+            if (cost_array[d][j] > 1.2f) b0++;
+            if (tca[j] < good_thr) g1++;
+            if (tca[j] > 1.2f) b1++;
+          }
+          if (!had || g1 > g0 || (g1 == g0 && b1 < b0)) {
+            positions[d] = mp;
+            for (int j = 0; j < n; ++j) cost_array[d][j] = tca[j];
+          }
+        }
+      }
+    }
+  } else {
+    // 0 up_near, 1 up_far, 2 down_near, 3 down_far, 4 left_near, 5 left_far, 6 right_near, 7 right_far
+    const int starts[4] = {center - 3 * W, center + 3 * W, center - 3, center + 3};
+    const int strides[4] = {-W, W, -1, 1};
+    const bool oks[4] = {py > 2, py < H - 3, px > 2, px < W - 3};
+    for (int f = 0; f < 4; ++f) {
+      if (!oks[f]) continue;
+      const int slot = 2 * f + 1;
+      flag[slot] = true;
+      float m = a.cost[starts[f]];
+      int mp = starts[f];
+      for (int i = 1; i < 11; ++i) {
+        bool ok;
+        switch (f) {
+          case 0: ok = py > 2 + 2 * i; break;
+          case 1: ok = py < H - 3 - 2 * i; break;
+          case 2: ok = px > 2 + 2 * i; break;
+          default: ok = px < W - 3 - 2 * i; break;
+        }
+        if (ok) {
+          const int t = starts[f] + 2 * i * strides[f];
+          const float ct = a.cost[t];
+          if (ct < m) { m = ct; mp = t; }
+        }
+      }
+      positions[slot] = mp;
+    }
+    // near: base pixel one step away, then diagonal pairs at distance 1..3
+    const int nbase[4] = {center - W, center + W, center - 1, center + 1};
+    const bool nok[4] = {py > 0, py < H - 1, px > 0, px < W - 1};
+    for (int f = 0; f < 4; ++f) {
+      if (!nok[f]) continue;
+      const int slot = 2 * f;
+      flag[slot] = true;
+      float m = a.cost[nbase[f]];
+      int mp = nbase[f];
+      for (int i = 0; i < 3; ++i)
+        for (int side = 0; side < 2; ++side) {
+          bool ok;
+          int t;
+          const int k = 1 + i;
+          switch (f) {
+            case 0: t = nbase[0] - k * W + (side ? k : -k); ok = py > 1 + i && (side ? px < W - 1 - i : px > i); break;
+            case 1: t = nbase[1] + k * W + (side ? k : -k); ok = py < H - 2 - i && (side ? px < W - 1 - i : px > i); break;
+            case 2: t = nbase[2] - k + (side ? k * W : -k * W); ok = px > 1 + i && (side ? py < H - 1 - i : py > i); break;
+            default: t = nbase[3] + k + (side ? k * W : -k * W); ok = px < W - 2 - i && (side ? py < H - 1 - i : py > i); break;
+          }
+          if (ok) {
+            const float ct = a.cost[t];
+            if (ct < m) { m = ct; mp = t; }
+          }
+        }
+      positions[slot] = mp;
+    }
+    for (int d = 0; d < 8; ++d) {
+      if (!flag[d]) continue;
+      const float4 cp = a.plane[positions[d]];
+      for (int j = 0; j < n; ++j) cost_array[d][j] = ncc_strong(a, px, py, j + 1, cp, rw);
+    }
+  }
+
+  float priors[kMaxSrc];
+  for (int j = 0; j < n; ++j) priors[j] = 0.0f;
+  const long total = (long)W * H;
+  const long nbr[4] = {(long)center - W, (long)center + W, (long)center - 1, (long)center + 1};
+  for (int i = 0; i < 4; ++i)
+    if (flag[2 * i]) {
+      const uint32_t sv = (nbr[i] >= 0 && nbr[i] < total) ? a.views[nbr[i]] : 0u;
+      for (int j = 0; j < n; ++j) priors[j] += isSet(sv, j) == 1 ? 0.9f : 0.1f;
+    }
+  Rng rng = make_rng(a, center);
+  uint8_t vw[32];
+  uint32_t temp_sel = 0;
+  const float wn = sample_views(a, rng, iter, cost_array, priors, vw, &temp_sel);
+  float final_costs[8];
+  for (int i = 0; i < 8; ++i) {
+    float fc = 0.0f;
+    for (int j = 0; j < n; ++j)
+      if (vw[j] > 0) fc += vw[j] * cost_array[i][j];
+    final_costs[i] = fc / wn;
+  }
+  const int mi = find_min_cost_index(final_costs, 8);
+  const float4 pl_cur = a.plane[center];
+  float cost_now = 0.0f;
+  for (int i = 0; i < n; ++i) {
+    // views with no samples contribute 0 * cost, and every cost is finite
+    if (vw[i] > 0) cost_now += vw[i] * ncc_strong(a, px, py, i + 1, pl_cur, rw);
+  }
+  cost_now /= wn;
+  const float cost_written = cost_now;
+  float depth_now = depth_from_plane(rc, pl_cur, px, py);
+  float4 pl_now = pl_cur;
+  uint32_t views_new = a.views[center];
+  if (flag[mi]) {
+    const float4 cand = cand_plane[positions[mi]];
+    const float db = depth_from_plane(rc, cand, px, py);
+    if (db >= a.P.depth_min && db <= a.P.depth_max && final_costs[mi] < cost_now) {
+      depth_now = db; pl_now = cand; cost_now = final_costs[mi];
+      views_new = temp_sel;
+    }
+  }
+  // PlaneHypothesisRefinementStrong (DPE.cu:1069-1122)
+  {
+    const float dmin = a.P.depth_min, dmax = a.P.depth_max;
+    const float depth_rand = rng.uniform() * (dmax - dmin) + dmin;
+    const float4 n_rand = random_normal(rc, px, py, rng, depth_now);
+    const float lo = (1 - 0.02f) * depth_now, hi = (1 + 0.02f) * depth_now;
+    const float depth_pert = rng.uniform() * (hi - lo) + lo;
+    const float4 n_pert = perturbed_normal(rc, px, py, pl_now, rng, (float)(0.02f * 3.14159265358979323846));
+    const float depths[5] = {depth_rand, depth_now, depth_rand, depth_now, depth_pert};
+    const float4 normals[5] = {pl_now, n_rand, n_rand, n_pert, pl_now};
+    for (int h = 0; h < 5; ++h) {
+      float4 t = normals[h];
+      t.w = dist_to_origin(rc, px, py, depths[h], t);
+      float tc = 0.0f;
+      for (int j = 0; j < n; ++j)
+        if (vw[j] > 0) tc += vw[j] * ncc_strong(a, px, py, j + 1, t, rw);
+      tc /= wn;
+      const float db = depth_from_plane(rc, t, px, py);
+      if (db >= dmin && db <= dmax && tc < cost_now) { depth_now = db; pl_now = t; cost_now = tc; }
+    }
+  }
+  a.rng_ctr[center] = rng.ctr;
+  a.views[center] = views_new;
+  store_vweight(&a.vweight[center], vw);
+  if (a.P.state == DPE_REFINE_INIT) {
+    if ((double)cost_now < (double)cost_written - 0.1) { a.cost[center] = cost_now; a.plane[center] = pl_now; }
+    else a.cost[center] = cost_written;
+  } else {
+    a.cost[center] = cost_now;
+    a.plane[center] = pl_now;
+  }
+}
+
+// ------------------------------------------------------------------ RANSACToGetFitPlane (DPE.cu:2895-3128)
+__global__ void __launch_bounds__(128) k_ransac_fit_plane(const __grid_constant__ PMArgs a) {
+  int px, py;
+  if (!full_pixel(a, &px, &py)) return;
+  const int W = a.W, center = px + py * W;
+  if (a.weak[center] != DPE_WEAK) { a.fit_plane[center] = a.plane[center]; return; }
+  Rng rng = make_rng(a, center);
+  const dpe_camera &cam = a.cam[0];
+  bool edge_limit = false;
+  if (a.P.use_limit) {
+    edge_limit = true;
+    if (a.P.use_edge) {
+      const float cv = a.complexity[center];
+      const float rp = rng.uniform() - FLT_EPSILON;
+      if (rp < cv) edge_limit = false;
+    }
+  }
+  short2 sp[kNeighbours - 1];
+  float3 sp3[kNeighbours - 1], spn[kNeighbours - 1];
+  int sc = 0;
+  float X[3];
+  for (int i = 1; i < kNeighbours; ++i) {
+    const short2 t = neighbour(a, center, i);
+    if (t.x == -1 || t.y == -1) continue;
+    sp[sc] = t;
+    const int tc = t.x + t.y * W;
+    const float4 tpl = a.plane[tc];
+    const float d = depth_from_plane(cam, tpl, t.x, t.y);
+    point3d(cam, t.x, t.y, d, X);
+    sp3[sc] = make_float3(X[0], X[1], X[2]);
+    spn[sc] = make_float3(tpl.x, tpl.y, tpl.z);
+    sc++;
+  }
+  if (sc < 3) { a.fit_plane[center] = a.plane[center]; a.rng_ctr[center] = rng.ctr; return; }
+  int ua = -1, ub = -1, uc = -1;
+  float min_cost = FLT_MAX;
+  float4 best = make_float4(0, 0, 0, 0);
+  bool has_best = false, has_strong = false;
+  bool must_tri = (a.P.use_label && a.label[center] > 0 && edge_limit) ? false : true;
+  for (int iteration = 0; iteration < 50; ++iteration) {
+    const int ia = (int)(rng.u32() % (uint32_t)sc);
+    const int ib = (int)(rng.u32() % (uint32_t)sc);
+    const int ic = (int)(rng.u32() % (uint32_t)sc);
+    if (ia == ib || ib == ic || ia == ic) continue;
+    bool is_strong = false;
+    if (a.P.geom_consistency && edge_limit) {
+      const float3 AN = spn[ia], BN = spn[ib], CN = spn[ic];
+      is_strong = true;
+      if ((double)(AN.x * BN.x + AN.y * BN.y + AN.z * BN.z) < 0.8660254 ||
+          (double)(AN.x * CN.x + AN.y * CN.y + AN.z * CN.z) < 0.8660254 ||
+          (double)(BN.x * CN.x + BN.y * CN.y + BN.z * CN.z) < 0.8660254)
+        is_strong = false;
+      if (has_strong && !is_strong) continue;
+    }
+    if (must_tri && !point_in_triangle(sp[ia], sp[ib], sp[ic], px, py)) continue;
+    if (edge_limit) {
+      if (bresenham(a, sp[ia].x, sp[ia].y, sp[ib].x, sp[ib].y) || bresenham(a, sp[ib].x, sp[ib].y, sp[ic].x, sp[ic].y) ||
+          bresenham(a, sp[ic].x, sp[ic].y, sp[ia].x, sp[ia].y))
+        continue;
+    }
+    const float3 A = sp3[ia], B = sp3[ib], C = sp3[ic];
+    const float3 AC = make_float3(A.x - C.x, A.y - C.y, A.z - C.z), BC = make_float3(B.x - C.x, B.y - C.y, B.z - C.z);
+    float4 cr;
+    cr.x = AC.y * BC.z - BC.y * AC.z;
+    cr.y = -(AC.x * BC.z - BC.x * AC.z);
+    cr.z = AC.x * BC.y - BC.x * AC.y;
+    if ((cr.x == 0 && cr.y == 0 && cr.z == 0) || isnan(cr.x) || isnan(cr.y) || isnan(cr.z)) continue;
+    normalize3(&cr);
+    cr.w = -(cr.x * A.x + cr.y * A.y + cr.z * A.z);
+    if (!has_strong && is_strong) has_strong = true;
+    float tc = 0.0f;
+    for (int s = 0; s < sc; ++s) {
+      if (s == ia || s == ib || s == ic) continue;
+      const float fx = (sp[s].x - cam.K[2]) / cam.K[0];
+      const float fy = (sp[s].y - cam.K[5]) / cam.K[4];
+      const float fd = -cr.w / (cr.x * fx + cr.y * fy + cr.z);
+      tc += fabsf(fd - sp3[s].z);
+    }
+    if (tc < min_cost) {
+      if (!must_tri && point_in_triangle(sp[ia], sp[ib], sp[ic], px, py)) must_tri = true;
+      min_cost = tc; best = cr; has_best = true; ua = ia; ub = ib; uc = ic;
+    }
+  }
+  a.rng_ctr[center] = rng.ctr;
+  if (has_best) {
+    const float depth = depth_from_plane(cam, a.plane[center], px, py);
+    const float4 v = view_direction(cam, px, py, depth);
+    if (best.x * v.x + best.y * v.y + best.z * v.z > 0) { best.x = -best.x; best.y = -best.y; best.z = -best.z; best.w = -best.w; }
+    a.fit_plane[center] = best;
+    if (a.P.use_radius) {
+      if (must_tri) {
+        const short2 A = sp[ua], B = sp[ub], C = sp[uc];
+        const float la = sqrtf((float)((A.x - B.x) * (A.x - B.x) + (A.y - B.y) * (A.y - B.y)));
+        const float lb = sqrtf((float)((B.x - C.x) * (B.x - C.x) + (B.y - C.y) * (B.y - C.y)));
+        const float lc = sqrtf((float)((C.x - A.x) * (C.x - A.x) + (C.y - A.y) * (C.y - A.y)));
+        const float p = (float)((la + lb + lc) / 2.0);
+        const float S = sqrtf(p * (p - la) * (p - lb) * (p - lc));
+        int radius = (int)floor(sqrtf(S) / 2.0);
+        const float ad = sqrtf((float)((A.x - px) * (A.x - px) + (A.y - py) * (A.y - py)));
+        const float bd = sqrtf((float)((B.x - px) * (B.x - px) + (B.y - py) * (B.y - py)));
+        const float cd = sqrtf((float)((C.x - px) * (C.x - px) + (C.y - py) * (C.y - py)));
+        const float md = cvmin(cvmin(ad, bd), cd);
+        if (2.5 * md < radius) radius = (int)md;
+        if (edge_limit) {
+          if (a.P.use_edge) {
+            float med = FLT_MAX;
+            const short2 *en = &a.edge_neigh[(size_t)center * 8];
+            for (int d = 0; d < 8; ++d) {
+              const short2 e = en[d];
+              if (e.x == -1 || e.y == -1) continue;
+              med = cvmin(med, sqrtf((float)((e.x - px) * (e.x - px) + (e.y - py) * (e.y - py))));
+            }
+            if (med < radius) radius = (int)med;
+          }
+          if (a.P.use_label && a.label[center] > 0) {
+            float mbd = FLT_MAX;
+            const short2 *lb2 = &a.lab_bound[(size_t)a.nmap[center] * 8];
+            for (int d = 0; d < 8; ++d) {
+              const short2 bb = lb2[d];
+              if (bb.x == -1 || bb.y == -1) continue;
+              const double ddx = (double)(px - bb.x), ddy = (double)(py - bb.y);
+              mbd = cvmin(mbd, (float)sqrt(ddx * ddx + ddy * ddy));
+            }
+            if (mbd < radius) radius = (int)mbd;
+          }
+        }
+        for (int guard = 0; (radius << 1) % 5 != 0 && guard < 5; ++guard) radius--;
+        if (!edge_limit) a.radius[center] = radius > a.P.strong_radius ? 0 : a.P.strong_radius;
+        else a.radius[center] = radius > a.P.strong_radius ? radius : a.P.strong_radius;
+      } else {
+        a.radius[center] = a.P.strong_radius;
+      }
+    }
+  } else {
+    a.fit_plane[center] = make_float4(0, 0, 0, 0);
+    if (a.P.use_radius) a.radius[center] = a.P.strong_radius;
+  }
+}
+
+// ------------------------------------------------------------------ weak update (DPE.cu:1672-1866, 1124-1216)
+__device__ __forceinline__ void cost_vector_weak(const PMArgs &a, int px, int py, float4 pl, float *cv) {
+  for (int i = 1; i < a.N; ++i) cv[i - 1] = ncc_weak(a, px, py, i, pl);
+}
+
+__global__ void __launch_bounds__(128) k_weak_update(const __grid_constant__ PMArgs a, int iter, int parity) {
+  int px, py;
+  if (!colour_pixel(a, parity, &px, &py)) return;
+  const int W = a.W, n = a.N - 1;
+  const int center = py * W + px;
+  if (a.weak[center] != DPE_WEAK) return;
+  const dpe_camera &rc = a.cam[0];
+  const bool geom = a.P.geom_consistency != 0;
+  const float gf = a.P.geom_factor;
+  float cost_array[8][kMaxSrc];
+  for (int d = 0; d < 8; ++d)
+    for (int j = 0; j < n; ++j) cost_array[d][j] = 0.0f;
+  cost_array[0][0] = 2.0f;
+  bool flag[8];
+  float4 cand[8];
+  for (int i = 0; i < 8; ++i) {
+    flag[i] = false;
+    cand[i] = make_float4(0, 0, 0, 0);
+    const short2 nb = neighbour(a, center, i + 1);
+    if (nb.x == -1 || nb.y == -1 || a.weak[nb.x + nb.y * W] != DPE_STRONG) continue;
+    flag[i] = true;
+    cand[i] = a.plane[nb.x + nb.y * W];
+    cost_vector_weak(a, px, py, cand[i], cost_array[i]);
+  }
+  float priors[kMaxSrc];
+  for (int j = 0; j < n; ++j) priors[j] = 0.0f;
+  for (int i = 0; i < 8; ++i) {
+    const short2 nb = neighbour(a, center, i + 1);
+    if (nb.x == -1 || nb.y == -1) continue;
+    const uint32_t sv = a.views[nb.x + nb.y * W];
+    for (int j = 0; j < n; ++j) priors[j] += isSet(sv, j) == 1 ? 0.9f : 0.1f;
+  }
+  Rng rng = make_rng(a, center);
+  uint8_t vw[32];
+  uint32_t temp_sel = 0;
+  const float wn = sample_views(a, rng, iter, cost_array, priors, vw, &temp_sel);
+  float final_costs[8];
+  for (int i = 0; i < 8; ++i) {
+    float fc = 0.0f;
+    for (int j = 0; j < n; ++j)
+      if (vw[j] > 0) {
+        if (geom) fc += vw[j] * (cost_array[i][j] + gf * (flag[i] ? geom_cost(a, px, py, j + 1, cand[i]) : 3.0f));
+        else fc += vw[j] * cost_array[i][j];
+      }
+    final_costs[i] = fc / wn;
+  }
+  const int mi = find_min_cost_index(final_costs, 8);
+  const float4 pl_cur = a.plane[center];
+  float cost_now = 0.0f;
+  for (int i = 0; i < n; ++i) {
+    if (vw[i] == 0) continue;  // 0 * (finite cost) contributes nothing
+    const float c = ncc_weak(a, px, py, i + 1, pl_cur);
+    if (geom) cost_now += vw[i] * (c + gf * geom_cost(a, px, py, i + 1, pl_cur));
+    else cost_now += vw[i] * c;
+  }
+  cost_now /= wn;
+  const float cost_written = cost_now;
+  float depth_now = depth_from_plane(rc, pl_cur, px, py);
+  float4 pl_now = pl_cur;
+  uint32_t views_new = a.views[center];
+  if (flag[mi]) {
+    const float db = depth_from_plane(rc, cand[mi], px, py);
+    if (db >= a.P.depth_min && db <= a.P.depth_max && final_costs[mi] < cost_now) {
+      depth_now = db; pl_now = cand[mi]; cost_now = final_costs[mi];
+      views_new = temp_sel;
+    }
+  }
+  // PlaneHypothesisRefinementWeak: the fitted plane, then five random hypotheses
+  const float dmin = a.P.depth_min, dmax = a.P.depth_max;
+  {
+    const float4 fp = a.fit_plane[center];
+    if (!(fp.x == 0 && fp.y == 0 && fp.z == 0)) {
+      float tc = 0.0f;
+      for (int j = 0; j < n; ++j)
+        if (vw[j] > 0) {
+          const float c = ncc_weak(a, px, py, j + 1, fp);
+          if (geom) tc += vw[j] * (c + gf * geom_cost(a, px, py, j + 1, fp));
+          else tc += vw[j] * c;
+        }
+      tc /= wn;
+      const float db = depth_from_plane(rc, fp, px, py);
+      if (db >= dmin && db <= dmax && tc < cost_now) { depth_now = db; pl_now = fp; cost_now = tc; }
+    }
+  }
+  {
+    const float depth_rand = rng.uniform() * (dmax - dmin) + dmin;
+    const float4 n_rand = random_normal(rc, px, py, rng, depth_now);
+    const float lo = (1 - 0.02f) * depth_now, hi = (1 + 0.02f) * depth_now;
+    const float depth_pert = rng.uniform() * (hi - lo) + lo;
+    const float4 n_pert = perturbed_normal(rc, px, py, pl_now, rng, (float)(0.02f * 3.14159265358979323846));
+    const float depths[5] = {depth_rand, depth_now, depth_rand, depth_now, depth_pert};
+    const float4 normals[5] = {pl_now, n_rand, n_rand, n_pert, pl_now};
+    for (int h = 0; h < 5; ++h) {
+      float4 t = normals[h];
+      t.w = dist_to_origin(rc, px, py, depths[h], t);
+      float tc = 0.0f;
+      for (int j = 0; j < n; ++j)
+        if (vw[j] > 0) {
+          const float c = ncc_weak(a, px, py, j + 1, t);
+          if (geom) tc += vw[j] * (c + gf * geom_cost(a, px, py, j + 1, t));
+          else tc += vw[j] * c;
+        }
+      tc /= wn;
+      const float db = depth_from_plane(rc, t, px, py);
+      if (db >= dmin && db <= dmax && tc < cost_now) { depth_now = db; pl_now = t; cost_now = tc; }
+    }
+  }
+  a.rng_ctr[center] = rng.ctr;
+  a.views[center] = views_new;
+  store_vweight(&a.vweight[center], vw);
+  float4 pl_final = pl_cur;
+  if (a.P.state == DPE_REFINE_INIT) {
+    if ((double)cost_now < (double)cost_written - 0.1) pl_final = pl_now;
+  } else {
+    pl_final = pl_now;
+  }
+  a.plane[center] = pl_final;
+  // final re-cost with the strong window (DPE.cu:1849-1865); the radius swap there has no effect
+  RefWindow rw;
+  build_ref_window(a, px, py, rw);
+  float cn = 0.0f;
+  for (int i = 0; i < n; ++i)
+    if (vw[i] > 0) cn += vw[i] * ncc_strong(a, px, py, i + 1, pl_final, rw);
+  a.cost[center] = cn / wn;
+}
+
+// ------------------------------------------------------------------ post passes
+__global__ void k_get_depth_normal(const __grid_constant__ PMArgs a) {
+  int px, py;
+  if (!full_pixel(a, &px, &py)) return;
+  const int c = py * a.W + px;
+  float4 pl = a.plane[c];
+  pl.w = depth_from_plane(a.cam[0], pl, px, py);
+  a.plane[c] = normal_to_world(a.cam[0], pl);
+}
+
+// CheckerboardFilterStrong (DPE.cu:1961-2071)
+__global__ void k_filter_strong(const __grid_constant__ PMArgs a, int parity) {
+  int px, py;
+  if (!colour_pixel(a, parity, &px, &py)) return;
+  const int W = a.W, H = a.H, center = py * W + px;
+  if (a.weak[center] == DPE_WEAK) return;
+  if (a.cost[center] < 0.001f) return;
+  float f[21];
+  int k = 0;
+  f[k++] = a.plane[center].w;
+  const int up = center - W, upup = center - 3 * W, dn = center + W, dndn = center + 3 * W;
+  const int lf = center - 1, lflf = center - 3, rt = center + 1, rtrt = center + 3;
+  const int idx[20] = {up, upup, upup - 2 * W, dn, dndn, dndn + 2 * W, lf, lflf, lflf - 2, rt, rtrt, rtrt + 2,
+                       up + 2, dn + 2, up - 2, dn - 2, lf - 2 * W, rt - 2 * W, lf + 2 * W, rt + 2 * W};
+  const bool ok[20] = {py > 0, py > 2, py > 4, py < H - 1, py < H - 3, py < H - 5, px > 0, px > 2, px > 4,
+                       px < W - 1, px < W - 3, px < W - 5, py > 0 && px < W - 2, py < H - 1 && px < W - 2,
+                       py > 0 && px > 1, py < H - 1 && px > 1, px > 0 && py > 2, px < W - 1 && py > 2,
+                       px > 0 && py < H - 2, px < W - 1 && py < H - 2};
+  for (int i = 0; i < 20; ++i)
+    if (ok[i] && a.weak[idx[i]] == DPE_STRONG) f[k++] = a.plane[idx[i]].w;
+  sort_small(f, k);
+  const int m = k / 2;
+  a.plane[center].w = (k % 2 == 0) ? (f[m - 1] + f[m]) / 2 : f[m];
+}
+
+// Common prologue of DepthToWeak / LocalRefine (DPE.cu:2619-2660, 2767-2806)
+struct Sweep {
+  float4 pl;
+  float depth, cost_now, base_line, weight_normal;
+  int valid;
+  uint32_t views;
+  uint4 vw;
+};
+__device__ __forceinline__ void sweep_setup(const PMArgs &a, int px, int py, const RefWindow &rw, Sweep &s) {
+  const int center = px + py * a.W;
+  s.pl = normal_to_ref(a.cam[0], a.plane[center]);
+  s.depth = s.pl.w;
+  s.cost_now = 0.0f; s.base_line = 0.0f; s.weight_normal = 0.0f; s.valid = 0;
+  s.views = a.views[center];
+  s.vw = a.vweight[center];
+  if (s.depth == 0) return;
+  for (int si = 1; si < a.N; ++si) {
+    const int vi = si - 1;
+    if (!isSet(s.views, vi)) continue;
+    float4 t = s.pl;
+    t.w = dist_to_origin(a.cam[0], px, py, s.depth, t);
+    float tc = ncc_strong(a, px, py, si, t, rw);
+    if (a.P.geom_consistency) tc += a.P.geom_factor * geom_cost(a, px, py, si, t);
+    const int w = vweight_at(s.vw, vi);
+    s.cost_now += tc * w;
+    s.weight_normal += w;
+    const float d0 = a.cam[0].c[0] - a.cam[si].c[0], d1 = a.cam[0].c[1] - a.cam[si].c[1], d2 = a.cam[0].c[2] - a.cam[si].c[2];
+    const double tv = d0 * d0 + d1 * d1 + d2 * d2;
+    s.base_line += sqrtf((float)tv);
+    s.valid++;
+  }
+}
+
+// DepthToWeak (DPE.cu:2597-2751)
+__global__ void __launch_bounds__(128) k_depth_to_weak(const __grid_constant__ PMArgs a, uint8_t *weak_out) {
+  int px, py;
+  if (!full_pixel(a, &px, &py)) return;
+  const int W = a.W, H = a.H, center = px + py * W, margin = 6;
+  if (px < margin || py < margin || px >= W - margin || py >= H - margin) { weak_out[center] = DPE_UNKNOWN; return; }
+  const dpe_camera &rc = a.cam[0];
+  RefWindow rw;
+  build_ref_window(a, px, py, rw);
+  Sweep s;
+  sweep_setup(a, px, py, rw, s);
+  if (s.depth == 0 || s.valid == 0) { weak_out[center] = DPE_UNKNOWN; return; }
+  s.cost_now /= s.weight_normal;
+  s.base_line /= s.valid;
+  const float disp = rc.K[0] * s.base_line / s.depth;
+  constexpr int R = 30, NS = 61;
+  float pc[NS];
+  for (int pd = -R; pd <= R; ++pd) {
+    const float pdep = rc.K[0] * s.base_line / (disp + pd);
+    if (pdep < a.P.depth_min || pdep > a.P.depth_max) { pc[pd + R] = 2.0f; continue; }
+    float4 t = s.pl;
+    t.w = dist_to_origin(rc, px, py, pdep, t);
+    float cost = 0.0f;
+    for (int si = 1; si < a.N; ++si) {
+      const int vi = si - 1;
+      if (isSet(s.views, vi)) {
+        float tc = ncc_strong(a, px, py, si, t, rw);
+        if (a.P.geom_consistency) tc += a.P.geom_factor * geom_cost(a, px, py, si, t);
+        cost += tc * vweight_at(s.vw, vi);
+      }
+    }
+    cost /= s.weight_normal;
+    pc[pd + R] = cvmin(2.0f, cost);
+  }
+  int peaks = 0, min_peak = 0;
+  float min_cost = 2.0f;
+  uint64_t peak_mask = 0;
+  for (int i = 2; i < NS - 2; ++i)
+    if (pc[i - 1] > pc[i] && pc[i + 1] > pc[i]) {
+      peak_mask |= 1ull << i; peaks++;
+      if (pc[i] < min_cost) { min_peak = i; min_cost = pc[i]; }
+    }
+  uint8_t res;
+  if (abs(min_peak - R) > a.P.weak_peak_radius || pc[min_peak] > 0.5f) res = DPE_WEAK;
+  else if (peaks == 1) res = pc[min_peak] <= 0.15f ? DPE_STRONG : DPE_WEAK;
+  else {
+    float var = 0.0f;
+    for (int i = 2; i < NS - 2; ++i)
+      if (((peak_mask >> i) & 1ull) && i != min_peak) { const float d = pc[i] - min_cost; var += d * d; }
+    var = sqrtf(var);
+    var /= (peaks - 1);
+    res = var > 0.2f ? DPE_STRONG : DPE_WEAK;
+  }
+  weak_out[center] = res;
+}
+
+// LocalRefine (DPE.cu:2753-2839)
+__global__ void __launch_bounds__(128) k_local_refine(const __grid_constant__ PMArgs a) {
+  int px, py;
+  if (!full_pixel(a, &px, &py)) return;
+  const int center = px + py * a.W;
+  const dpe_camera &rc = a.cam[0];
+  RefWindow rw;
+  build_ref_window(a, px, py, rw);
+  Sweep s;
+  sweep_setup(a, px, py, rw, s);
+  if (s.depth == 0) return;
+  if (s.weight_normal == 0 || s.valid == 0) return;
+  s.cost_now /= s.weight_normal;
+  s.base_line /= s.valid;
+  const float disp = rc.K[0] * s.base_line / s.depth;
+  float min_cost = 2.0f, best = s.depth;
+  for (int pd = -5; pd <= 5; ++pd) {
+    const float pdep = rc.K[0] * s.base_line / (disp + pd);
+    if (pdep < a.P.depth_min || pdep > a.P.depth_max) continue;
+    float4 t = s.pl;
+    t.w = dist_to_origin(rc, px, py, pdep, t);
+    float tc = 0.0f;
+    for (int si = 1; si < a.N; ++si) {
+      const int vi = si - 1;
+      if (isSet(s.views, vi)) {
+        const int w = vweight_at(s.vw, vi);
+        tc += ncc_strong(a, px, py, si, t, rw) * w;
+        if (a.P.geom_consistency) tc += a.P.geom_factor * geom_cost(a, px, py, si, t) * w;
+      }
+    }
+    tc /= s.weight_normal;
+    if (tc < min_cost) { min_cost = tc; best = pdep; }
+  }
+  if ((double)(s.cost_now - min_cost) > 0.1) a.plane[center].w = best;
+}
+
+}  // namespace dpe

@@ -1,0 +1,287 @@
+"""Python binding of the C ABI in include/dpe_b200.h (ctypes; no torch types cross the boundary).
+
+This is the host-side mirror of the reference's per-view interface (class DPE, DPE.h:140-243, and
+RunFusion, DPE.h:95-96) used by the tests and the bench.  The library is the in-tree
+libdpe_sm100.so; loading fails loudly when it is missing -- there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Dict, List, Optional, Sequence
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libdpe_sm100.so")
+
+MAX_IMAGES = 32
+NEIGHBOUR_NUM = 9
+OK, ERR_INVALID_ARGUMENT, ERR_CUDA, ERR_OUT_OF_MEMORY, ERR_CAPACITY, ERR_NO_DEVICE, ERR_DEVICE_TIMEOUT = range(7)
+WEAK, STRONG, UNKNOWN = 0, 1, 2
+FIRST_INIT, REFINE_INIT, REFINE_ITER = 0, 1, 2
+MEM_HOST, MEM_DEVICE = 0, 1
+FUSE_FP64, FUSE_FLOAT = 0, 1
+
+
+class Camera(C.Structure):
+    _fields_ = [("K", C.c_float * 9), ("R", C.c_float * 9), ("t", C.c_float * 3), ("c", C.c_float * 3),
+                ("height", C.c_int), ("width", C.c_int), ("depth_min", C.c_float), ("depth_max", C.c_float)]
+
+
+class Params(C.Structure):
+    _fields_ = [(n, t) for n, t in [
+        ("max_iterations", C.c_int), ("num_images", C.c_int), ("sigma_spatial", C.c_float),
+        ("sigma_color", C.c_float), ("top_k", C.c_int), ("depth_min", C.c_float), ("depth_max", C.c_float),
+        ("geom_consistency", C.c_int), ("strong_radius", C.c_int), ("strong_increment", C.c_int),
+        ("weak_radius", C.c_int), ("weak_increment", C.c_int), ("use_APD", C.c_int), ("use_edge", C.c_int),
+        ("use_limit", C.c_int), ("use_label", C.c_int), ("use_radius", C.c_int), ("high_res_img", C.c_int),
+        ("max_scale_size", C.c_int), ("scale_size", C.c_int), ("weak_peak_radius", C.c_int),
+        ("rotate_time", C.c_int), ("ransac_threshold", C.c_float), ("geom_factor", C.c_float), ("state", C.c_int)]]
+
+
+class Problem(C.Structure):
+    _fields_ = [("width", C.c_int), ("height", C.c_int), ("num_images", C.c_int),
+                ("images", C.c_void_p * MAX_IMAGES), ("cameras", Camera * MAX_IMAGES), ("params", Params),
+                ("plane_in", C.c_void_p), ("selected_views_in", C.c_void_p), ("weak_in", C.c_void_p),
+                ("edge", C.c_void_p), ("edge_low_res", C.c_void_p), ("low_width", C.c_int), ("low_height", C.c_int),
+                ("label", C.c_void_p), ("depths", C.c_void_p * MAX_IMAGES), ("seed", C.c_uint64), ("memory", C.c_int)]
+
+
+class PMOut(C.Structure):
+    _fields_ = [("plane", C.c_void_p), ("weak", C.c_void_p), ("selected_views", C.c_void_p), ("costs", C.c_void_p),
+                ("gpu_ms", C.c_float), ("strong_ncc_evals", C.c_uint64), ("weak_ncc_evals", C.c_uint64)]
+
+
+class FusionView(C.Structure):
+    _fields_ = [("width", C.c_int), ("height", C.c_int), ("depth", C.c_void_p), ("normal", C.c_void_p),
+                ("weak", C.c_void_p), ("bgr", C.c_void_p), ("block_mask", C.c_void_p), ("camera", Camera),
+                ("num_src", C.c_int), ("src_views", C.c_void_p)]
+
+
+class FusionIn(C.Structure):
+    _fields_ = [("num_views", C.c_int), ("views", C.POINTER(FusionView)), ("mode", C.c_int), ("memory", C.c_int)]
+
+
+class FusionOut(C.Structure):
+    _fields_ = [("capacity", C.c_int64), ("count", C.c_int64), ("xyz", C.c_void_p), ("bgr", C.c_void_p),
+                ("origin", C.c_void_p), ("num_consistent", C.c_void_p), ("gpu_ms", C.c_float)]
+
+
+class NCCQuery(C.Structure):
+    _fields_ = [("width", C.c_int), ("height", C.c_int), ("num_images", C.c_int),
+                ("images", C.c_void_p * MAX_IMAGES), ("cameras", Camera * MAX_IMAGES), ("params", Params),
+                ("count", C.c_int64), ("px", C.c_void_p), ("py", C.c_void_p), ("src", C.c_void_p), ("plane", C.c_void_p)]
+
+
+class Limits(C.Structure):
+    _fields_ = [("max_width", C.c_int), ("max_height", C.c_int), ("max_images", C.c_int)]
+
+
+EXPORTED = ["dpe_status_string", "dpe_params_default", "dpe_ctx_create", "dpe_ctx_destroy", "dpe_pm_run",
+            "dpe_fuse", "dpe_ncc_eval", "dpe_ctx_set_eval_counting"]
+
+_lib = None
+
+
+def load_library(path: Optional[str] = None) -> C.CDLL:
+    """Load libdpe_sm100.so (built by build.py).  Raises when it is missing: no fallback path."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise RuntimeError(f"{p} is missing: build it with `python dpe-mvs-fast_b200/build.py`")
+    lib = C.CDLL(p)
+    lib.dpe_status_string.restype = C.c_char_p
+    lib.dpe_status_string.argtypes = [C.c_int]
+    lib.dpe_params_default.argtypes = [C.POINTER(Params)]
+    lib.dpe_ctx_create.argtypes = [C.c_int, C.POINTER(Limits), C.POINTER(C.c_void_p)]
+    lib.dpe_ctx_destroy.argtypes = [C.c_void_p]
+    lib.dpe_pm_run.argtypes = [C.c_void_p, C.POINTER(Problem), C.POINTER(PMOut)]
+    lib.dpe_fuse.argtypes = [C.c_void_p, C.POINTER(FusionIn), C.POINTER(FusionOut)]
+    lib.dpe_ncc_eval.argtypes = [C.c_void_p, C.POINTER(NCCQuery), C.c_void_p]
+    lib.dpe_ctx_set_eval_counting.argtypes = [C.c_void_p, C.c_int]
+    if path is None:
+        _lib = lib
+    return lib
+
+
+class DPEError(RuntimeError):
+    def __init__(self, status: int, what: str):
+        lib = load_library()
+        super().__init__(f"{what}: {lib.dpe_status_string(status).decode()} (status {status})")
+        self.status = status
+
+
+def default_params(lib: Optional[C.CDLL] = None) -> Params:
+    p = Params()
+    (lib or load_library()).dpe_params_default(C.byref(p))
+    return p
+
+
+def make_camera(d: Dict) -> Camera:
+    cam = Camera()
+    for name in ("K", "R", "t", "c"):
+        arr = np.asarray(d[name], dtype=np.float32).reshape(-1)
+        getattr(cam, name)[:] = arr.tolist()
+    cam.height = int(d["height"])
+    cam.width = int(d["width"])
+    cam.depth_min = float(d["depth_min"])
+    cam.depth_max = float(d["depth_max"])
+    return cam
+
+
+def _ptr(x) -> Optional[int]:
+    """Raw address of a C-contiguous numpy array or a CUDA tensor (anything with data_ptr())."""
+    if x is None:
+        return None
+    if hasattr(x, "data_ptr"):
+        return int(x.data_ptr())
+    assert isinstance(x, np.ndarray) and x.flags["C_CONTIGUOUS"], "arrays must be C-contiguous"
+    return int(x.ctypes.data)
+
+
+def build_problem(images: Sequence, cameras: Sequence[Dict], params: Params, *, plane_in=None, views_in=None,
+                  weak_in=None, edge=None, edge_low=None, label=None, depths=None, seed: int = 0,
+                  memory: int = MEM_HOST) -> Problem:
+    n = len(images)
+    pr = Problem()
+    shape = images[0].shape
+    pr.height, pr.width = int(shape[0]), int(shape[1])
+    pr.num_images = n
+    for i in range(n):
+        pr.images[i] = _ptr(images[i])
+        pr.cameras[i] = make_camera(cameras[i])
+        if depths is not None:
+            pr.depths[i] = _ptr(depths[i])
+    pr.params = params
+    pr.params.num_images = n
+    pr.plane_in = _ptr(plane_in)
+    pr.selected_views_in = _ptr(views_in)
+    pr.weak_in = _ptr(weak_in)
+    pr.edge = _ptr(edge)
+    if edge_low is not None:
+        pr.edge_low_res = _ptr(edge_low)
+        pr.low_height, pr.low_width = int(edge_low.shape[0]), int(edge_low.shape[1])
+    pr.label = _ptr(label)
+    pr.seed = int(seed) & 0xFFFFFFFFFFFFFFFF
+    pr.memory = memory
+    return pr
+
+
+class Context:
+    """A dpe_ctx on one device."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load_library()
+        h = C.c_void_p()
+        st = self.lib.dpe_ctx_create(device, None, C.byref(h))
+        if st != OK:
+            raise DPEError(st, "dpe_ctx_create")
+        self.handle = h
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.dpe_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_eval_counting(self, on: bool):
+        self.lib.dpe_ctx_set_eval_counting(self.handle, 1 if on else 0)
+
+    # ------------------------------------------------------------------ PatchMatch
+    def pm_run(self, images, cameras, params: Params, *, out=None, want_costs=True, **kw) -> Dict:
+        """One per-view call on host arrays (memory=MEM_HOST) or device tensors (memory=MEM_DEVICE)."""
+        memory = kw.get("memory", MEM_HOST)
+        pr = build_problem(images, cameras, params, **kw)
+        H, W = pr.height, pr.width
+        if out is None:
+            assert memory == MEM_HOST, "device calls pass preallocated outputs"
+            out = dict(plane=np.zeros((H, W, 4), np.float32), weak=np.zeros((H, W), np.uint8),
+                       views=np.zeros((H, W), np.uint32), costs=np.zeros((H, W), np.float32) if want_costs else None)
+        po = PMOut()
+        po.plane = _ptr(out["plane"])
+        po.weak = _ptr(out["weak"])
+        po.selected_views = _ptr(out["views"])
+        po.costs = _ptr(out.get("costs"))
+        st = self.lib.dpe_pm_run(self.handle, C.byref(pr), C.byref(po))
+        if st != OK:
+            raise DPEError(st, "dpe_pm_run")
+        out["gpu_ms"] = po.gpu_ms
+        out["strong_ncc_evals"] = int(po.strong_ncc_evals)
+        out["weak_ncc_evals"] = int(po.weak_ncc_evals)
+        return out
+
+    # ------------------------------------------------------------------ fusion
+    def fuse(self, views: List[Dict], mode: int = FUSE_FP64, capacity: Optional[int] = None,
+             memory: int = MEM_HOST) -> Dict:
+        arr = (FusionView * len(views))()
+        keep = []
+        total = 0
+        for i, v in enumerate(views):
+            fv = arr[i]
+            H, W = v["depth"].shape[:2]
+            fv.width, fv.height = W, H
+            fv.depth = _ptr(v["depth"])
+            fv.normal = _ptr(v["normal"])
+            fv.weak = _ptr(v["weak"])
+            fv.bgr = _ptr(v["bgr"])
+            fv.block_mask = _ptr(v.get("block"))
+            fv.camera = make_camera(v["camera"])
+            src = np.ascontiguousarray(np.asarray(v["src"], dtype=np.int32))
+            keep.append(src)
+            fv.num_src = len(src)
+            fv.src_views = _ptr(src) if len(src) else None
+            total += W * H
+        cap = total if capacity is None else capacity
+        xyz = np.zeros((max(cap, 1), 3), np.float32)
+        bgr = np.zeros((max(cap, 1), 3), np.uint8)
+        origin = np.zeros((max(cap, 1), 2), np.int32)
+        ncons = np.zeros(max(cap, 1), np.uint8)
+        fin = FusionIn(len(views), arr, mode, memory)
+        fo = FusionOut()
+        fo.capacity = cap
+        fo.xyz, fo.bgr, fo.origin, fo.num_consistent = _ptr(xyz), _ptr(bgr), _ptr(origin), _ptr(ncons)
+        st = self.lib.dpe_fuse(self.handle, C.byref(fin), C.byref(fo))
+        if st != OK:
+            raise DPEError(st, "dpe_fuse")
+        n = int(fo.count)
+        return dict(count=n, xyz=xyz[:n], bgr=bgr[:n], origin=origin[:n], num_consistent=ncons[:n], gpu_ms=fo.gpu_ms)
+
+    # ------------------------------------------------------------------ NCC queries
+    def ncc_eval(self, images, cameras, params: Params, px, py, src, planes) -> np.ndarray:
+        q = make_query(images, cameras, params, px, py, src, planes)
+        out = np.zeros(len(q.keep[0]), np.float32)
+        st = self.lib.dpe_ncc_eval(self.handle, C.byref(q.struct), _ptr(out))
+        if st != OK:
+            raise DPEError(st, "dpe_ncc_eval")
+        return out
+
+
+class _Query:
+    def __init__(self, struct, keep):
+        self.struct = struct
+        self.keep = keep
+
+
+def make_query(images, cameras, params: Params, px, py, src, planes) -> _Query:
+    q = NCCQuery()
+    q.height, q.width = int(images[0].shape[0]), int(images[0].shape[1])
+    q.num_images = len(images)
+    for i, im in enumerate(images):
+        q.images[i] = _ptr(im)
+        q.cameras[i] = make_camera(cameras[i])
+    q.params = params
+    px = np.ascontiguousarray(px, dtype=np.int32)
+    py = np.ascontiguousarray(py, dtype=np.int32)
+    src = np.ascontiguousarray(src, dtype=np.int32)
+    planes = np.ascontiguousarray(planes, dtype=np.float32).reshape(-1, 4)
+    q.count = len(px)
+    q.px, q.py, q.src, q.plane = _ptr(px), _ptr(py), _ptr(src), _ptr(planes)
+    return _Query(q, [px, py, src, planes, images])

@@ -1,0 +1,212 @@
+/*
+ * dpe_b200.h -- C ABI of the B200-native DPE-MVS PatchMatch + fusion path.
+ *
+ * The reference exposes this path as a C++ class and a free function:
+ *   class DPE                    DPE.h:140-243 (setup: DPE.cpp:934-1252, kernels: DPE.cu:1-3262)
+ *   RunFusion(...)               DPE.h:95-96, DPE.cpp:1387-1548
+ * and its only caller is ProcessProblem / main (main.cpp:241-466).  Each entry point below
+ * names the reference interface it replaces.  All structs are plain C (no C++ or torch types),
+ * every call returns an int status (DPE_OK == 0) and never exits the process.
+ *
+ * Threading: one dpe_ctx per host thread.  Calls are stream-ordered on the context's stream and
+ * return after the work has completed.
+ */
+#ifndef DPE_B200_H_
+#define DPE_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DPE_MAX_IMAGES 32     /* main.h:42  MAX_IMAGES      */
+#define DPE_NEIGHBOUR_NUM 9   /* main.h:43  NEIGHBOUR_NUM   */
+
+/* ---- status codes (replace CudaSafeCall's exit(EXIT_FAILURE), DPE.cpp:646-679) ---- */
+enum {
+  DPE_OK = 0,
+  DPE_ERR_INVALID_ARGUMENT = 1,  /* null pointer, bad size, >32 images, bad enum ... */
+  DPE_ERR_CUDA = 2,              /* a CUDA runtime call failed                       */
+  DPE_ERR_OUT_OF_MEMORY = 3,     /* device allocation failed                         */
+  DPE_ERR_CAPACITY = 4,          /* caller-provided output buffer too small          */
+  DPE_ERR_NO_DEVICE = 5,         /* no CUDA device / wrong device index              */
+  DPE_ERR_DEVICE_TIMEOUT = 6     /* a bounded device-side wait gave up               */
+};
+
+/* pixel states, main.h:70-74 */
+enum { DPE_WEAK = 0, DPE_STRONG = 1, DPE_UNKNOWN = 2 };
+/* run states, main.h:64-68 */
+enum { DPE_FIRST_INIT = 0, DPE_REFINE_INIT = 1, DPE_REFINE_ITER = 2 };
+/* where the pointers of a problem live */
+enum { DPE_MEM_HOST = 0, DPE_MEM_DEVICE = 1 };
+/* fusion arithmetic for the consistency test */
+enum { DPE_FUSE_FP64 = 0, DPE_FUSE_FLOAT = 1 };
+
+/* Camera, byte-identical to the reference struct (main.h:53-62): K, R row-major 3x3, t, centre c
+ * (computed in double by ReadCamera, DPE.cpp:366-369), image size, depth range from the cam file. */
+typedef struct dpe_camera {
+  float K[9];
+  float R[9];
+  float t[3];
+  float c[3];
+  int height;
+  int width;
+  float depth_min;
+  float depth_max;
+} dpe_camera;
+
+/* PatchMatchParams (main.h:81-109) with the bools widened to int. */
+typedef struct dpe_params {
+  int max_iterations;
+  int num_images;
+  float sigma_spatial;
+  float sigma_color;
+  int top_k;
+  float depth_min;
+  float depth_max;
+  int geom_consistency;
+  int strong_radius;
+  int strong_increment;
+  int weak_radius;
+  int weak_increment;
+  int use_APD;
+  int use_edge;
+  int use_limit;
+  int use_label;
+  int use_radius;
+  int high_res_img;
+  int max_scale_size;
+  int scale_size;
+  int weak_peak_radius;
+  int rotate_time;
+  float ransac_threshold;
+  float geom_factor;
+  int state; /* DPE_FIRST_INIT / DPE_REFINE_INIT / DPE_REFINE_ITER */
+} dpe_params;
+
+/* One per-view PatchMatch call: the inputs DPE::InuputInitialization / SupportInitialization /
+ * CudaSpaceInitialization gather (DPE.cpp:934-1214).  All pointers are host or device memory
+ * according to `memory`.  Image 0 is the reference view, 1..num_images-1 the sources. */
+typedef struct dpe_problem {
+  int width;
+  int height;
+  int num_images;                       /* 2..32 */
+  const float *images[DPE_MAX_IMAGES];  /* gray float W*H row-major (SceneCache::GetGrayFloatImage) */
+  dpe_camera cameras[DPE_MAX_IMAGES];   /* K scaled to W,H (SceneCache::GetCamera, DPE.cpp:739-760) */
+  dpe_params params;                    /* depth_min/max already x0.6 / x1.2 (DPE.cpp:953-954) */
+  const float *plane_in;                /* float4 per pixel (world normal xyz, depth); REFINE_* only */
+  const uint32_t *selected_views_in;    /* per pixel view bitmask; NULL = zeros                  */
+  const uint8_t *weak_in;               /* per pixel state; read when use_APD, else all STRONG  */
+  const uint8_t *edge;                  /* W*H edge map (edges_<scale>.dmb); when use_edge||use_limit */
+  const uint8_t *edge_low_res;          /* low_width*low_height (edges_<max_scale>.dmb)          */
+  int low_width;
+  int low_height;
+  const int32_t *label;                 /* W*H labels (labels_<scale>.dmb); when use_label      */
+  const float *depths[DPE_MAX_IMAGES];  /* W*H depth maps of every image; when geom_consistency */
+  uint64_t seed;                        /* Philox key of this call's random streams             */
+  int memory;                           /* DPE_MEM_HOST or DPE_MEM_DEVICE                        */
+} dpe_problem;
+
+/* Outputs of one call (the three D2H copies of DPE.cu:3258-3260, plus optional costs).
+ * Caller-allocated, in the memory space named by dpe_problem.memory. */
+typedef struct dpe_pm_out {
+  float *plane;              /* float4 per pixel: world normal xyz, depth (after GetDepthandNormal) */
+  uint8_t *weak;             /* per pixel state after DepthToWeak                                   */
+  uint32_t *selected_views;  /* per pixel view bitmask                                              */
+  float *costs;              /* optional (may be NULL): final per-pixel cost                         */
+  float gpu_ms;              /* device time of the kernel sequence (DPE::GetLastGpuTimeMs)           */
+  uint64_t strong_ncc_evals; /* number of strong-window NCC evaluations (filled when counting on)   */
+  uint64_t weak_ncc_evals;   /* number of deformable (weak) NCC evaluations                          */
+} dpe_pm_out;
+
+/* ---- fusion (RunFusion, DPE.cpp:1387-1548) ---- */
+typedef struct dpe_fusion_view {
+  int width;
+  int height;
+  const float *depth;          /* W*H, <= 0 means no depth                             */
+  const float *normal;         /* W*H*3 world normals                                  */
+  const uint8_t *weak;         /* W*H pixel states                                     */
+  const uint8_t *bgr;          /* W*H*3 colour at depth resolution                     */
+  const uint8_t *block_mask;   /* optional W*H; pixels < 128 are skipped (blocks/)    */
+  dpe_camera camera;           /* camera at depth resolution                           */
+  int num_src;
+  const int *src_views;        /* host array of view indices (into the views array)   */
+} dpe_fusion_view;
+
+typedef struct dpe_fusion_in {
+  int num_views;
+  const dpe_fusion_view *views;  /* host array, in pair.txt order */
+  int mode;                      /* DPE_FUSE_FP64 or DPE_FUSE_FLOAT */
+  int memory;                    /* where depth/normal/weak/bgr/block_mask live */
+} dpe_fusion_in;
+
+typedef struct dpe_fusion_out {
+  int64_t capacity;      /* points the buffers below can hold                       */
+  int64_t count;         /* points produced (set even when capacity is too small)   */
+  float *xyz;            /* capacity*3, host memory                                  */
+  uint8_t *bgr;          /* capacity*3, host memory (PLY diffuse_blue/green/red)     */
+  int32_t *origin;       /* optional capacity*2: (view index, pixel index) per point */
+  uint8_t *num_consistent; /* optional capacity: consistent sources per point        */
+  float gpu_ms;
+} dpe_fusion_out;
+
+/* ---- NCC evaluation at explicit (pixel, plane, source) queries ---- */
+typedef struct dpe_ncc_query {
+  int width;
+  int height;
+  int num_images;
+  const float *images[DPE_MAX_IMAGES];  /* host memory */
+  dpe_camera cameras[DPE_MAX_IMAGES];
+  dpe_params params;                    /* strong_radius/increment, sigmas */
+  int64_t count;
+  const int32_t *px;      /* count pixel x */
+  const int32_t *py;      /* count pixel y */
+  const int32_t *src;     /* count source index 1..num_images-1 */
+  const float *plane;     /* count*4 plane in reference-camera coordinates (n, distance) */
+} dpe_ncc_query;
+
+/* ---- context ---- */
+typedef struct dpe_ctx dpe_ctx;
+
+typedef struct dpe_limits {
+  int max_width;      /* 0 = no preallocation */
+  int max_height;
+  int max_images;
+} dpe_limits;
+
+/* Human-readable text of a status code. */
+const char *dpe_status_string(int status);
+
+/* PatchMatchParams default member initialisers (main.h:81-109). */
+void dpe_params_default(dpe_params *params);
+
+/* Replaces the process-wide GpuWorkspace (DPE.cpp:775-837) and cudaSetDevice (main.cpp:343):
+ * a context owns the device arena, a stream and events on `device`. */
+int dpe_ctx_create(int device, const dpe_limits *limits, dpe_ctx **out);
+int dpe_ctx_destroy(dpe_ctx *ctx);
+
+/* Replaces DPE::CudaSpaceInitialization + SetDataPassHelperInCuda + RunPatchMatch and the
+ * getters GetPlaneHypothesis / GetPixelStates / GetSelectedViews / GetLastGpuTimeMs
+ * (DPE.cpp:1071-1288, DPE.cu:3130-3262) for one reference view. */
+int dpe_pm_run(dpe_ctx *ctx, const dpe_problem *problem, dpe_pm_out *out);
+
+/* Replaces the compute of RunFusion (DPE.cpp:1387-1548): returns the fused points in the
+ * reference order (view order, then raster order).  Writing the PLY stays with the caller
+ * (ExportPointCloud, DPE.cpp:532-572). */
+int dpe_fuse(dpe_ctx *ctx, const dpe_fusion_in *in, dpe_fusion_out *out);
+
+/* Strong bilateral NCC (ComputeBilateralNCCOld, DPE.cu:696-782) at explicit queries; test and
+ * measurement entry point. */
+int dpe_ncc_eval(dpe_ctx *ctx, const dpe_ncc_query *q, float *costs_out);
+
+/* Statistics switch: when on, dpe_pm_run counts its NCC evaluations into
+ * dpe_pm_out.strong_ncc_evals / weak_ncc_evals (device atomics; off by default).  The reference
+ * has no counterpart (it prints stage times only, main.cpp:17-45). */
+int dpe_ctx_set_eval_counting(dpe_ctx *ctx, int on);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DPE_B200_H_ */

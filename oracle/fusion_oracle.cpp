@@ -1,0 +1,147 @@
+// fusion_oracle.cpp -- CPU restatement of RunFusion (DPE.cpp:1387-1548), ETH variant.
+//
+// TEST INFRASTRUCTURE ONLY: the checker for the fusion kernels.  The loop order is the
+// reference's: views in pair.txt order, pixels in raster order, sources in list order, with the
+// consumed-pixel masks updated as points are accepted, so the result depends on that order
+// exactly as the reference's does.  Two arithmetic modes:
+//   DPE_FUSE_FP64  -- the reprojection / relative-depth / angle test and the score in double;
+//   DPE_FUSE_FLOAT -- the reference's float arithmetic (pow/sqrt of the reprojection error in
+//                     double as C++ promotes them, DPE.cpp:1504).
+// In both modes the emitted coordinates are the float back-projection of DPE.cpp:1337-1359 and
+// the colour is the float mean truncated to uchar (ExportPointCloud, DPE.cpp:549-551).
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "oracle_common.h"
+
+namespace oracle {
+
+// Get3DPointonWorld, DPE.cpp:1337-1359 (recomputes the centre from R, t in float)
+template <class T> static inline void world_point(T x, T y, T depth, const dpe_camera &c, T out[3]) {
+  const T px = depth * (x - (T)c.K[2]) / (T)c.K[0];
+  const T py = depth * (y - (T)c.K[5]) / (T)c.K[4];
+  const T pz = depth;
+  const T tx = (T)c.R[0] * px + (T)c.R[3] * py + (T)c.R[6] * pz;
+  const T ty = (T)c.R[1] * px + (T)c.R[4] * py + (T)c.R[7] * pz;
+  const T tz = (T)c.R[2] * px + (T)c.R[5] * py + (T)c.R[8] * pz;
+  const T Cx = -((T)c.R[0] * (T)c.t[0] + (T)c.R[3] * (T)c.t[1] + (T)c.R[6] * (T)c.t[2]);
+  const T Cy = -((T)c.R[1] * (T)c.t[0] + (T)c.R[4] * (T)c.t[1] + (T)c.R[7] * (T)c.t[2]);
+  const T Cz = -((T)c.R[2] * (T)c.t[0] + (T)c.R[5] * (T)c.t[1] + (T)c.R[8] * (T)c.t[2]);
+  out[0] = tx + Cx; out[1] = ty + Cy; out[2] = tz + Cz;
+}
+// ProjectCamera, DPE.cpp:1361-1371
+template <class T> static inline void project(const T X[3], const dpe_camera &c, T &u, T &v, T &depth) {
+  const T tx = (T)c.R[0] * X[0] + (T)c.R[1] * X[1] + (T)c.R[2] * X[2] + (T)c.t[0];
+  const T ty = (T)c.R[3] * X[0] + (T)c.R[4] * X[1] + (T)c.R[5] * X[2] + (T)c.t[1];
+  const T tz = (T)c.R[6] * X[0] + (T)c.R[7] * X[1] + (T)c.R[8] * X[2] + (T)c.t[2];
+  depth = (T)c.K[6] * tx + (T)c.K[7] * ty + (T)c.K[8] * tz;
+  u = ((T)c.K[0] * tx + (T)c.K[1] * ty + (T)c.K[2] * tz) / depth;
+  v = ((T)c.K[3] * tx + (T)c.K[4] * ty + (T)c.K[5] * tz) / depth;
+}
+
+}  // namespace oracle
+
+using namespace oracle;
+
+extern "C" int oracle_fuse(const dpe_fusion_in *in, dpe_fusion_out *out) {
+  if (!in || !out || in->memory != DPE_MEM_HOST) return DPE_ERR_INVALID_ARGUMENT;
+  const int nv = in->num_views;
+  std::vector<std::vector<uint8_t>> masks(nv);
+  for (int i = 0; i < nv; ++i) masks[i].assign((size_t)in->views[i].width * in->views[i].height, 0);
+  int64_t count = 0;
+  for (int i = 0; i < nv; ++i) {
+    const dpe_fusion_view &V = in->views[i];
+    const int cols = V.width, rows = V.height, ns = V.num_src;
+    std::vector<int> used_c(ns), used_r(ns);
+    for (int r = 0; r < rows; ++r)
+      for (int c = 0; c < cols; ++c) {
+        const size_t pix = (size_t)r * cols + c;
+        if (V.block_mask && V.block_mask[pix] < 128) continue;
+        if (masks[i][pix] == 1) continue;
+        const float ref_depth = V.depth[pix];
+        if (ref_depth <= 0.0) continue;
+        const float *rn = &V.normal[3 * pix];
+        float Xf[3];
+        world_point<float>((float)c, (float)r, ref_depth, V.camera, Xf);
+        double Xd[3];
+        world_point<double>((double)c, (double)r, (double)ref_depth, V.camera, Xd);
+        int n_cons = 0;
+        float dyn_f = 0.0f;
+        double dyn_d = 0.0;
+        for (int j = 0; j < ns; ++j) {
+          used_c[j] = -1; used_r[j] = -1;
+          const int s = V.src_views[j];
+          const dpe_fusion_view &S = in->views[s];
+          int src_r, src_c;
+          if (in->mode == DPE_FUSE_FP64) {
+            double u, v, pd;
+            project<double>(Xd, S.camera, u, v, pd);
+            src_r = f2i(v + 0.5); src_c = f2i(u + 0.5);
+          } else {
+            float u, v, pd;
+            project<float>(Xf, S.camera, u, v, pd);
+            src_r = f2i(v + 0.5f); src_c = f2i(u + 0.5f);
+          }
+          if (!(src_c >= 0 && src_c < S.width && src_r >= 0 && src_r < S.height)) continue;
+          const size_t sp = (size_t)src_r * S.width + src_c;
+          if (masks[s][sp] == 1) continue;
+          const float src_depth = S.depth[sp];
+          if (src_depth <= 0.0) continue;
+          const float *sn = &S.normal[3 * sp];
+          bool ok;
+          if (in->mode == DPE_FUSE_FP64) {
+            double T[3], u, v, pd;
+            world_point<double>((double)src_c, (double)src_r, (double)src_depth, S.camera, T);
+            project<double>(T, V.camera, u, v, pd);
+            const double ex = (double)c - u, ey = (double)r - v;
+            const double reproj = std::sqrt(ex * ex + ey * ey);
+            const double rel = std::fabs(pd - (double)ref_depth) / (double)ref_depth;
+            const double dot = (double)rn[0] * sn[0] + (double)rn[1] * sn[1] + (double)rn[2] * sn[2];
+            double ang = std::acos(dot);
+            if (ang != ang) ang = 0.0;
+            ok = reproj < 2.0 && rel < 0.01 && ang < (double)0.174533f;
+            if (ok) dyn_d += std::exp(-(reproj + 200.0 * rel + ang * 10.0));
+          } else {
+            float T[3], u, v, pd;
+            world_point<float>((float)src_c, (float)src_r, src_depth, S.camera, T);
+            project<float>(T, V.camera, u, v, pd);
+            const float ex = (float)c - u, ey = (float)r - v;
+            const float reproj = (float)std::sqrt((double)ex * (double)ex + (double)ey * (double)ey);
+            const float rel = std::fabs(pd - ref_depth) / ref_depth;
+            const float dot = rn[0] * sn[0] + rn[1] * sn[1] + rn[2] * sn[2];
+            float ang = std::acos(dot);
+            if (ang != ang) ang = 0.0f;
+            ok = reproj < 2.0f && rel < 0.01f && ang < 0.174533f;
+            if (ok) dyn_f += (float)std::exp(-(double)(reproj + 200 * rel + ang * 10));
+          }
+          if (ok) { used_c[j] = src_c; used_r[j] = src_r; n_cons++; }
+        }
+        const float factor = V.weak[pix] == DPE_WEAK ? 0.45f : 0.3f;
+        const bool accept = in->mode == DPE_FUSE_FP64 ? (n_cons >= 1 && dyn_d > (double)factor * n_cons)
+                                                      : (n_cons >= 1 && dyn_f > factor * n_cons);
+        if (!accept) continue;
+        const uint8_t *rc = &V.bgr[3 * pix];
+        float col[3] = {(float)rc[0], (float)rc[1], (float)rc[2]};
+        for (int j = 0; j < ns; ++j) {
+          if (used_c[j] == -1) continue;
+          const int s = V.src_views[j];
+          const size_t sp = (size_t)used_r[j] * in->views[s].width + used_c[j];
+          masks[s][sp] = 1;
+          const uint8_t *sc = &in->views[s].bgr[3 * sp];
+          col[0] += sc[0]; col[1] += sc[1]; col[2] += sc[2];
+        }
+        col[0] /= (n_cons + 1); col[1] /= (n_cons + 1); col[2] /= (n_cons + 1);
+        if (count < out->capacity) {
+          out->xyz[3 * count] = Xf[0]; out->xyz[3 * count + 1] = Xf[1]; out->xyz[3 * count + 2] = Xf[2];
+          out->bgr[3 * count] = (uint8_t)col[0]; out->bgr[3 * count + 1] = (uint8_t)col[1]; out->bgr[3 * count + 2] = (uint8_t)col[2];
+          if (out->origin) { out->origin[2 * count] = i; out->origin[2 * count + 1] = (int32_t)pix; }
+          if (out->num_consistent) out->num_consistent[count] = (uint8_t)n_cons;
+        }
+        count++;
+      }
+  }
+  out->count = count;
+  out->gpu_ms = 0.0f;
+  return count > out->capacity ? DPE_ERR_CAPACITY : DPE_OK;
+}
