@@ -12,6 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libdpe_sm100.so")
+LIB_CHECKED = os.path.join(HERE, "libdpe_sm100_checked.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2"]
 # per-source extra flags: fusion rounds like its CPU restatement (no FMA contraction)
@@ -33,18 +34,22 @@ def _deps() -> list:
     return files
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
+def build(force: bool = False, verbose: bool = False, checked: bool = False) -> str:
+    """Compile csrc/*.cu for sm_100a and link libdpe_sm100.so (checked=True: the bounds-checked
+    debug variant libdpe_sm100_checked.so, built with -DDPE_CHECKED)."""
     os.makedirs(OBJ, exist_ok=True)
+    lib = LIB_CHECKED if checked else LIB
     newest = max(os.path.getmtime(f) for f in _deps())
-    if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= newest:
-        return LIB
+    if not force and os.path.exists(lib) and os.path.getmtime(lib) >= newest:
+        return lib
     nvcc = _nvcc()
     procs = []
     objs = []
     for src, extra in UNITS.items():
-        obj = os.path.join(OBJ, src.replace(".cu", ".o"))
+        obj = os.path.join(OBJ, src.replace(".cu", "_checked.o" if checked else ".o"))
         objs.append(obj)
-        cmd = [nvcc, *ARCH, *COMMON, *extra, "-c", os.path.join(CSRC, src), "-o", obj]
+        flags = ["-DDPE_CHECKED"] if checked else []
+        cmd = [nvcc, *ARCH, *COMMON, *extra, *flags, "-c", os.path.join(CSRC, src), "-o", obj]
         if verbose:
             print(" ".join(cmd), flush=True)
         procs.append((cmd, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)))
@@ -52,11 +57,11 @@ def build(force: bool = False, verbose: bool = False) -> str:
         out, _ = p.communicate()
         if p.returncode != 0:
             raise RuntimeError(f"nvcc failed: {' '.join(cmd)}\n{out.decode(errors='replace')}")
-    link = [nvcc, *ARCH, "-shared", *objs, "-o", LIB + ".tmp", "-lcudart"]
+    link = [nvcc, *ARCH, "-shared", *objs, "-o", lib + ".tmp", "-lcudart"]
     subprocess.run(link, check=True, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)
-    os.replace(LIB + ".tmp", LIB)
-    return LIB
+    os.replace(lib + ".tmp", lib)
+    return lib
 
 
 if __name__ == "__main__":
-    print(build(force="--force" in sys.argv, verbose=True))
+    print(build(force="--force" in sys.argv, verbose=True, checked="--checked" in sys.argv))

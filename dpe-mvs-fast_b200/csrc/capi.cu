@@ -18,21 +18,6 @@ using namespace dpe;
 // ------------------------------------------------------------------ host helpers
 namespace {
 
-// Relative pose of source s with respect to the reference, with the float operation order of
-// ComputeHomography (DPE.cu:459-485).
-void relative_pose(const dpe_camera &rc, const dpe_camera &sc, float Rrel[9], float trel[3]) {
-  float rC[3], sC[3], Cr[3];
-  for (int k = 0; k < 3; ++k) {
-    rC[k] = -(rc.R[k] * rc.t[0] + rc.R[3 + k] * rc.t[1] + rc.R[6 + k] * rc.t[2]);
-    sC[k] = -(sc.R[k] * sc.t[0] + sc.R[3 + k] * sc.t[1] + sc.R[6 + k] * sc.t[2]);
-  }
-  for (int a = 0; a < 3; ++a)
-    for (int b = 0; b < 3; ++b)
-      Rrel[3 * a + b] = sc.R[3 * a] * rc.R[3 * b] + sc.R[3 * a + 1] * rc.R[3 * b + 1] + sc.R[3 * a + 2] * rc.R[3 * b + 2];
-  for (int k = 0; k < 3; ++k) Cr[k] = rC[k] - sC[k];
-  for (int a = 0; a < 3; ++a) trel[a] = sc.R[3 * a] * Cr[0] + sc.R[3 * a + 1] * Cr[1] + sc.R[3 * a + 2] * Cr[2];
-}
-
 int check_problem(const dpe_problem *p) {
   if (!p) return DPE_ERR_INVALID_ARGUMENT;
   if (p->width < 16 || p->height < 16 || p->width > 32767 || p->height > 32767) return DPE_ERR_INVALID_ARGUMENT;
@@ -57,6 +42,54 @@ int check_problem(const dpe_problem *p) {
 }
 
 }  // namespace
+
+// ------------------------------------------------------------------ error reporting
+namespace {
+thread_local std::string g_last_error;
+}
+
+void dpe_set_last_error(const char *what, cudaError_t err, const char *file, int line) {
+  char buf[512];
+  std::snprintf(buf, sizeof(buf), "%s failed: %s (%s) at %s:%d", what, cudaGetErrorName(err), cudaGetErrorString(err),
+                file, line);
+  g_last_error = buf;
+}
+
+bool dpe_debug_sync() {
+  static const bool on = [] {
+    const char *v = std::getenv("DPE_DEBUG_SYNC");
+    return v && v[0] && v[0] != '0';
+  }();
+  return on;
+}
+
+extern "C" const char *dpe_last_error(void) { return g_last_error.c_str(); }
+
+// In checked builds (-DDPE_CHECKED) every kernel is followed by a read of the out-of-range record.
+#ifdef DPE_CHECKED
+static int dpe_check_oob(const char *name, cudaStream_t s) {
+  long long o[4] = {0, 0, 0, 0};
+  if (cudaStreamSynchronize(s) != cudaSuccess || cudaMemcpyFromSymbol(o, dpe::g_oob, sizeof(o)) != cudaSuccess) {
+    cudaGetLastError();
+    return DPE_ERR_CUDA;
+  }
+  if (o[3] == 0) return DPE_OK;
+  char buf[256];
+  std::snprintf(buf, sizeof(buf), "%s: %lld out-of-range accesses, first at tag %lld index %lld bound %lld", name, o[3],
+                o[0], o[1], o[2]);
+  g_last_error = buf;
+  const long long z[4] = {0, 0, 0, 0};
+  cudaMemcpyToSymbol(dpe::g_oob, z, sizeof(z));
+  return DPE_ERR_CUDA;
+}
+#define PM_LAUNCHED(name, stream)                  \
+  do {                                             \
+    DPE_LAUNCHED(name, stream);                    \
+    if (dpe_check_oob(name, stream)) return DPE_ERR_CUDA; \
+  } while (0)
+#else
+#define PM_LAUNCHED(name, stream) DPE_LAUNCHED(name, stream)
+#endif
 
 // ------------------------------------------------------------------ context
 extern "C" const char *dpe_status_string(int s) {
@@ -269,9 +302,14 @@ extern "C" int dpe_pm_run(dpe_ctx *ctx, const dpe_problem *p, dpe_pm_out *out) {
   if (ctx->count_evals) DPE_TRY(cudaMemsetAsync(counters, 0, 16, s));
 
   // ---- kernel sequence (DPE.cu:3157-3234)
+  PM_LAUNCHED("k_pad_image", s);
+  PMArgs *d_args = A.get<PMArgs>("pm_args", 1);
+  if (!d_args) return DPE_ERR_OUT_OF_MEMORY;
+  DPE_TRY(cudaMemcpyAsync(d_args, &a, sizeof(PMArgs), cudaMemcpyHostToDevice, s));
   DPE_TRY(cudaEventRecord(ctx->ev0, s));
   const dim3 fg = full_grid(W, H), hg = half_grid(W, H);
-  k_init_state<<<fg, kFullBlock, 0, s>>>(a, plane_in, views_in, weak_in, weak_flag);
+  k_init_state<<<fg, kFullBlock, 0, s>>>(d_args, plane_in, views_in, weak_in, weak_flag);
+  PM_LAUNCHED("k_init_state", s);
   if (a.P.use_APD) {
     size_t tmp_bytes = 0;
     cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, weak_flag, a.nmap, (int)L, s);
@@ -281,28 +319,43 @@ extern "C" int dpe_pm_run(dpe_ctx *ctx, const dpe_problem *p, dpe_pm_out *out) {
   } else {
     DPE_TRY(cudaMemsetAsync(a.nmap, 0, L * 4, s));
   }
-  k_gen_edge_inform<<<fg, kFullBlock, 0, s>>>(a);
-  k_find_nearest_strong<<<fg, kFullBlock, 0, s>>>(a);
-  k_gen_neighbours<<<fg, kFullBlock, 0, s>>>(a);
-  k_neighbour_update<<<fg, kFullBlock, 0, s>>>(a);
-  k_random_init<<<fg, kFullBlock, 0, s>>>(a);
+  k_gen_edge_inform<<<fg, kFullBlock, 0, s>>>(d_args);
+  PM_LAUNCHED("k_gen_edge_inform", s);
+  k_find_nearest_strong<<<fg, kFullBlock, 0, s>>>(d_args);
+  PM_LAUNCHED("k_find_nearest_strong", s);
+  k_gen_neighbours<<<fg, kFullBlock, 0, s>>>(d_args);
+  PM_LAUNCHED("k_gen_neighbours", s);
+  k_neighbour_update<<<fg, kFullBlock, 0, s>>>(d_args);
+  PM_LAUNCHED("k_neighbour_update", s);
+  k_random_init<<<fg, kFullBlock, 0, s>>>(d_args);
+  PM_LAUNCHED("k_random_init", s);
   for (int it = 0; it < a.P.max_iterations; ++it) {
     for (int parity = 0; parity < 2; ++parity) {
       if (a.P.use_edge) {
         DPE_TRY(cudaMemcpyAsync(a.plane_snap, a.plane, L * sizeof(float4), cudaMemcpyDeviceToDevice, s));
         DPE_TRY(cudaMemcpyAsync(a.cost_snap, a.cost, L * 4, cudaMemcpyDeviceToDevice, s));
       }
-      k_strong_update<<<hg, kHalfBlock, 0, s>>>(a, it, parity);
+      k_strong_update<<<hg, kHalfBlock, 0, s>>>(d_args, it, parity);
+      PM_LAUNCHED("k_strong_update", s);
     }
-    k_ransac_fit_plane<<<fg, kFullBlock, 0, s>>>(a);
+    k_ransac_fit_plane<<<fg, kFullBlock, 0, s>>>(d_args);
+    PM_LAUNCHED("k_ransac_fit_plane", s);
     if (a.P.use_APD)
-      for (int parity = 0; parity < 2; ++parity) k_weak_update<<<hg, kHalfBlock, 0, s>>>(a, it, parity);
+      for (int parity = 0; parity < 2; ++parity) {
+        k_weak_update<<<hg, kHalfBlock, 0, s>>>(d_args, it, parity);
+        PM_LAUNCHED("k_weak_update", s);
+      }
   }
-  k_get_depth_normal<<<fg, kFullBlock, 0, s>>>(a);
-  for (int parity = 0; parity < 2; ++parity) k_filter_strong<<<hg, kHalfBlock, 0, s>>>(a, parity);
-  k_depth_to_weak<<<fg, kFullBlock, 0, s>>>(a, a.weak);
-  k_local_refine<<<fg, kFullBlock, 0, s>>>(a);
-  DPE_TRY(cudaGetLastError());
+  k_get_depth_normal<<<fg, kFullBlock, 0, s>>>(d_args);
+  PM_LAUNCHED("k_get_depth_normal", s);
+  for (int parity = 0; parity < 2; ++parity) {
+    k_filter_strong<<<hg, kHalfBlock, 0, s>>>(d_args, parity);
+    PM_LAUNCHED("k_filter_strong", s);
+  }
+  k_depth_to_weak<<<fg, kFullBlock, 0, s>>>(d_args, a.weak);
+  PM_LAUNCHED("k_depth_to_weak", s);
+  k_local_refine<<<fg, kFullBlock, 0, s>>>(d_args);
+  PM_LAUNCHED("k_local_refine", s);
   DPE_TRY(cudaEventRecord(ctx->ev1, s));
 
   // ---- outputs (DPE.cu:3258-3260)
@@ -324,8 +377,9 @@ extern "C" int dpe_pm_run(dpe_ctx *ctx, const dpe_problem *p, dpe_pm_out *out) {
 
 // ------------------------------------------------------------------ dpe_ncc_eval
 namespace {
-__global__ void k_ncc_queries(const __grid_constant__ PMArgs a, int64_t n, const int32_t *px, const int32_t *py,
+__global__ void k_ncc_queries(const PMArgs *__restrict__ pa, int64_t n, const int32_t *px, const int32_t *py,
                               const int32_t *src, const float4 *pl, float *out) {
+  const PMArgs &a = *pa;
   const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
   RefWindow rw;
@@ -365,13 +419,17 @@ extern "C" int dpe_ncc_eval(dpe_ctx *ctx, const dpe_ncc_query *q, float *costs_o
     DPE_TRY(cudaMemcpyAsync(stage + L * i, q->images[i], L * 4, cudaMemcpyHostToDevice, s));
     a.img[i] = img_pad + PL * i;
     k_pad_image<<<dim3((W + 2 + 31) / 32, (H + 2 + 7) / 8), dim3(32, 8), 0, s>>>(stage + L * i, img_pad + PL * i, W, H);
+    PM_LAUNCHED("k_pad_image", s);
   }
   DPE_TRY(cudaMemcpyAsync(dpx, q->px, n * 4, cudaMemcpyHostToDevice, s));
   DPE_TRY(cudaMemcpyAsync(dpy, q->py, n * 4, cudaMemcpyHostToDevice, s));
   DPE_TRY(cudaMemcpyAsync(dsrc, q->src, n * 4, cudaMemcpyHostToDevice, s));
   DPE_TRY(cudaMemcpyAsync(dpl, q->plane, n * 16, cudaMemcpyHostToDevice, s));
-  k_ncc_queries<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(a, n, dpx, dpy, dsrc, dpl, dout);
-  DPE_TRY(cudaGetLastError());
+  PMArgs *d_args = A.get<PMArgs>("pm_args", 1);
+  if (!d_args) return DPE_ERR_OUT_OF_MEMORY;
+  DPE_TRY(cudaMemcpyAsync(d_args, &a, sizeof(PMArgs), cudaMemcpyHostToDevice, s));
+  k_ncc_queries<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(d_args, n, dpx, dpy, dsrc, dpl, dout);
+  PM_LAUNCHED("k_ncc_queries", s);
   DPE_TRY(cudaMemcpyAsync(costs_out, dout, n * 4, cudaMemcpyDeviceToHost, s));
   DPE_TRY(cudaStreamSynchronize(s));
   return DPE_OK;

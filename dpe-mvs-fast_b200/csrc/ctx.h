@@ -8,6 +8,9 @@
 
 #include "../../include/dpe_b200.h"
 
+// Text of the last failure on this host thread (read through dpe_last_error()).
+void dpe_set_last_error(const char *what, cudaError_t err, const char *file, int line);
+
 // Return DPE_ERR_CUDA (or DPE_ERR_OUT_OF_MEMORY) from the enclosing ABI function when a CUDA call
 // fails; the reference exits the process instead (CudaSafeCall, DPE.cpp:646-679).
 #define DPE_TRY(call)                                                              \
@@ -15,7 +18,23 @@
     cudaError_t dpe_err_ = (call);                                                 \
     if (dpe_err_ != cudaSuccess) {                                                 \
       cudaGetLastError();                                                          \
+      dpe_set_last_error(#call, dpe_err_, __FILE__, __LINE__);                     \
       return dpe_err_ == cudaErrorMemoryAllocation ? DPE_ERR_OUT_OF_MEMORY : DPE_ERR_CUDA; \
+    }                                                                              \
+  } while (0)
+
+// After a kernel launch: report launch-configuration errors with the kernel's name; with
+// DPE_DEBUG_SYNC=1 in the environment also synchronise, so an execution error names its kernel
+// (the reference's DPE_POST_KERNEL, DPE.cu:3-7).
+bool dpe_debug_sync();
+#define DPE_LAUNCHED(name, stream)                                                 \
+  do {                                                                             \
+    cudaError_t dpe_err_ = cudaPeekAtLastError();                                  \
+    if (dpe_err_ == cudaSuccess && dpe_debug_sync()) dpe_err_ = cudaStreamSynchronize(stream); \
+    if (dpe_err_ != cudaSuccess) {                                                 \
+      cudaGetLastError();                                                          \
+      dpe_set_last_error(name, dpe_err_, __FILE__, __LINE__);                      \
+      return DPE_ERR_CUDA;                                                         \
     }                                                                              \
   } while (0)
 

@@ -18,7 +18,8 @@ constexpr int kMaxSrc = DPE_MAX_IMAGES - 1;
 constexpr int kNeighbours = DPE_NEIGHBOUR_NUM;
 constexpr int kMaxWin = 6;  // taps per window side for radius 5 / step 2 (DPE.cu:728-737)
 
-// All per-call read-only data, passed by value as a __grid_constant__ kernel parameter.
+// All per-call read-only data (cameras, relative poses, params, buffer pointers).  It lives in a
+// small device buffer written once per call; kernels receive its address.
 struct PMArgs {
   int W, H, N, lowW, lowH, pad_w;  // pad_w = W + 2 (images carry a 1-texel clamp border)
   dpe_params P;
@@ -51,6 +52,41 @@ struct PMArgs {
   short2 *nearest;
   unsigned long long *counters;  // [0] strong NCC evals, [1] weak NCC evals (stats builds)
 };
+
+// Relative pose of source s with respect to the reference, computed once per call on the host
+// with the float operation order of ComputeHomography (DPE.cu:459-485).
+inline void relative_pose(const dpe_camera &rc, const dpe_camera &sc, float Rrel[9], float trel[3]) {
+  float rC[3], sC[3], Cr[3];
+  for (int k = 0; k < 3; ++k) {
+    rC[k] = -(rc.R[k] * rc.t[0] + rc.R[3 + k] * rc.t[1] + rc.R[6 + k] * rc.t[2]);
+    sC[k] = -(sc.R[k] * sc.t[0] + sc.R[3 + k] * sc.t[1] + sc.R[6 + k] * sc.t[2]);
+  }
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b)
+      Rrel[3 * a + b] = sc.R[3 * a] * rc.R[3 * b] + sc.R[3 * a + 1] * rc.R[3 * b + 1] + sc.R[3 * a + 2] * rc.R[3 * b + 2];
+  for (int k = 0; k < 3; ++k) Cr[k] = rC[k] - sC[k];
+  for (int a = 0; a < 3; ++a) trel[a] = sc.R[3 * a] * Cr[0] + sc.R[3 * a + 1] * Cr[1] + sc.R[3 * a + 2] * Cr[2];
+}
+
+// ------------------------------------------------------------------ checked builds
+// With -DDPE_CHECKED every global access of the PatchMatch kernels goes through G(): an index
+// outside [0, n) is recorded in g_oob (first hit: tag, index, bound; plus a hit count) and
+// redirected to element 0, so a bad index is reported instead of faulting.
+#ifdef DPE_CHECKED
+__device__ long long g_oob[4];
+template <class T> __device__ __forceinline__ T *dpe_chk(T *base, long long idx, long long n, int tag) {
+  if (idx < 0 || idx >= n) {
+    if (atomicAdd((unsigned long long *)&g_oob[3], 1ull) == 0ull) {
+      g_oob[0] = tag; g_oob[1] = idx; g_oob[2] = n;
+    }
+    idx = 0;
+  }
+  return base + idx;
+}
+#define G(arr, idx, n, tag) (*::dpe::dpe_chk(&(arr)[0], (long long)(idx), (long long)(n), (tag)))
+#else
+#define G(arr, idx, n, tag) ((arr)[idx])
+#endif
 
 // ------------------------------------------------------------------ OpenCV MIN/MAX semantics
 template <class A, class B> __device__ __forceinline__ auto cvmin(A a, B b) -> decltype(a + b) { return a > b ? b : a; }
@@ -94,14 +130,21 @@ struct Rng {
   __device__ __forceinline__ float uniform() { return (float)((u32() >> 8) + 1u) * (1.0f / 16777216.0f); }
 };
 __device__ __forceinline__ Rng make_rng(const PMArgs &a, int center) {
-  return Rng{a.key[0], a.key[1], (uint32_t)center, a.rng_ctr[center]};
+  return Rng{a.key[0], a.key[1], (uint32_t)center, G(a.rng_ctr, center, (long long)a.W * a.H, 106)};
 }
 
 // ------------------------------------------------------------------ image access
+__device__ __forceinline__ float img_ld(const float *img, long long off, long long n, int tag) {
+#ifdef DPE_CHECKED
+  return *dpe_chk(img, off, n, tag);
+#else
+  return __ldg(img + off);
+#endif
+}
 __device__ __forceinline__ float texel(const PMArgs &a, int im, int x, int y) {
   x = min(max(x, 0), a.W - 1);
   y = min(max(y, 0), a.H - 1);
-  return __ldg(a.img[im] + (size_t)(y + 1) * a.pad_w + (x + 1));
+  return img_ld(a.img[im], (long long)(y + 1) * a.pad_w + (x + 1), (long long)a.pad_w * (a.H + 2), 101);
 }
 // tex2D(x+0.5, y+0.5) with linear filtering and clamp-to-edge addressing, exact FP32 weights.
 // The padded border makes the four reads branch-free for x0 in [-1, W-1].
@@ -110,8 +153,10 @@ __device__ __forceinline__ float bilinear(const float *__restrict__ img, int pad
   const float yc = fminf(fmaxf(y, -1.0f), (float)(H - 1));
   const float fx = floorf(xc), fy = floorf(yc);
   const float ax = xc - fx, ay = yc - fy;
-  const float *p = img + (size_t)((int)fy + 1) * pad_w + ((int)fx + 1);
-  const float v00 = __ldg(p), v10 = __ldg(p + 1), v01 = __ldg(p + pad_w), v11 = __ldg(p + pad_w + 1);
+  const long long o = (long long)((int)fy + 1) * pad_w + ((int)fx + 1);
+  const long long n = (long long)pad_w * (H + 2);
+  const float v00 = img_ld(img, o, n, 102), v10 = img_ld(img, o + 1, n, 103);
+  const float v01 = img_ld(img, o + pad_w, n, 104), v11 = img_ld(img, o + pad_w + 1, n, 105);
   const float top = (1.0f - ax) * v00 + ax * v10;
   const float bot = (1.0f - ax) * v01 + ax * v11;
   return (1.0f - ay) * top + ay * bot;
@@ -234,31 +279,36 @@ __device__ __forceinline__ float bilateral_weight(float dx, float dy, float pix,
 }
 
 // ------------------------------------------------------------------ strong NCC
+// The weighted moments are accumulated on intensities shifted by the window's reference centre
+// value c (r - c, s - c).  Variance and covariance are shift invariant, so the cost is the
+// reference's; the shift removes the cancellation of E[x^2] - E[x]^2 at mean ~128-200 that costs
+// FP32 about 1e-4 on low-contrast windows (the compensated form).
+
 // Hypothesis-invariant part of the strong window of one pixel: per tap the bilateral weight w and
-// w*r, plus the normalised reference moments.
+// w*(r - c), plus the normalised reference moments.
 struct RefWindow {
   float w[kMaxWin * kMaxWin];
   float wr[kMaxWin * kMaxWin];
-  float inv_wsum, mean_r, var_r;
-  int taps_side;
+  float center, inv_wsum, mean_r, var_r;
 };
 
 __device__ __forceinline__ void build_ref_window(const PMArgs &a, int px, int py, RefWindow &rw) {
   const int r = a.P.strong_radius, inc = a.P.strong_increment;
   const float center = texel(a, 0, px, py);
   float sw = 0.f, swr = 0.f, swrr = 0.f;
-  int k = 0, side = 0;
-  for (int i = -r; i <= r; i += inc, ++side) {
+  int k = 0;
+  for (int i = -r; i <= r; i += inc) {
     for (int j = -r; j <= r; j += inc) {
       const float rp = texel(a, 0, px + i, py + j);
       const float w = bilateral_weight((float)i, (float)j, rp, center, a.P.sigma_spatial, a.P.sigma_color);
+      const float rc = rp - center;
       rw.w[k] = w;
-      rw.wr[k] = w * rp;
-      sw += w; swr += w * rp; swrr += w * rp * rp;
+      rw.wr[k] = w * rc;
+      sw += w; swr += w * rc; swrr += w * rc * rc;
       ++k;
     }
   }
-  rw.taps_side = side;
+  rw.center = center;
   rw.inv_wsum = 1.0f / sw;
   rw.mean_r = swr * rw.inv_wsum;
   rw.var_r = swrr * rw.inv_wsum - rw.mean_r * rw.mean_r;
@@ -284,7 +334,7 @@ __device__ __forceinline__ float ncc_strong(const PMArgs &a, int px, int py, int
       const float y = (float)(py + j);
       const float X = H[1] * y + bx, Y = H[4] * y + by, Z = H[7] * y + bz;
       const float iz = 1.0f / Z;
-      const float sv = bilinear(img, a.pad_w, a.W, a.H, X * iz, Y * iz);
+      const float sv = bilinear(img, a.pad_w, a.W, a.H, X * iz, Y * iz) - rw.center;
       const float ws = rw.w[k] * sv;
       s_s += ws;
       s_ss += ws * sv;
@@ -299,7 +349,8 @@ __device__ __forceinline__ float ncc_strong(const PMArgs &a, int px, int py, int
   return fmaxf(0.0f, fminf(2.0f, 1.0f - cov / sqrtf(rw.var_r * var_s)));
 }
 
-// Window NCC with the window built on the fly (deformable weak window, DPE.cu:628-672).
+// Window NCC with the window built on the fly (deformable weak window, DPE.cu:628-672), with the
+// same compensated moments (shift by the reference centre value).
 __device__ __forceinline__ float window_ncc(const PMArgs &a, const float H[9], int s, int cx, int cy, int radius, int inc,
                                             float ref_center) {
   const float *__restrict__ img = a.img[s];
@@ -310,9 +361,10 @@ __device__ __forceinline__ float window_ncc(const PMArgs &a, const float H[9], i
       const int rx = cx + i, ry = cy + j;
       const float rp = texel(a, 0, rx, ry);
       const float2 sp = project(H, rx, ry);
-      const float sv = bilinear(img, a.pad_w, a.W, a.H, sp.x, sp.y);
+      const float sv = bilinear(img, a.pad_w, a.W, a.H, sp.x, sp.y) - ref_center;
       const float w = bilateral_weight((float)i, (float)j, rp, ref_center, a.P.sigma_spatial, a.P.sigma_color);
-      r_r += w * rp; r_rr += w * rp * rp; r_s += w * sv; r_ss += w * sv * sv; r_rs += w * rp * sv; r_w += w;
+      const float rc = rp - ref_center;
+      r_r += w * rc; r_rr += w * rc * rc; r_s += w * sv; r_ss += w * sv * sv; r_rs += w * rc * sv; r_w += w;
     }
     s_r += r_r; s_rr += r_rr; s_s += r_s; s_ss += r_ss; s_rs += r_rs; s_w += r_w;
   }

@@ -37,8 +37,9 @@ __global__ void k_pad_image(const float *__restrict__ src, float *__restrict__ d
   dst[(size_t)(y + 1) * (W + 2) + (x + 1)] = src[(size_t)sy * W + sx];
 }
 
-__global__ void k_init_state(const __grid_constant__ PMArgs a, const float4 *plane_in, const uint32_t *views_in,
+__global__ void k_init_state(const PMArgs *__restrict__ pa, const float4 *plane_in, const uint32_t *views_in,
                              const uint8_t *weak_in, int *weak_flag) {
+  const PMArgs &a = *pa;
   int px, py;
   if (!full_pixel(a, &px, &py)) return;
   const int c = px + py * a.W;
@@ -57,7 +58,8 @@ __global__ void k_init_state(const __grid_constant__ PMArgs a, const float4 *pla
 }
 
 // ------------------------------------------------------------------ GenEdgeInform (DPE.cu:2487-2595)
-__global__ void k_gen_edge_inform(const __grid_constant__ PMArgs a) {
+__global__ void k_gen_edge_inform(const PMArgs *__restrict__ pa) {
+  const PMArgs &a = *pa;
   int px, py;
   if (!full_pixel(a, &px, &py)) return;
   const int W = a.W, H = a.H, center = px + py * W;
@@ -107,7 +109,8 @@ __global__ void k_gen_edge_inform(const __grid_constant__ PMArgs a) {
 }
 
 // ------------------------------------------------------------------ FindNearestStrongPoint (DPE.cu:2859-2893)
-__global__ void k_find_nearest_strong(const __grid_constant__ PMArgs a) {
+__global__ void k_find_nearest_strong(const PMArgs *__restrict__ pa) {
+  const PMArgs &a = *pa;
   int px, py;
   if (!full_pixel(a, &px, &py)) return;
   const int W = a.W, H = a.H, center = px + py * W;
@@ -193,7 +196,8 @@ __device__ __forceinline__ void sort_small(float *d, int n) {
 }
 
 // ------------------------------------------------------------------ GenNeighbours (DPE.cu:2107-2467)
-__global__ void __launch_bounds__(128) k_gen_neighbours(const __grid_constant__ PMArgs a) {
+__global__ void __launch_bounds__(128) k_gen_neighbours(const PMArgs *__restrict__ pa) {
+  const PMArgs &a = *pa;
   int px, py;
   if (!full_pixel(a, &px, &py)) return;
   const int W = a.W, H = a.H, center = px + py * W;
@@ -429,7 +433,8 @@ __global__ void __launch_bounds__(128) k_gen_neighbours(const __grid_constant__ 
   a.reliable[center] = 1;
 }
 
-__global__ void k_neighbour_update(const __grid_constant__ PMArgs a) {
+__global__ void k_neighbour_update(const PMArgs *__restrict__ pa) {
+  const PMArgs &a = *pa;
   int px, py;
   if (!full_pixel(a, &px, &py)) return;
   const int c = px + py * a.W;
@@ -437,7 +442,8 @@ __global__ void k_neighbour_update(const __grid_constant__ PMArgs a) {
 }
 
 // ------------------------------------------------------------------ RandomInitialization (DPE.cu:1039-1067, 784-861)
-__global__ void __launch_bounds__(128) k_random_init(const __grid_constant__ PMArgs a) {
+__global__ void __launch_bounds__(128) k_random_init(const PMArgs *__restrict__ pa) {
+  const PMArgs &a = *pa;
   int px, py;
   if (!full_pixel(a, &px, &py)) return;
   const int center = px + py * a.W;
@@ -543,12 +549,14 @@ __device__ __forceinline__ int find_min_cost_index(const float *c, int n) {
 }
 
 // ------------------------------------------------------------------ strong update (DPE.cu:1218-1670, 1069-1122)
-__global__ void __launch_bounds__(128) k_strong_update(const __grid_constant__ PMArgs a, int iter, int parity) {
+__global__ void __launch_bounds__(128) k_strong_update(const PMArgs *__restrict__ pa, int iter, int parity) {
+  const PMArgs &a = *pa;
   int px, py;
   if (!colour_pixel(a, parity, &px, &py)) return;
   const int W = a.W, H = a.H, n = a.N - 1;
   const int center = py * W + px;
-  if (a.weak[center] == DPE_WEAK) return;
+  const long long L = (long long)W * H;
+  if (G(a.weak, center, L, 201) == DPE_WEAK) return;
   const dpe_camera &rc = a.cam[0];
   RefWindow rw;
   build_ref_window(a, px, py, rw);
@@ -562,10 +570,10 @@ __global__ void __launch_bounds__(128) k_strong_update(const __grid_constant__ P
   const float *cand_cost = a.P.use_edge ? a.cost_snap : a.cost;
 
   if (a.P.use_edge) {
-    const short2 *en = &a.edge_neigh[(size_t)center * 8];
+    const short2 *en = &G(a.edge_neigh, (long long)center * 8, L * 8, 202);
     const float max_edge_dist = cvmax(H, W) / 30.0f;
     const int min_step = 2;
-    const bool on_edge = a.edge[center] != 0;
+    const bool on_edge = G(a.edge, center, L, 203) != 0;
     for (int d = 0; d < 8; ++d) {
       const int dx = kDir[d][0], dy = kDir[d][1];
       const int sx = cvmax(1, 5 - 2 * iter) * dx, sy = cvmax(1, 5 - 2 * iter) * dy;
@@ -589,13 +597,13 @@ __global__ void __launch_bounds__(128) k_strong_update(const __grid_constant__ P
         const int tx = px + sx + s * step_len * dx + fx, ty = py + sy + s * step_len * dy + fy;
         if (!(tx >= 0 && ty >= 0 && tx < W && ty < H)) continue;
         const int tc = tx + ty * W;
-        const float cc = cand_cost[tc];
+        const float cc = G(cand_cost, tc, L, 204);
         if (mc > cc) { mp = tc; mc = cc; }
       }
       if (mc < FLT_MAX) {
         flag[d] = true;
         positions[d] = mp;
-        const float4 cp = cand_plane[mp];
+        const float4 cp = G(cand_plane, mp, L, 205);
         for (int j = 0; j < n; ++j) cost_array[d][j] = ncc_strong(a, px, py, j + 1, cp, rw);
       }
     }
@@ -613,13 +621,13 @@ __global__ void __launch_bounds__(128) k_strong_update(const __grid_constant__ P
           const int tx = px + sx + s * min_step * dx + fx, ty = py + sy + s * min_step * dy + fy;
           if (!(tx >= 0 && ty >= 0 && tx < W && ty < H)) continue;
           const int tc = tx + ty * W;
-          const float cc = cand_cost[tc];
+          const float cc = G(cand_cost, tc, L, 204);
           if (mc > cc) { mp = tc; mc = cc; }
         }
         if (mc < FLT_MAX) {
           flag[d] = true;
           float tca[kMaxSrc];
-          const float4 cp = cand_plane[mp];
+          const float4 cp = G(cand_plane, mp, L, 205);
           for (int j = 0; j < n; ++j) tca[j] = ncc_strong(a, px, py, j + 1, cp, rw);
           int g0 = 0, g1 = 0, b0 = 0, b1 = 0;
           for (int j = 0; j < n; ++j) {
@@ -644,7 +652,7 @@ __global__ void __launch_bounds__(128) k_strong_update(const __grid_constant__ P
       if (!oks[f]) continue;
       const int slot = 2 * f + 1;
       flag[slot] = true;
-      float m = a.cost[starts[f]];
+      float m = G(a.cost, starts[f], L, 206);
       int mp = starts[f];
       for (int i = 1; i < 11; ++i) {
         bool ok;
@@ -656,7 +664,7 @@ __global__ void __launch_bounds__(128) k_strong_update(const __grid_constant__ P
         }
         if (ok) {
           const int t = starts[f] + 2 * i * strides[f];
-          const float ct = a.cost[t];
+          const float ct = G(a.cost, t, L, 207);
           if (ct < m) { m = ct; mp = t; }
         }
       }
@@ -669,7 +677,7 @@ __global__ void __launch_bounds__(128) k_strong_update(const __grid_constant__ P
       if (!nok[f]) continue;
       const int slot = 2 * f;
       flag[slot] = true;
-      float m = a.cost[nbase[f]];
+      float m = G(a.cost, nbase[f], L, 208);
       int mp = nbase[f];
       for (int i = 0; i < 3; ++i)
         for (int side = 0; side < 2; ++side) {
@@ -683,7 +691,7 @@ __global__ void __launch_bounds__(128) k_strong_update(const __grid_constant__ P
             default: t = nbase[3] + k + (side ? k * W : -k * W); ok = px < W - 2 - i && (side ? py < H - 1 - i : py > i); break;
           }
           if (ok) {
-            const float ct = a.cost[t];
+            const float ct = G(a.cost, t, L, 209);
             if (ct < m) { m = ct; mp = t; }
           }
         }
@@ -691,7 +699,7 @@ __global__ void __launch_bounds__(128) k_strong_update(const __grid_constant__ P
     }
     for (int d = 0; d < 8; ++d) {
       if (!flag[d]) continue;
-      const float4 cp = a.plane[positions[d]];
+      const float4 cp = G(a.plane, positions[d], L, 210);
       for (int j = 0; j < n; ++j) cost_array[d][j] = ncc_strong(a, px, py, j + 1, cp, rw);
     }
   }
@@ -702,7 +710,7 @@ __global__ void __launch_bounds__(128) k_strong_update(const __grid_constant__ P
   const long nbr[4] = {(long)center - W, (long)center + W, (long)center - 1, (long)center + 1};
   for (int i = 0; i < 4; ++i)
     if (flag[2 * i]) {
-      const uint32_t sv = (nbr[i] >= 0 && nbr[i] < total) ? a.views[nbr[i]] : 0u;
+      const uint32_t sv = (nbr[i] >= 0 && nbr[i] < total) ? G(a.views, nbr[i], L, 211) : 0u;
       for (int j = 0; j < n; ++j) priors[j] += isSet(sv, j) == 1 ? 0.9f : 0.1f;
     }
   Rng rng = make_rng(a, center);
@@ -717,7 +725,7 @@ __global__ void __launch_bounds__(128) k_strong_update(const __grid_constant__ P
     final_costs[i] = fc / wn;
   }
   const int mi = find_min_cost_index(final_costs, 8);
-  const float4 pl_cur = a.plane[center];
+  const float4 pl_cur = G(a.plane, center, L, 212);
   float cost_now = 0.0f;
   for (int i = 0; i < n; ++i) {
     // views with no samples contribute 0 * cost, and every cost is finite
@@ -727,9 +735,9 @@ __global__ void __launch_bounds__(128) k_strong_update(const __grid_constant__ P
   const float cost_written = cost_now;
   float depth_now = depth_from_plane(rc, pl_cur, px, py);
   float4 pl_now = pl_cur;
-  uint32_t views_new = a.views[center];
+  uint32_t views_new = G(a.views, center, L, 213);
   if (flag[mi]) {
-    const float4 cand = cand_plane[positions[mi]];
+    const float4 cand = G(cand_plane, positions[mi], L, 214);
     const float db = depth_from_plane(rc, cand, px, py);
     if (db >= a.P.depth_min && db <= a.P.depth_max && final_costs[mi] < cost_now) {
       depth_now = db; pl_now = cand; cost_now = final_costs[mi];
@@ -757,20 +765,21 @@ __global__ void __launch_bounds__(128) k_strong_update(const __grid_constant__ P
       if (db >= dmin && db <= dmax && tc < cost_now) { depth_now = db; pl_now = t; cost_now = tc; }
     }
   }
-  a.rng_ctr[center] = rng.ctr;
-  a.views[center] = views_new;
-  store_vweight(&a.vweight[center], vw);
+  G(a.rng_ctr, center, L, 215) = rng.ctr;
+  G(a.views, center, L, 216) = views_new;
+  store_vweight(&G(a.vweight, center, L, 217), vw);
   if (a.P.state == DPE_REFINE_INIT) {
-    if ((double)cost_now < (double)cost_written - 0.1) { a.cost[center] = cost_now; a.plane[center] = pl_now; }
-    else a.cost[center] = cost_written;
+    if ((double)cost_now < (double)cost_written - 0.1) { G(a.cost, center, L, 218) = cost_now; G(a.plane, center, L, 219) = pl_now; }
+    else G(a.cost, center, L, 220) = cost_written;
   } else {
-    a.cost[center] = cost_now;
-    a.plane[center] = pl_now;
+    G(a.cost, center, L, 221) = cost_now;
+    G(a.plane, center, L, 222) = pl_now;
   }
 }
 
 // ------------------------------------------------------------------ RANSACToGetFitPlane (DPE.cu:2895-3128)
-__global__ void __launch_bounds__(128) k_ransac_fit_plane(const __grid_constant__ PMArgs a) {
+__global__ void __launch_bounds__(128) k_ransac_fit_plane(const PMArgs *__restrict__ pa) {
+  const PMArgs &a = *pa;
   int px, py;
   if (!full_pixel(a, &px, &py)) return;
   const int W = a.W, center = px + py * W;
@@ -913,7 +922,8 @@ __device__ __forceinline__ void cost_vector_weak(const PMArgs &a, int px, int py
   for (int i = 1; i < a.N; ++i) cv[i - 1] = ncc_weak(a, px, py, i, pl);
 }
 
-__global__ void __launch_bounds__(128) k_weak_update(const __grid_constant__ PMArgs a, int iter, int parity) {
+__global__ void __launch_bounds__(128) k_weak_update(const PMArgs *__restrict__ pa, int iter, int parity) {
+  const PMArgs &a = *pa;
   int px, py;
   if (!colour_pixel(a, parity, &px, &py)) return;
   const int W = a.W, n = a.N - 1;
@@ -980,11 +990,13 @@ __global__ void __launch_bounds__(128) k_weak_update(const __grid_constant__ PMA
       views_new = temp_sel;
     }
   }
-  // PlaneHypothesisRefinementWeak: the fitted plane, then five random hypotheses
+  // PlaneHypothesisRefinementWeak: the fitted plane, then five random hypotheses.  A zero fitted
+  // plane ends the refinement before the random hypotheses (DPE.cu:1146-1148).
   const float dmin = a.P.depth_min, dmax = a.P.depth_max;
-  {
-    const float4 fp = a.fit_plane[center];
-    if (!(fp.x == 0 && fp.y == 0 && fp.z == 0)) {
+  const float4 fp = a.fit_plane[center];
+  const bool refine = !(fp.x == 0 && fp.y == 0 && fp.z == 0);
+  if (refine) {
+    {
       float tc = 0.0f;
       for (int j = 0; j < n; ++j)
         if (vw[j] > 0) {
@@ -997,7 +1009,7 @@ __global__ void __launch_bounds__(128) k_weak_update(const __grid_constant__ PMA
       if (db >= dmin && db <= dmax && tc < cost_now) { depth_now = db; pl_now = fp; cost_now = tc; }
     }
   }
-  {
+  if (refine) {
     const float depth_rand = rng.uniform() * (dmax - dmin) + dmin;
     const float4 n_rand = random_normal(rc, px, py, rng, depth_now);
     const float lo = (1 - 0.02f) * depth_now, hi = (1 + 0.02f) * depth_now;
@@ -1040,7 +1052,8 @@ __global__ void __launch_bounds__(128) k_weak_update(const __grid_constant__ PMA
 }
 
 // ------------------------------------------------------------------ post passes
-__global__ void k_get_depth_normal(const __grid_constant__ PMArgs a) {
+__global__ void k_get_depth_normal(const PMArgs *__restrict__ pa) {
+  const PMArgs &a = *pa;
   int px, py;
   if (!full_pixel(a, &px, &py)) return;
   const int c = py * a.W + px;
@@ -1050,7 +1063,8 @@ __global__ void k_get_depth_normal(const __grid_constant__ PMArgs a) {
 }
 
 // CheckerboardFilterStrong (DPE.cu:1961-2071)
-__global__ void k_filter_strong(const __grid_constant__ PMArgs a, int parity) {
+__global__ void k_filter_strong(const PMArgs *__restrict__ pa, int parity) {
+  const PMArgs &a = *pa;
   int px, py;
   if (!colour_pixel(a, parity, &px, &py)) return;
   const int W = a.W, H = a.H, center = py * W + px;
@@ -1108,7 +1122,8 @@ __device__ __forceinline__ void sweep_setup(const PMArgs &a, int px, int py, con
 }
 
 // DepthToWeak (DPE.cu:2597-2751)
-__global__ void __launch_bounds__(128) k_depth_to_weak(const __grid_constant__ PMArgs a, uint8_t *weak_out) {
+__global__ void __launch_bounds__(128) k_depth_to_weak(const PMArgs *__restrict__ pa, uint8_t *weak_out) {
+  const PMArgs &a = *pa;
   int px, py;
   if (!full_pixel(a, &px, &py)) return;
   const int W = a.W, H = a.H, center = px + py * W, margin = 6;
@@ -1164,7 +1179,8 @@ __global__ void __launch_bounds__(128) k_depth_to_weak(const __grid_constant__ P
 }
 
 // LocalRefine (DPE.cu:2753-2839)
-__global__ void __launch_bounds__(128) k_local_refine(const __grid_constant__ PMArgs a) {
+__global__ void __launch_bounds__(128) k_local_refine(const PMArgs *__restrict__ pa) {
+  const PMArgs &a = *pa;
   int px, py;
   if (!full_pixel(a, &px, &py)) return;
   const int center = px + py * a.W;

@@ -13,7 +13,8 @@ from typing import Dict, List, Optional, Sequence
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libdpe_sm100.so")
+# DPE_LIBRARY selects another in-tree build (e.g. the bounds-checked libdpe_sm100_checked.so)
+LIB_PATH = os.path.join(HERE, os.environ.get("DPE_LIBRARY", "libdpe_sm100.so"))
 
 MAX_IMAGES = 32
 NEIGHBOUR_NUM = 9
@@ -78,7 +79,7 @@ class Limits(C.Structure):
     _fields_ = [("max_width", C.c_int), ("max_height", C.c_int), ("max_images", C.c_int)]
 
 
-EXPORTED = ["dpe_status_string", "dpe_params_default", "dpe_ctx_create", "dpe_ctx_destroy", "dpe_pm_run",
+EXPORTED = ["dpe_status_string", "dpe_last_error", "dpe_params_default", "dpe_ctx_create", "dpe_ctx_destroy", "dpe_pm_run",
             "dpe_fuse", "dpe_ncc_eval", "dpe_ctx_set_eval_counting"]
 
 _lib = None
@@ -95,6 +96,8 @@ def load_library(path: Optional[str] = None) -> C.CDLL:
     lib = C.CDLL(p)
     lib.dpe_status_string.restype = C.c_char_p
     lib.dpe_status_string.argtypes = [C.c_int]
+    lib.dpe_last_error.restype = C.c_char_p
+    lib.dpe_last_error.argtypes = []
     lib.dpe_params_default.argtypes = [C.POINTER(Params)]
     lib.dpe_ctx_create.argtypes = [C.c_int, C.POINTER(Limits), C.POINTER(C.c_void_p)]
     lib.dpe_ctx_destroy.argtypes = [C.c_void_p]
@@ -110,7 +113,8 @@ def load_library(path: Optional[str] = None) -> C.CDLL:
 class DPEError(RuntimeError):
     def __init__(self, status: int, what: str):
         lib = load_library()
-        super().__init__(f"{what}: {lib.dpe_status_string(status).decode()} (status {status})")
+        detail = lib.dpe_last_error().decode() if status in (ERR_CUDA, ERR_OUT_OF_MEMORY) else ""
+        super().__init__(f"{what}: {lib.dpe_status_string(status).decode()} (status {status}) {detail}".rstrip())
         self.status = status
 
 

@@ -179,6 +179,13 @@ typedef struct dpe_limits {
 /* Human-readable text of a status code. */
 const char *dpe_status_string(int status);
 
+/* Text of the last CUDA failure on the calling host thread (failing call or kernel, CUDA error
+ * name and message); empty when there was none.  Replaces CudaSafeCall's stderr message
+ * (DPE.cpp:646-679).  Setting DPE_DEBUG_SYNC=1 in the environment synchronises after every
+ * kernel so that an execution error names its kernel (the reference's DPE_DEBUG_SYNC build
+ * option, DPE.cu:3-7). */
+const char *dpe_last_error(void);
+
 /* PatchMatchParams default member initialisers (main.h:81-109). */
 void dpe_params_default(dpe_params *params);
 

@@ -38,8 +38,14 @@ def load() -> C.CDLL:
     lib.oracle_ncc_strong.argtypes = [C.POINTER(D.NCCQuery), C.c_int, C.c_void_p]
     lib.oracle_pm_run.argtypes = [C.POINTER(D.Problem), C.POINTER(D.PMOut), C.c_int]
     lib.oracle_fuse.argtypes = [C.POINTER(D.FusionIn), C.POINTER(D.FusionOut)]
+    lib.oracle_set_raw_moments.argtypes = [C.c_int]
     _lib = lib
     return lib
+
+
+def set_raw_moments(on: bool) -> None:
+    """Select the reference's raw-moment NCC arithmetic (default: compensated, shifted moments)."""
+    load().oracle_set_raw_moments(1 if on else 0)
 
 
 def philox(ctr, key) -> np.ndarray:

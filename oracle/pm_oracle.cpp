@@ -256,19 +256,28 @@ static inline float bilateral_weight(float dx, float dy, float pix, float center
   return std::exp(-spatial / (2.0f * ss * ss) - color / (2.0f * sc * sc));
 }
 
+// Moment form of the window NCC.  The reference accumulates raw moments (E[x^2] - E[x]^2,
+// DPE.cu:661-662); the default here accumulates on intensities shifted by the reference centre
+// value, which leaves variance and covariance unchanged mathematically but avoids FP32
+// cancellation (the compensated form the CUDA kernels use).  oracle_set_raw_moments(1) selects
+// the reference's raw form.
+static bool g_raw_moments = false;
+
 // Window moments of one NCC window (the shared core of DPE.cu:628-672 and :728-778).
 static float window_ncc(const Ctx &c, const float H[9], const Image &src, int cx, int cy, int radius, int inc,
                         float ref_center) {
   const Image &ref = c.img[0];
+  const float shift = g_raw_moments ? 0.0f : ref_center;
   float s_r = 0, s_rr = 0, s_s = 0, s_ss = 0, s_rs = 0, s_w = 0;
   for (int i = -radius; i <= radius; i += inc) {
     float r_r = 0, r_rr = 0, r_s = 0, r_ss = 0, r_rs = 0, r_w = 0;
     for (int j = -radius; j <= radius; j += inc) {
       const int rx = cx + i, ry = cy + j;
-      const float rp = ref.texel(rx, ry);
+      const float rp0 = ref.texel(rx, ry);
       const f2 sp = project(H, rx, ry);
-      const float sv = src.bilinear(sp.x, sp.y);
-      const float w = bilateral_weight((float)i, (float)j, rp, ref_center, c.P.sigma_spatial, c.P.sigma_color);
+      const float sv = src.bilinear(sp.x, sp.y) - shift;
+      const float w = bilateral_weight((float)i, (float)j, rp0, ref_center, c.P.sigma_spatial, c.P.sigma_color);
+      const float rp = rp0 - shift;
       r_r += w * rp; r_rr += w * rp * rp; r_s += w * sv; r_ss += w * sv * sv; r_rs += w * rp * sv; r_w += w;
     }
     s_r += r_r; s_rr += r_rr; s_s += r_s; s_ss += r_ss; s_rs += r_rs; s_w += r_w;
@@ -283,7 +292,12 @@ static float window_ncc(const Ctx &c, const float H[9], const Image &src, int cx
   return std::fmax(0.0f, std::fmin(2.0f, 1.0f - cov / vrs));
 }
 
-// ComputeBilateralNCCOld, DPE.cu:696-782
+// ComputeBilateralNCCOld, DPE.cu:696-782.
+// Evaluation order: the hypothesis-invariant reference half of the window (bilateral weights,
+// weighted reference moments) is summed first, tap by tap; each source tap is then projected
+// with the numerators affine in y along a window column.  This is the same mathematics as the
+// reference's per-row loop (and the same order as the CUDA kernels); g_raw_moments selects the
+// reference's own loop order and raw moments instead.
 static float ncc_strong(const Ctx &c, int px, int py, int src, const f4 &pl) {
   float H[9];
   homography(c.cam[0], c.cam[src], pl, H);
@@ -291,7 +305,46 @@ static float ncc_strong(const Ctx &c, int px, int py, int src, const f4 &pl) {
   const dpe_camera &sc = c.cam[src];
   if (pt.x >= sc.width || pt.x < 0.0f || pt.y >= sc.height || pt.y < 0.0f) return 2.0f;
   const float center = c.img[0].texel(px, py);
-  return window_ncc(c, H, c.img[src], px, py, c.P.strong_radius, c.P.strong_increment, center);
+  const int r = c.P.strong_radius, inc = c.P.strong_increment;
+  if (g_raw_moments) return window_ncc(c, H, c.img[src], px, py, r, inc, center);
+  float w[64], wr[64];
+  float sw = 0.f, swr = 0.f, swrr = 0.f;
+  int k = 0;
+  for (int i = -r; i <= r; i += inc)
+    for (int j = -r; j <= r; j += inc) {
+      const float rp = c.img[0].texel(px + i, py + j);
+      const float wt = bilateral_weight((float)i, (float)j, rp, center, c.P.sigma_spatial, c.P.sigma_color);
+      const float rc = rp - center;
+      w[k] = wt;
+      wr[k] = wt * rc;
+      sw += wt; swr += wt * rc; swrr += wt * rc * rc;
+      ++k;
+    }
+  const float inv = 1.0f / sw;
+  const float mean_r = swr * inv;
+  const float var_r = swrr * inv - mean_r * mean_r;
+  float s_s = 0.f, s_ss = 0.f, s_rs = 0.f;
+  k = 0;
+  for (int i = -r; i <= r; i += inc) {
+    const float x = (float)(px + i);
+    const float bx = H[0] * x + H[2], by = H[3] * x + H[5], bz = H[6] * x + H[8];
+    for (int j = -r; j <= r; j += inc) {
+      const float y = (float)(py + j);
+      const float X = H[1] * y + bx, Y = H[4] * y + by, Z = H[7] * y + bz;
+      const float iz = 1.0f / Z;
+      const float sv = c.img[src].bilinear(X * iz, Y * iz) - center;
+      const float ws = w[k] * sv;
+      s_s += ws;
+      s_ss += ws * sv;
+      s_rs += wr[k] * sv;
+      ++k;
+    }
+  }
+  const float m_s = s_s * inv;
+  const float var_s = s_ss * inv - m_s * m_s;
+  if (var_r < 1e-5f || var_s < 1e-5f) return 2.0f;
+  const float cov = s_rs * inv - mean_r * m_s;
+  return std::fmax(0.0f, std::fmin(2.0f, 1.0f - cov / std::sqrt(var_r * var_s)));
 }
 
 // ComputeBilateralNCCNew (deformable window), DPE.cu:561-694
@@ -1444,6 +1497,8 @@ using namespace oracle;
 extern "C" {
 
 void oracle_philox(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) { philox4x32_10(ctr, key, out); }
+
+void oracle_set_raw_moments(int on) { g_raw_moments = on != 0; }
 
 // Strong NCC at explicit queries.  fp64 != 0 evaluates the cost in double precision end to end
 // (homography from the float cameras, exact bilinear, double exp/sqrt).

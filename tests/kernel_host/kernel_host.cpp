@@ -1,0 +1,112 @@
+// kernel_host.cpp -- TEST INFRASTRUCTURE: the CUDA PatchMatch kernel source compiled for the host.
+//
+// Every kernel of dpe-mvs-fast_b200/csrc/pm_kernels.cuh is executed here thread by thread on the
+// CPU, in the launch order of dpe_pm_run, so that the kernels' logic can be compared with the
+// oracle without a GPU (bit for bit: both sides run IEEE float without contraction) and checked
+// under AddressSanitizer / UBSan.  The few device intrinsics the kernels use get host stand-ins.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+using std::max;
+using std::min;
+static dim3 blockIdx, threadIdx, blockDim;
+#define __global__
+#define __device__
+#define __host__
+#define __forceinline__ inline
+#define __launch_bounds__(x)
+#define __grid_constant__
+#define __constant__
+#define __restrict__
+static inline unsigned __umulhi(unsigned a, unsigned b) { return (unsigned)(((unsigned long long)a * b) >> 32); }
+template <class T> static inline T __ldg(const T *p) { return *p; }
+static inline unsigned long long atomicAdd(unsigned long long *p, unsigned long long v) {
+  const unsigned long long o = *p;
+  *p += v;
+  return o;
+}
+using std::isnan;
+#include "../../dpe-mvs-fast_b200/csrc/pm_kernels.cuh"
+using namespace dpe;
+
+template <class K, class... Args> static void launch(dim3 grid, dim3 block, K k, Args... args) {
+  blockDim = block;
+  for (unsigned by = 0; by < grid.y; ++by)
+    for (unsigned bx = 0; bx < grid.x; ++bx)
+      for (unsigned ty = 0; ty < block.y; ++ty)
+        for (unsigned tx = 0; tx < block.x; ++tx) {
+          blockIdx = dim3(bx, by, 1);
+          threadIdx = dim3(tx, ty, 1);
+          k(args...);
+        }
+}
+template <class T> static T *alloc(size_t n) { return (T *)calloc(n, sizeof(T)); }
+
+// The kernel sequence of dpe_pm_run (dpe-mvs-fast_b200/csrc/capi.cu), host memory only.
+extern "C" int host_pm_run(const dpe_problem *p, dpe_pm_out *out) {
+  const int W = p->width, H = p->height, N = p->num_images;
+  const size_t L = (size_t)W * H, PL = (size_t)(W + 2) * (H + 2);
+  PMArgs a;
+  memset(&a, 0, sizeof(a));
+  a.W = W; a.H = H; a.N = N; a.pad_w = W + 2;
+  a.P = p->params;
+  a.P.num_images = N;
+  for (int i = 0; i < N; ++i) a.cam[i] = p->cameras[i];
+  for (int i = 1; i < N; ++i) relative_pose(a.cam[0], a.cam[i], a.Rrel[i], a.trel[i]);
+  a.key[0] = (uint32_t)p->seed;
+  a.key[1] = (uint32_t)(p->seed >> 32);
+  std::vector<float *> imgs;
+  for (int i = 0; i < N; ++i) {
+    float *d = alloc<float>(PL);
+    launch(dim3((W + 2 + 31) / 32, (H + 2 + 7) / 8), dim3(32, 8), k_pad_image, p->images[i], d, W, H);
+    a.img[i] = d;
+    imgs.push_back(d);
+    if (a.P.geom_consistency) a.dep[i] = p->depths[i];
+  }
+  a.plane = alloc<float4>(L); a.plane_snap = alloc<float4>(L); a.fit_plane = alloc<float4>(L);
+  a.cost = alloc<float>(L); a.cost_snap = alloc<float>(L); a.complexity = alloc<float>(L);
+  a.views = alloc<uint32_t>(L); a.rng_ctr = alloc<uint32_t>(L); a.vweight = alloc<uint4>(L);
+  a.weak = alloc<uint8_t>(L); a.reliable = alloc<uint8_t>(L); a.nmap = alloc<int32_t>(L); a.radius = alloc<int32_t>(L);
+  int *weak_flag = alloc<int>(L);
+  a.neigh = alloc<short2>(L * kNeighbours); a.lab_bound = alloc<short2>(L * 8);
+  a.edge_neigh = alloc<short2>(L * 8); a.nearest = alloc<short2>(L);
+  a.lowW = p->low_width; a.lowH = p->low_height;
+  a.edge = p->edge; a.edge_low = p->edge_low_res; a.label = p->label;
+  const dim3 fg((W + 15) / 16, (H + 7) / 8), fb(16, 8), hg((W + 31) / 32, ((H + 1) / 2 + 3) / 4), hb(32, 4);
+  launch(fg, fb, k_init_state, &a, (const float4 *)p->plane_in, p->selected_views_in, p->weak_in, weak_flag);
+  int acc = 0;
+  for (size_t i = 0; i < L; ++i) { a.nmap[i] = acc; acc += weak_flag[i]; }
+  launch(fg, fb, k_gen_edge_inform, &a);
+  launch(fg, fb, k_find_nearest_strong, &a);
+  launch(fg, fb, k_gen_neighbours, &a);
+  launch(fg, fb, k_neighbour_update, &a);
+  launch(fg, fb, k_random_init, &a);
+  for (int it = 0; it < a.P.max_iterations; ++it) {
+    for (int parity = 0; parity < 2; ++parity) {
+      if (a.P.use_edge) { memcpy(a.plane_snap, a.plane, L * 16); memcpy(a.cost_snap, a.cost, L * 4); }
+      launch(hg, hb, k_strong_update, &a, it, parity);
+    }
+    launch(fg, fb, k_ransac_fit_plane, &a);
+    if (a.P.use_APD)
+      for (int parity = 0; parity < 2; ++parity) launch(hg, hb, k_weak_update, &a, it, parity);
+  }
+  launch(fg, fb, k_get_depth_normal, &a);
+  for (int parity = 0; parity < 2; ++parity) launch(hg, hb, k_filter_strong, &a, parity);
+  launch(fg, fb, k_depth_to_weak, &a, a.weak);
+  launch(fg, fb, k_local_refine, &a);
+  memcpy(out->plane, a.plane, L * 16);
+  memcpy(out->weak, a.weak, L);
+  memcpy(out->selected_views, a.views, L * 4);
+  if (out->costs) memcpy(out->costs, a.cost, L * 4);
+  for (float *d : imgs) free(d);
+  free(a.plane); free(a.plane_snap); free(a.fit_plane); free(a.cost); free(a.cost_snap); free(a.complexity);
+  free(a.views); free(a.rng_ctr); free(a.vweight); free(a.weak); free(a.reliable); free(a.nmap); free(a.radius);
+  free(weak_flag); free(a.neigh); free(a.lab_bound); free(a.edge_neigh); free(a.nearest);
+  return 0;
+}
