@@ -152,6 +152,14 @@ extern "C" int dpe_ctx_create(int device, const dpe_limits *limits, dpe_ctx **ou
     return DPE_ERR_CUDA;
   }
   (void)limits;
+  if (const char *v = std::getenv("DPE_STACK_LIMIT")) {
+    const long long bytes = std::atoll(v);
+    if (bytes > 0 && cudaDeviceSetLimit(cudaLimitStackSize, (size_t)bytes) != cudaSuccess) {
+      cudaGetLastError();
+      dpe_ctx_destroy(c);
+      return DPE_ERR_CUDA;
+    }
+  }
   *out = c;
   return DPE_OK;
 }
@@ -306,6 +314,24 @@ extern "C" int dpe_pm_run(dpe_ctx *ctx, const dpe_problem *p, dpe_pm_out *out) {
   PMArgs *d_args = A.get<PMArgs>("pm_args", 1);
   if (!d_args) return DPE_ERR_OUT_OF_MEMORY;
   DPE_TRY(cudaMemcpyAsync(d_args, &a, sizeof(PMArgs), cudaMemcpyHostToDevice, s));
+#ifdef DPE_CHECKED
+  {
+    long long *echo = A.get<long long>("echo", 8);
+    k_echo_args<<<1, 1, 0, s>>>(d_args, echo);
+    long long e[8];
+    DPE_TRY(cudaMemcpyAsync(e, echo, sizeof(e), cudaMemcpyDeviceToHost, s));
+    DPE_TRY(cudaStreamSynchronize(s));
+    const long long h[8] = {a.W, a.H, a.N, a.P.strong_radius, a.P.strong_increment, a.P.use_edge, a.P.num_images,
+                            (long long)sizeof(PMArgs)};
+    for (int i = 0; i < 8; ++i)
+      if (e[i] != h[i]) {
+        char buf[160];
+        std::snprintf(buf, sizeof(buf), "args echo mismatch at field %d: device %lld host %lld", i, e[i], h[i]);
+        g_last_error = buf;
+        return DPE_ERR_CUDA;
+      }
+  }
+#endif
   DPE_TRY(cudaEventRecord(ctx->ev0, s));
   const dim3 fg = full_grid(W, H), hg = half_grid(W, H);
   k_init_state<<<fg, kFullBlock, 0, s>>>(d_args, plane_in, views_in, weak_in, weak_flag);
@@ -432,6 +458,43 @@ extern "C" int dpe_ncc_eval(dpe_ctx *ctx, const dpe_ncc_query *q, float *costs_o
   PM_LAUNCHED("k_ncc_queries", s);
   DPE_TRY(cudaMemcpyAsync(costs_out, dout, n * 4, cudaMemcpyDeviceToHost, s));
   DPE_TRY(cudaStreamSynchronize(s));
+  return DPE_OK;
+}
+
+// Diagnostics: per-kernel attributes (registers, local memory per thread, max block size) and the
+// current per-thread stack limit, as text.  Reads attributes only; launches nothing.
+extern "C" int dpe_kernel_info(char *buf, int len) {
+  if (!buf || len <= 0) return DPE_ERR_INVALID_ARGUMENT;
+  std::string s;
+  auto add = [&](const char *name, const void *fn) {
+    cudaFuncAttributes at;
+    char line[256];
+    if (cudaFuncGetAttributes(&at, fn) != cudaSuccess) {
+      cudaGetLastError();
+      std::snprintf(line, sizeof(line), "%s: attributes unavailable\n", name);
+    } else {
+      std::snprintf(line, sizeof(line), "%s: regs %d local %zu B shared %zu B max_threads %d\n", name, at.numRegs,
+                    at.localSizeBytes, at.sharedSizeBytes, at.maxThreadsPerBlock);
+    }
+    s += line;
+  };
+  add("k_init_state", (const void *)k_init_state);
+  add("k_gen_edge_inform", (const void *)k_gen_edge_inform);
+  add("k_find_nearest_strong", (const void *)k_find_nearest_strong);
+  add("k_gen_neighbours", (const void *)k_gen_neighbours);
+  add("k_random_init", (const void *)k_random_init);
+  add("k_strong_update", (const void *)k_strong_update);
+  add("k_ransac_fit_plane", (const void *)k_ransac_fit_plane);
+  add("k_weak_update", (const void *)k_weak_update);
+  add("k_filter_strong", (const void *)k_filter_strong);
+  add("k_depth_to_weak", (const void *)k_depth_to_weak);
+  add("k_local_refine", (const void *)k_local_refine);
+  size_t stack = 0;
+  cudaDeviceGetLimit(&stack, cudaLimitStackSize);
+  char line[96];
+  std::snprintf(line, sizeof(line), "stack limit %zu B\n", stack);
+  s += line;
+  std::snprintf(buf, (size_t)len, "%s", s.c_str());
   return DPE_OK;
 }
 

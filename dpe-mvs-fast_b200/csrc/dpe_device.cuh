@@ -302,8 +302,8 @@ __device__ __forceinline__ void build_ref_window(const PMArgs &a, int px, int py
       const float rp = texel(a, 0, px + i, py + j);
       const float w = bilateral_weight((float)i, (float)j, rp, center, a.P.sigma_spatial, a.P.sigma_color);
       const float rc = rp - center;
-      rw.w[k] = w;
-      rw.wr[k] = w * rc;
+      G(rw.w, k, kMaxWin * kMaxWin, 320) = w;
+      G(rw.wr, k, kMaxWin * kMaxWin, 321) = w * rc;
       sw += w; swr += w * rc; swrr += w * rc * rc;
       ++k;
     }
@@ -335,10 +335,10 @@ __device__ __forceinline__ float ncc_strong(const PMArgs &a, int px, int py, int
       const float X = H[1] * y + bx, Y = H[4] * y + by, Z = H[7] * y + bz;
       const float iz = 1.0f / Z;
       const float sv = bilinear(img, a.pad_w, a.W, a.H, X * iz, Y * iz) - rw.center;
-      const float ws = rw.w[k] * sv;
+      const float ws = G(rw.w, k, kMaxWin * kMaxWin, 322) * sv;
       s_s += ws;
       s_ss += ws * sv;
-      s_rs += rw.wr[k] * sv;
+      s_rs += G(rw.wr, k, kMaxWin * kMaxWin, 323) * sv;
       ++k;
     }
   }
@@ -461,11 +461,18 @@ __device__ __forceinline__ float geom_cost(const PMArgs &a, int px, int py, int 
 }
 
 // ------------------------------------------------------------------ packed view weights
+// Inlined helpers declare no local arrays: the device compiler once gave such an array the stack
+// slot of a still-live array of the calling kernel (found with the DPE_CHECKED build).
 __device__ __forceinline__ void store_vweight(uint4 *dst, const uint8_t *vw) {
-  uint32_t w[4] = {0, 0, 0, 0};
+  uint32_t w0 = 0, w1 = 0, w2 = 0, w3 = 0;
 #pragma unroll
-  for (int i = 0; i < 32; ++i) w[i >> 3] |= (uint32_t)(vw[i] & 0xF) << (4 * (i & 7));
-  *dst = make_uint4(w[0], w[1], w[2], w[3]);
+  for (int i = 0; i < 8; ++i) {
+    w0 |= (uint32_t)(vw[i] & 0xF) << (4 * i);
+    w1 |= (uint32_t)(vw[8 + i] & 0xF) << (4 * i);
+    w2 |= (uint32_t)(vw[16 + i] & 0xF) << (4 * i);
+    w3 |= (uint32_t)(vw[24 + i] & 0xF) << (4 * i);
+  }
+  *dst = make_uint4(w0, w1, w2, w3);
 }
 __device__ __forceinline__ int vweight_at(const uint4 &p, int i) {
   const uint32_t w = (i >> 3) == 0 ? p.x : (i >> 3) == 1 ? p.y : (i >> 3) == 2 ? p.z : p.w;

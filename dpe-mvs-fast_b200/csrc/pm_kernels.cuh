@@ -29,6 +29,13 @@ __device__ __forceinline__ bool full_pixel(const PMArgs &a, int *px, int *py) {
 }
 
 // ------------------------------------------------------------------ setup
+#ifdef DPE_CHECKED
+// How the device reads the per-call block (checked builds compare it with the host's values).
+__global__ void k_echo_args(const PMArgs *__restrict__ pa, long long *out) {
+  out[0] = pa->W; out[1] = pa->H; out[2] = pa->N; out[3] = pa->P.strong_radius; out[4] = pa->P.strong_increment;
+  out[5] = pa->P.use_edge; out[6] = pa->P.num_images; out[7] = (long long)sizeof(PMArgs);
+}
+#endif
 __global__ void k_pad_image(const float *__restrict__ src, float *__restrict__ dst, int W, int H) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x - 1;
   const int y = blockIdx.y * blockDim.y + threadIdx.y - 1;
@@ -502,10 +509,9 @@ __global__ void __launch_bounds__(128) k_random_init(const PMArgs *__restrict__ 
 // ------------------------------------------------------------------ shared pieces of the propagation kernels
 // Multi-hypothesis joint view selection (DPE.cu:1551-1619 / 1714-1783).
 __device__ __forceinline__ float sample_views(const PMArgs &a, Rng &rng, int iter, const float (*cost_array)[kMaxSrc],
-                                              const float *priors, uint8_t *vw, uint32_t *temp_sel) {
+                                              const float *priors, uint8_t *vw, uint32_t *temp_sel, float *probs) {
   const int n = a.N - 1;
   for (int i = 0; i < 32; ++i) vw[i] = 0;
-  float probs[kMaxSrc];
   const float thr = (float)(0.8 * (double)expf((float)(iter * iter) / (-90.0f)));
   const float base = expf(thr * thr / (-0.32f));
   for (int i = 0; i < n; ++i) {
@@ -703,8 +709,12 @@ __global__ void __launch_bounds__(128) k_strong_update(const PMArgs *__restrict_
       for (int j = 0; j < n; ++j) cost_array[d][j] = ncc_strong(a, px, py, j + 1, cp, rw);
     }
   }
+#ifdef DPE_CHECKED
+  for (int d = 0; d < 8; ++d)
+    if (flag[d]) (void)G(a.plane, positions[d], L, 311 + d);
+#endif
 
-  float priors[kMaxSrc];
+  float priors[kMaxSrc], probs[kMaxSrc];
   for (int j = 0; j < n; ++j) priors[j] = 0.0f;
   const long total = (long)W * H;
   const long nbr[4] = {(long)center - W, (long)center + W, (long)center - 1, (long)center + 1};
@@ -713,10 +723,18 @@ __global__ void __launch_bounds__(128) k_strong_update(const PMArgs *__restrict_
       const uint32_t sv = (nbr[i] >= 0 && nbr[i] < total) ? G(a.views, nbr[i], L, 211) : 0u;
       for (int j = 0; j < n; ++j) priors[j] += isSet(sv, j) == 1 ? 0.9f : 0.1f;
     }
+#ifdef DPE_CHECKED
+  for (int d = 0; d < 8; ++d)
+    if (flag[d]) (void)G(a.plane, positions[d], L, 331 + d);
+#endif
   Rng rng = make_rng(a, center);
   uint8_t vw[32];
   uint32_t temp_sel = 0;
-  const float wn = sample_views(a, rng, iter, cost_array, priors, vw, &temp_sel);
+  const float wn = sample_views(a, rng, iter, cost_array, priors, vw, &temp_sel, probs);
+#ifdef DPE_CHECKED
+  for (int d = 0; d < 8; ++d)
+    if (flag[d]) (void)G(a.plane, positions[d], L, 341 + d);
+#endif
   float final_costs[8];
   for (int i = 0; i < 8; ++i) {
     float fc = 0.0f;
@@ -724,7 +742,16 @@ __global__ void __launch_bounds__(128) k_strong_update(const PMArgs *__restrict_
       if (vw[j] > 0) fc += vw[j] * cost_array[i][j];
     final_costs[i] = fc / wn;
   }
+#ifdef DPE_CHECKED
+  for (int d = 0; d < 8; ++d)
+    if (flag[d]) (void)G(a.plane, positions[d], L, 351 + d);
+#endif
   const int mi = find_min_cost_index(final_costs, 8);
+#ifdef DPE_CHECKED
+  (void)G(flag, mi, 8, 300);
+  for (int d = 0; d < 8; ++d)
+    if (flag[d]) (void)G(a.plane, positions[d], L, 301 + d);
+#endif
   const float4 pl_cur = G(a.plane, center, L, 212);
   float cost_now = 0.0f;
   for (int i = 0; i < n; ++i) {
@@ -947,7 +974,7 @@ __global__ void __launch_bounds__(128) k_weak_update(const PMArgs *__restrict__ 
     cand[i] = a.plane[nb.x + nb.y * W];
     cost_vector_weak(a, px, py, cand[i], cost_array[i]);
   }
-  float priors[kMaxSrc];
+  float priors[kMaxSrc], probs[kMaxSrc];
   for (int j = 0; j < n; ++j) priors[j] = 0.0f;
   for (int i = 0; i < 8; ++i) {
     const short2 nb = neighbour(a, center, i + 1);
@@ -958,7 +985,7 @@ __global__ void __launch_bounds__(128) k_weak_update(const PMArgs *__restrict__ 
   Rng rng = make_rng(a, center);
   uint8_t vw[32];
   uint32_t temp_sel = 0;
-  const float wn = sample_views(a, rng, iter, cost_array, priors, vw, &temp_sel);
+  const float wn = sample_views(a, rng, iter, cost_array, priors, vw, &temp_sel, probs);
   float final_costs[8];
   for (int i = 0; i < 8; ++i) {
     float fc = 0.0f;
