@@ -18,6 +18,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler",
 # per-source extra flags: fusion rounds like its CPU restatement (no FMA contraction)
 UNITS = {
     "capi.cu": [],
+    "scene.cu": [],
     "fusion.cu": ["-fmad=false"],
 }
 

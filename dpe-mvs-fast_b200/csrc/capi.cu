@@ -5,6 +5,8 @@
 // the process-wide GpuWorkspace, DPE.cpp:775-837), one stream and timing events.
 #include <cub/cub.cuh>
 
+#include <algorithm>
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -64,6 +66,12 @@ bool dpe_debug_sync() {
 }
 
 extern "C" const char *dpe_last_error(void) { return g_last_error.c_str(); }
+
+namespace {
+std::atomic<unsigned long long> g_launches{0};
+}
+void dpe_count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+extern "C" uint64_t dpe_launch_count(void) { return g_launches.load(); }
 
 // In checked builds (-DDPE_CHECKED) every kernel is followed by a read of the out-of-range record.
 #ifdef DPE_CHECKED
@@ -304,10 +312,10 @@ extern "C" int dpe_pm_run(dpe_ctx *ctx, const dpe_problem *p, dpe_pm_out *out) {
     a.img[i] = img_pad + PL * i;
     k_pad_image<<<dim3((W + 2 + 31) / 32, (H + 2 + 7) / 8), dim3(32, 8), 0, s>>>(src, img_pad + PL * i, W, H);
   }
-  unsigned long long *counters = A.get<unsigned long long>("counters", 2);
+  unsigned long long *counters = A.get<unsigned long long>("counters", 2 * KID_COUNT);
   if (!counters) return DPE_ERR_OUT_OF_MEMORY;
   a.counters = ctx->count_evals ? counters : nullptr;
-  if (ctx->count_evals) DPE_TRY(cudaMemsetAsync(counters, 0, 16, s));
+  if (ctx->count_evals) DPE_TRY(cudaMemsetAsync(counters, 0, 16 * KID_COUNT, s));
 
   // ---- kernel sequence (DPE.cu:3157-3234)
   PM_LAUNCHED("k_pad_image", s);
@@ -334,7 +342,7 @@ extern "C" int dpe_pm_run(dpe_ctx *ctx, const dpe_problem *p, dpe_pm_out *out) {
 #endif
   DPE_TRY(cudaEventRecord(ctx->ev0, s));
   const dim3 fg = full_grid(W, H), hg = half_grid(W, H);
-  k_init_state<<<fg, kFullBlock, 0, s>>>(d_args, plane_in, views_in, weak_in, weak_flag);
+  DPE_TIMED(ctx, KID_INIT_STATE, s, k_init_state<<<fg, kFullBlock, 0, s>>>(d_args, plane_in, views_in, weak_in, weak_flag));
   PM_LAUNCHED("k_init_state", s);
   if (a.P.use_APD) {
     size_t tmp_bytes = 0;
@@ -345,15 +353,15 @@ extern "C" int dpe_pm_run(dpe_ctx *ctx, const dpe_problem *p, dpe_pm_out *out) {
   } else {
     DPE_TRY(cudaMemsetAsync(a.nmap, 0, L * 4, s));
   }
-  k_gen_edge_inform<<<fg, kFullBlock, 0, s>>>(d_args);
+  DPE_TIMED(ctx, KID_GEN_EDGE_INFORM, s, k_gen_edge_inform<<<fg, kFullBlock, 0, s>>>(d_args));
   PM_LAUNCHED("k_gen_edge_inform", s);
-  k_find_nearest_strong<<<fg, kFullBlock, 0, s>>>(d_args);
+  DPE_TIMED(ctx, KID_FIND_NEAREST, s, k_find_nearest_strong<<<fg, kFullBlock, 0, s>>>(d_args));
   PM_LAUNCHED("k_find_nearest_strong", s);
-  k_gen_neighbours<<<fg, kFullBlock, 0, s>>>(d_args);
+  DPE_TIMED(ctx, KID_GEN_NEIGHBOURS, s, k_gen_neighbours<<<fg, kFullBlock, 0, s>>>(d_args));
   PM_LAUNCHED("k_gen_neighbours", s);
-  k_neighbour_update<<<fg, kFullBlock, 0, s>>>(d_args);
+  DPE_TIMED(ctx, KID_NEIGHBOUR_UPDATE, s, k_neighbour_update<<<fg, kFullBlock, 0, s>>>(d_args));
   PM_LAUNCHED("k_neighbour_update", s);
-  k_random_init<<<fg, kFullBlock, 0, s>>>(d_args);
+  DPE_TIMED(ctx, KID_RANDOM_INIT, s, k_random_init<<<fg, kFullBlock, 0, s>>>(d_args));
   PM_LAUNCHED("k_random_init", s);
   for (int it = 0; it < a.P.max_iterations; ++it) {
     for (int parity = 0; parity < 2; ++parity) {
@@ -361,26 +369,26 @@ extern "C" int dpe_pm_run(dpe_ctx *ctx, const dpe_problem *p, dpe_pm_out *out) {
         DPE_TRY(cudaMemcpyAsync(a.plane_snap, a.plane, L * sizeof(float4), cudaMemcpyDeviceToDevice, s));
         DPE_TRY(cudaMemcpyAsync(a.cost_snap, a.cost, L * 4, cudaMemcpyDeviceToDevice, s));
       }
-      k_strong_update<<<hg, kHalfBlock, 0, s>>>(d_args, it, parity);
+      DPE_TIMED(ctx, KID_STRONG_UPDATE, s, k_strong_update<<<hg, kHalfBlock, 0, s>>>(d_args, it, parity));
       PM_LAUNCHED("k_strong_update", s);
     }
-    k_ransac_fit_plane<<<fg, kFullBlock, 0, s>>>(d_args);
+    DPE_TIMED(ctx, KID_RANSAC, s, k_ransac_fit_plane<<<fg, kFullBlock, 0, s>>>(d_args));
     PM_LAUNCHED("k_ransac_fit_plane", s);
     if (a.P.use_APD)
       for (int parity = 0; parity < 2; ++parity) {
-        k_weak_update<<<hg, kHalfBlock, 0, s>>>(d_args, it, parity);
+        DPE_TIMED(ctx, KID_WEAK_UPDATE, s, k_weak_update<<<hg, kHalfBlock, 0, s>>>(d_args, it, parity));
         PM_LAUNCHED("k_weak_update", s);
       }
   }
-  k_get_depth_normal<<<fg, kFullBlock, 0, s>>>(d_args);
+  DPE_TIMED(ctx, KID_DEPTH_NORMAL, s, k_get_depth_normal<<<fg, kFullBlock, 0, s>>>(d_args));
   PM_LAUNCHED("k_get_depth_normal", s);
   for (int parity = 0; parity < 2; ++parity) {
-    k_filter_strong<<<hg, kHalfBlock, 0, s>>>(d_args, parity);
+    DPE_TIMED(ctx, KID_FILTER, s, k_filter_strong<<<hg, kHalfBlock, 0, s>>>(d_args, parity));
     PM_LAUNCHED("k_filter_strong", s);
   }
-  k_depth_to_weak<<<fg, kFullBlock, 0, s>>>(d_args, a.weak);
+  DPE_TIMED(ctx, KID_DEPTH_TO_WEAK, s, k_depth_to_weak<<<fg, kFullBlock, 0, s>>>(d_args, a.weak));
   PM_LAUNCHED("k_depth_to_weak", s);
-  k_local_refine<<<fg, kFullBlock, 0, s>>>(d_args);
+  DPE_TIMED(ctx, KID_LOCAL_REFINE, s, k_local_refine<<<fg, kFullBlock, 0, s>>>(d_args));
   PM_LAUNCHED("k_local_refine", s);
   DPE_TRY(cudaEventRecord(ctx->ev1, s));
 
@@ -390,14 +398,22 @@ extern "C" int dpe_pm_run(dpe_ctx *ctx, const dpe_problem *p, dpe_pm_out *out) {
   DPE_TRY(cudaMemcpyAsync(out->weak, a.weak, L, d2o, s));
   DPE_TRY(cudaMemcpyAsync(out->selected_views, a.views, L * 4, d2o, s));
   if (out->costs) DPE_TRY(cudaMemcpyAsync(out->costs, a.cost, L * 4, d2o, s));
-  unsigned long long cnt[2] = {0, 0};
-  if (ctx->count_evals) DPE_TRY(cudaMemcpyAsync(cnt, counters, 16, cudaMemcpyDeviceToHost, s));
+  unsigned long long cnt[2 * KID_COUNT] = {};
+  if (ctx->count_evals) DPE_TRY(cudaMemcpyAsync(cnt, counters, sizeof(cnt), cudaMemcpyDeviceToHost, s));
   DPE_TRY(cudaStreamSynchronize(s));
+  ctx->collect();
+  unsigned long long strong_total = 0, weak_total = 0;
+  for (int k = 0; k < KID_COUNT; ++k) {
+    ctx->kevals[k][0] += cnt[2 * k];
+    ctx->kevals[k][1] += cnt[2 * k + 1];
+    strong_total += cnt[2 * k];
+    weak_total += cnt[2 * k + 1];
+  }
   float ms = 0.f;
   DPE_TRY(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
   out->gpu_ms = ms;
-  out->strong_ncc_evals = cnt[0];
-  out->weak_ncc_evals = cnt[1];
+  out->strong_ncc_evals = strong_total;
+  out->weak_ncc_evals = weak_total;
   return DPE_OK;
 }
 
@@ -409,7 +425,7 @@ __global__ void k_ncc_queries(const PMArgs *__restrict__ pa, int64_t n, const in
   const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
   RefWindow rw;
-  build_ref_window(a, px[k], py[k], rw);
+  build_ref_window(a, px[k], py[k], rw, KID_NCC_QUERY);
   out[k] = ncc_strong(a, px[k], py[k], src[k], pl[k], rw);
 }
 }  // namespace
@@ -454,10 +470,11 @@ extern "C" int dpe_ncc_eval(dpe_ctx *ctx, const dpe_ncc_query *q, float *costs_o
   PMArgs *d_args = A.get<PMArgs>("pm_args", 1);
   if (!d_args) return DPE_ERR_OUT_OF_MEMORY;
   DPE_TRY(cudaMemcpyAsync(d_args, &a, sizeof(PMArgs), cudaMemcpyHostToDevice, s));
-  k_ncc_queries<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(d_args, n, dpx, dpy, dsrc, dpl, dout);
+  DPE_TIMED(ctx, KID_NCC_QUERY, s, k_ncc_queries<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(d_args, n, dpx, dpy, dsrc, dpl, dout));
   PM_LAUNCHED("k_ncc_queries", s);
   DPE_TRY(cudaMemcpyAsync(costs_out, dout, n * 4, cudaMemcpyDeviceToHost, s));
   DPE_TRY(cudaStreamSynchronize(s));
+  ctx->collect();
   return DPE_OK;
 }
 
@@ -495,6 +512,83 @@ extern "C" int dpe_kernel_info(char *buf, int len) {
   std::snprintf(line, sizeof(line), "stack limit %zu B\n", stack);
   s += line;
   std::snprintf(buf, (size_t)len, "%s", s.c_str());
+  return DPE_OK;
+}
+
+// ------------------------------------------------------------------ statistics
+extern "C" int dpe_ctx_set_profiling(dpe_ctx *ctx, int on) {
+  if (!ctx) return DPE_ERR_INVALID_ARGUMENT;
+  ctx->profile = on != 0;
+  return DPE_OK;
+}
+
+extern "C" int dpe_ctx_reset_kernel_stats(dpe_ctx *ctx) {
+  if (!ctx) return DPE_ERR_INVALID_ARGUMENT;
+  for (int k = 0; k < KID_COUNT; ++k) {
+    ctx->kms[k] = 0.0;
+    ctx->klaunch[k] = 0;
+    ctx->kevals[k][0] = ctx->kevals[k][1] = 0;
+  }
+  return DPE_OK;
+}
+
+extern "C" int dpe_ctx_get_kernel_stats(dpe_ctx *ctx, dpe_kernel_stat *out, int capacity, int *count) {
+  if (!ctx || !count || (capacity > 0 && !out)) return DPE_ERR_INVALID_ARGUMENT;
+  int n = 0;
+  for (int k = 0; k < KID_COUNT; ++k) {
+    if (ctx->klaunch[k] == 0 && ctx->kevals[k][0] == 0 && ctx->kevals[k][1] == 0) continue;
+    if (n < capacity) {
+      std::snprintf(out[n].name, sizeof(out[n].name), "%s", kKernelNames[k]);
+      out[n].launches = ctx->klaunch[k];
+      out[n].ms = ctx->kms[k];
+      out[n].strong_ncc_evals = ctx->kevals[k][0];
+      out[n].weak_ncc_evals = ctx->kevals[k][1];
+    }
+    ++n;
+  }
+  *count = n;
+  return n > capacity ? DPE_ERR_CAPACITY : DPE_OK;
+}
+
+namespace {
+// 8 independent FMA chains per thread; 2 FLOP per FMA.
+__global__ void k_fma_throughput(float *out, int iters, float a, float b) {
+  float x0 = threadIdx.x * 1e-3f, x1 = x0 + 1.f, x2 = x0 + 2.f, x3 = x0 + 3.f;
+  float x4 = x0 + 4.f, x5 = x0 + 5.f, x6 = x0 + 6.f, x7 = x0 + 7.f;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      x0 = fmaf(x0, a, b); x1 = fmaf(x1, a, b); x2 = fmaf(x2, a, b); x3 = fmaf(x3, a, b);
+      x4 = fmaf(x4, a, b); x5 = fmaf(x5, a, b); x6 = fmaf(x6, a, b); x7 = fmaf(x7, a, b);
+    }
+  }
+  const float r = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+  if (r == 1234.5f) out[blockIdx.x] = r;
+}
+}  // namespace
+
+extern "C" int dpe_fp32_peak(dpe_ctx *ctx, double *tflops) {
+  if (!ctx || !tflops) return DPE_ERR_INVALID_ARGUMENT;
+  DPE_TRY(cudaSetDevice(ctx->device));
+  cudaStream_t s = ctx->stream;
+  int sms = 0;
+  DPE_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+  float *out = ctx->arena.get<float>("fma_out", 4096);
+  if (!out) return DPE_ERR_OUT_OF_MEMORY;
+  const int blocks = sms * 8, threads = 256, iters = 4096;
+  double best = 0.0;
+  for (int rep = 0; rep < 4; ++rep) {
+    DPE_TRY(cudaEventRecord(ctx->ev0, s));
+    k_fma_throughput<<<blocks, threads, 0, s>>>(out, iters, 0.999f, 1e-3f);
+    DPE_LAUNCHED("k_fma_throughput", s);
+    DPE_TRY(cudaEventRecord(ctx->ev1, s));
+    DPE_TRY(cudaEventSynchronize(ctx->ev1));
+    float ms = 0.f;
+    DPE_TRY(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    const double flops = 2.0 * 32.0 * (double)iters * blocks * threads;
+    if (rep > 0) best = std::max(best, flops / (ms * 1e-3) / 1e12);
+  }
+  *tflops = best;
   return DPE_OK;
 }
 

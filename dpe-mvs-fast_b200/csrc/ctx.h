@@ -5,6 +5,7 @@
 
 #include <map>
 #include <string>
+#include <vector>
 
 #include "../../include/dpe_b200.h"
 
@@ -27,8 +28,10 @@ void dpe_set_last_error(const char *what, cudaError_t err, const char *file, int
 // DPE_DEBUG_SYNC=1 in the environment also synchronise, so an execution error names its kernel
 // (the reference's DPE_POST_KERNEL, DPE.cu:3-7).
 bool dpe_debug_sync();
+void dpe_count_launch();
 #define DPE_LAUNCHED(name, stream)                                                 \
   do {                                                                             \
+    dpe_count_launch();                                                            \
     cudaError_t dpe_err_ = cudaPeekAtLastError();                                  \
     if (dpe_err_ == cudaSuccess && dpe_debug_sync()) dpe_err_ = cudaStreamSynchronize(stream); \
     if (dpe_err_ != cudaSuccess) {                                                 \
@@ -82,10 +85,61 @@ class Arena {
   size_t reserved_ = 0;
 };
 
+#include "kernel_ids.h"
+
 struct dpe_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   bool count_evals = false;
+  bool profile = false;
   Arena arena;
+  // per-kernel statistics since the last reset
+  double kms[KID_COUNT] = {};
+  long long klaunch[KID_COUNT] = {};
+  unsigned long long kevals[KID_COUNT][2] = {};
+  struct Pending { int kid; cudaEvent_t a, b; };
+  std::vector<Pending> pending;
+  std::vector<cudaEvent_t> pool;
+  cudaEvent_t event() {
+    if (pool.empty()) {
+      cudaEvent_t e = nullptr;
+      cudaEventCreate(&e);
+      return e;
+    }
+    cudaEvent_t e = pool.back();
+    pool.pop_back();
+    return e;
+  }
+  // after the stream has been synchronised: fold the recorded launch times into kms/klaunch
+  void collect() {
+    for (const Pending &p : pending) {
+      float ms = 0.f;
+      if (cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) {
+        kms[p.kid] += ms;
+        klaunch[p.kid] += 1;
+      } else {
+        cudaGetLastError();
+      }
+      pool.push_back(p.a);
+      pool.push_back(p.b);
+    }
+    pending.clear();
+  }
 };
+
+// Launch with per-kernel timing when ctx->profile is on (event pair around the launch).
+#define DPE_TIMED(ctx, kid, stream, ...)                            \
+  do {                                                              \
+    cudaEvent_t t0_ = nullptr, t1_ = nullptr;                       \
+    if ((ctx)->profile) {                                           \
+      t0_ = (ctx)->event();                                         \
+      t1_ = (ctx)->event();                                         \
+      cudaEventRecord(t0_, stream);                                 \
+    }                                                               \
+    __VA_ARGS__;                                                    \
+    if ((ctx)->profile) {                                           \
+      cudaEventRecord(t1_, stream);                                 \
+      (ctx)->pending.push_back(dpe_ctx::Pending{kid, t0_, t1_});    \
+    }                                                               \
+  } while (0)

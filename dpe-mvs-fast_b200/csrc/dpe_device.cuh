@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/dpe_b200.h"
+#include "kernel_ids.h"
 
 namespace dpe {
 
@@ -50,7 +51,7 @@ struct PMArgs {
   short2 *lab_bound;
   short2 *edge_neigh;
   short2 *nearest;
-  unsigned long long *counters;  // [0] strong NCC evals, [1] weak NCC evals (stats builds)
+  unsigned long long *counters;  // per kernel class: [2k] strong NCC evals, [2k+1] weak (counting runs)
 };
 
 // Relative pose of source s with respect to the reference, computed once per call on the host
@@ -290,9 +291,11 @@ struct RefWindow {
   float w[kMaxWin * kMaxWin];
   float wr[kMaxWin * kMaxWin];
   float center, inv_wsum, mean_r, var_r;
+  unsigned long long *cnt;  // this kernel's strong-evaluation counter (counting runs only)
 };
 
-__device__ __forceinline__ void build_ref_window(const PMArgs &a, int px, int py, RefWindow &rw) {
+__device__ __forceinline__ void build_ref_window(const PMArgs &a, int px, int py, RefWindow &rw, int kid) {
+  rw.cnt = a.counters ? a.counters + 2 * kid : nullptr;
   const int r = a.P.strong_radius, inc = a.P.strong_increment;
   const float center = texel(a, 0, px, py);
   float sw = 0.f, swr = 0.f, swrr = 0.f;
@@ -321,7 +324,7 @@ __device__ __forceinline__ float ncc_strong(const PMArgs &a, int px, int py, int
   const float2 pt = project(H, px, py);
   const dpe_camera &sc = a.cam[s];
   if (pt.x >= sc.width || pt.x < 0.0f || pt.y >= sc.height || pt.y < 0.0f) return 2.0f;
-  if (a.counters) atomicAdd(&a.counters[0], 1ull);
+  if (rw.cnt) atomicAdd(rw.cnt, 1ull);
   const int r = a.P.strong_radius, inc = a.P.strong_increment;
   const float *__restrict__ img = a.img[s];
   float s_s = 0.f, s_ss = 0.f, s_rs = 0.f;
@@ -388,7 +391,7 @@ __device__ __forceinline__ float ncc_weak(const PMArgs &a, int px, int py, int s
   const float2 pt = project(H, px, py);
   const dpe_camera &sc = a.cam[s];
   if (pt.x >= sc.width || pt.x < 0.0f || pt.y >= sc.height || pt.y < 0.0f) return 2.0f;
-  if (a.counters) atomicAdd(&a.counters[1], 1ull);
+  if (a.counters) atomicAdd(&a.counters[2 * KID_WEAK_UPDATE + 1], 1ull);
   const int center = px + py * a.W;
   const float ref_center = texel(a, 0, px, py);
   float center_cost = 0.0f, strong_cost = 0.0f;

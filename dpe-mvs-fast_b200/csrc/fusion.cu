@@ -41,6 +41,7 @@ constexpr int kMaxSrc = 32;
 
 struct FuseArgs {
   int mode;
+  int min_consistent;
   int ref;
   int ns;
   int src[kMaxSrc];
@@ -172,7 +173,8 @@ __global__ void k_decide(const __grid_constant__ FuseArgs f, int npix) {
     dyn_f += (float)es[j];
   }
   const float factor = V.weak[pix] == DPE_WEAK ? 0.45f : 0.3f;
-  const bool accept = f.mode == DPE_FUSE_FP64 ? (n >= 1 && dyn_d > (double)factor * n) : (n >= 1 && dyn_f > factor * n);
+  const int need = f.min_consistent > 1 ? f.min_consistent : 1;
+  const bool accept = f.mode == DPE_FUSE_FP64 ? (n >= need && dyn_d > (double)factor * n) : (n >= need && dyn_f > factor * n);
   f.status[pix] = accept ? 1 : 2;
   if (accept)
     for (int j = 0; j < f.ns; ++j)
@@ -302,6 +304,7 @@ extern "C" int dpe_fuse(dpe_ctx *ctx, const dpe_fusion_in *in, dpe_fusion_out *o
   FuseArgs f;
   std::memset(&f, 0, sizeof(f));
   f.mode = in->mode;
+  f.min_consistent = in->min_consistent;
   f.views = d_views;
   f.entry_q = entry_q;
   f.entry_score = entry_s;
@@ -319,7 +322,8 @@ extern "C" int dpe_fuse(dpe_ctx *ctx, const dpe_fusion_in *in, dpe_fusion_out *o
       DPE_TRY(cudaMemsetAsync(S.acc_min, 0x7F, (size_t)S.W * S.H * 4, s));
     }
     if (v.num_src > 0) {
-      k_entries<<<blocks, 256, 0, s>>>(f);
+      DPE_TIMED(ctx, KID_FUSE_ENTRIES, s, k_entries<<<blocks, 256, 0, s>>>(f));
+      DPE_LAUNCHED("k_entries", s);
       // waves until every candidate pixel is decided; each wave decides at least the first one
       for (int wave = 0; wave < npix + 1; ++wave) {
         for (int j = 0; j < v.num_src; ++j) {
@@ -327,8 +331,10 @@ extern "C" int dpe_fuse(dpe_ctx *ctx, const dpe_fusion_in *in, dpe_fusion_out *o
           DPE_TRY(cudaMemsetAsync(S.und_min, 0x7F, (size_t)S.W * S.H * 4, s));
         }
         DPE_TRY(cudaMemsetAsync(remaining, 0, 4, s));
-        k_mark_undecided<<<blocks, 256, 0, s>>>(f, npix);
-        k_decide<<<blocks, 256, 0, s>>>(f, npix);
+        DPE_TIMED(ctx, KID_FUSE_WAVES, s, k_mark_undecided<<<blocks, 256, 0, s>>>(f, npix));
+        DPE_LAUNCHED("k_mark_undecided", s);
+        DPE_TIMED(ctx, KID_FUSE_WAVES, s, k_decide<<<blocks, 256, 0, s>>>(f, npix));
+        DPE_LAUNCHED("k_decide", s);
         int rem = 0;
         DPE_TRY(cudaMemcpyAsync(&rem, remaining, 4, cudaMemcpyDeviceToHost, s));
         DPE_TRY(cudaStreamSynchronize(s));
@@ -338,11 +344,13 @@ extern "C" int dpe_fuse(dpe_ctx *ctx, const dpe_fusion_in *in, dpe_fusion_out *o
       DPE_TRY(cudaMemsetAsync(status, 2, npix, s));
     }
     k_accept_flags<<<blocks, 256, 0, s>>>(status, flags, npix);
+    DPE_LAUNCHED("k_accept_flags", s);
     DPE_TRY(cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, flags, offsets, npix, s));
-    k_emit<<<blocks, 256, 0, s>>>(f, offsets, base, cap_dev, d_xyz, d_rgb, d_origin, d_ncons, i);
+    DPE_TIMED(ctx, KID_FUSE_EMIT, s, k_emit<<<blocks, 256, 0, s>>>(f, offsets, base, cap_dev, d_xyz, d_rgb, d_origin, d_ncons, i));
+    DPE_LAUNCHED("k_emit", s);
     k_advance_base<<<1, 1, 0, s>>>(base, offsets, status, npix);
+    DPE_LAUNCHED("k_advance_base", s);
   }
-  DPE_TRY(cudaGetLastError());
   DPE_TRY(cudaEventRecord(ctx->ev1, s));
   long long count = 0;
   DPE_TRY(cudaMemcpyAsync(&count, base, sizeof(long long), cudaMemcpyDeviceToHost, s));
@@ -355,6 +363,7 @@ extern "C" int dpe_fuse(dpe_ctx *ctx, const dpe_fusion_in *in, dpe_fusion_out *o
     if (out->num_consistent) DPE_TRY(cudaMemcpyAsync(out->num_consistent, d_ncons, (size_t)ncopy, cudaMemcpyDeviceToHost, s));
   }
   DPE_TRY(cudaStreamSynchronize(s));
+  ctx->collect();
   float ms = 0.f;
   DPE_TRY(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
   out->gpu_ms = ms;

@@ -456,7 +456,7 @@ __global__ void __launch_bounds__(128) k_random_init(const PMArgs *__restrict__ 
   const int center = px + py * a.W;
   const dpe_camera &rc = a.cam[0];
   RefWindow rw;
-  build_ref_window(a, px, py, rw);
+  build_ref_window(a, px, py, rw, KID_RANDOM_INIT);
   const int n = a.N - 1;
   if (a.P.state == DPE_FIRST_INIT) {
     Rng rng = make_rng(a, center);
@@ -565,7 +565,7 @@ __global__ void __launch_bounds__(128) k_strong_update(const PMArgs *__restrict_
   if (G(a.weak, center, L, 201) == DPE_WEAK) return;
   const dpe_camera &rc = a.cam[0];
   RefWindow rw;
-  build_ref_window(a, px, py, rw);
+  build_ref_window(a, px, py, rw, KID_STRONG_UPDATE);
   float cost_array[8][kMaxSrc];
   for (int d = 0; d < 8; ++d)
     for (int j = 0; j < n; ++j) cost_array[d][j] = 0.0f;
@@ -1071,7 +1071,7 @@ __global__ void __launch_bounds__(128) k_weak_update(const PMArgs *__restrict__ 
   a.plane[center] = pl_final;
   // final re-cost with the strong window (DPE.cu:1849-1865); the radius swap there has no effect
   RefWindow rw;
-  build_ref_window(a, px, py, rw);
+  build_ref_window(a, px, py, rw, KID_WEAK_UPDATE);
   float cn = 0.0f;
   for (int i = 0; i < n; ++i)
     if (vw[i] > 0) cn += vw[i] * ncc_strong(a, px, py, i + 1, pl_final, rw);
@@ -1157,7 +1157,7 @@ __global__ void __launch_bounds__(128) k_depth_to_weak(const PMArgs *__restrict_
   if (px < margin || py < margin || px >= W - margin || py >= H - margin) { weak_out[center] = DPE_UNKNOWN; return; }
   const dpe_camera &rc = a.cam[0];
   RefWindow rw;
-  build_ref_window(a, px, py, rw);
+  build_ref_window(a, px, py, rw, KID_DEPTH_TO_WEAK);
   Sweep s;
   sweep_setup(a, px, py, rw, s);
   if (s.depth == 0 || s.valid == 0) { weak_out[center] = DPE_UNKNOWN; return; }
@@ -1213,7 +1213,7 @@ __global__ void __launch_bounds__(128) k_local_refine(const PMArgs *__restrict__
   const int center = px + py * a.W;
   const dpe_camera &rc = a.cam[0];
   RefWindow rw;
-  build_ref_window(a, px, py, rw);
+  build_ref_window(a, px, py, rw, KID_LOCAL_REFINE);
   Sweep s;
   sweep_setup(a, px, py, rw, s);
   if (s.depth == 0) return;

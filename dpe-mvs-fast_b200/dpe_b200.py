@@ -61,7 +61,8 @@ class FusionView(C.Structure):
 
 
 class FusionIn(C.Structure):
-    _fields_ = [("num_views", C.c_int), ("views", C.POINTER(FusionView)), ("mode", C.c_int), ("memory", C.c_int)]
+    _fields_ = [("num_views", C.c_int), ("views", C.POINTER(FusionView)), ("mode", C.c_int), ("memory", C.c_int),
+                ("min_consistent", C.c_int)]
 
 
 class FusionOut(C.Structure):
@@ -75,12 +76,39 @@ class NCCQuery(C.Structure):
                 ("count", C.c_int64), ("px", C.c_void_p), ("py", C.c_void_p), ("src", C.c_void_p), ("plane", C.c_void_p)]
 
 
+class SceneView(C.Structure):
+    _fields_ = [("gray", C.c_void_p), ("bgr", C.c_void_p), ("camera", Camera), ("num_src", C.c_int),
+                ("src_views", C.c_void_p), ("edges", C.POINTER(C.c_void_p)), ("labels", C.POINTER(C.c_void_p))]
+
+
+class Schedule(C.Structure):
+    _fields_ = [("num_levels", C.c_int), ("refine_calls", C.c_int), ("max_iterations", C.c_int),
+                ("fuse_mode", C.c_int), ("min_consistent", C.c_int), ("seed", C.c_uint64)]
+
+
+class KernelStat(C.Structure):
+    _fields_ = [("name", C.c_char * 32), ("launches", C.c_int64), ("ms", C.c_double),
+                ("strong_ncc_evals", C.c_uint64), ("weak_ncc_evals", C.c_uint64)]
+
+
+class SceneIn(C.Structure):
+    _fields_ = [("num_views", C.c_int), ("width", C.c_int), ("height", C.c_int), ("views", C.POINTER(SceneView)),
+                ("memory", C.c_int)]
+
+
+class SceneOut(C.Structure):
+    _fields_ = [("depth", C.POINTER(C.c_void_p)), ("normal", C.POINTER(C.c_void_p)), ("weak", C.POINTER(C.c_void_p)),
+                ("selected_views", C.POINTER(C.c_void_p)), ("out_memory", C.c_int), ("fusion", FusionOut),
+                ("gpu_ms", C.c_float), ("fusion_ms", C.c_float), ("num_levels", C.c_int), ("calls", C.c_int)]
+
+
 class Limits(C.Structure):
     _fields_ = [("max_width", C.c_int), ("max_height", C.c_int), ("max_images", C.c_int)]
 
 
 EXPORTED = ["dpe_status_string", "dpe_last_error", "dpe_params_default", "dpe_ctx_create", "dpe_ctx_destroy", "dpe_pm_run",
-            "dpe_fuse", "dpe_ncc_eval", "dpe_ctx_set_eval_counting"]
+            "dpe_fuse", "dpe_ncc_eval", "dpe_ctx_set_eval_counting", "dpe_scene_run", "dpe_ctx_set_profiling",
+            "dpe_ctx_reset_kernel_stats", "dpe_ctx_get_kernel_stats", "dpe_launch_count", "dpe_fp32_peak"]
 
 _lib = None
 
@@ -105,6 +133,13 @@ def load_library(path: Optional[str] = None) -> C.CDLL:
     lib.dpe_fuse.argtypes = [C.c_void_p, C.POINTER(FusionIn), C.POINTER(FusionOut)]
     lib.dpe_ncc_eval.argtypes = [C.c_void_p, C.POINTER(NCCQuery), C.c_void_p]
     lib.dpe_ctx_set_eval_counting.argtypes = [C.c_void_p, C.c_int]
+    lib.dpe_scene_run.argtypes = [C.c_void_p, C.POINTER(SceneIn), C.POINTER(Schedule), C.POINTER(SceneOut)]
+    lib.dpe_ctx_set_profiling.argtypes = [C.c_void_p, C.c_int]
+    lib.dpe_ctx_reset_kernel_stats.argtypes = [C.c_void_p]
+    lib.dpe_ctx_get_kernel_stats.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int)]
+    lib.dpe_launch_count.restype = C.c_uint64
+    lib.dpe_launch_count.argtypes = []
+    lib.dpe_fp32_peak.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
     if path is None:
         _lib = lib
     return lib
@@ -199,6 +234,29 @@ class Context:
     def set_eval_counting(self, on: bool):
         self.lib.dpe_ctx_set_eval_counting(self.handle, 1 if on else 0)
 
+    def set_profiling(self, on: bool):
+        self.lib.dpe_ctx_set_profiling(self.handle, 1 if on else 0)
+
+    def reset_kernel_stats(self):
+        self.lib.dpe_ctx_reset_kernel_stats(self.handle)
+
+    def kernel_stats(self) -> Dict[str, Dict]:
+        arr = (KernelStat * 64)()
+        n = C.c_int()
+        st = self.lib.dpe_ctx_get_kernel_stats(self.handle, arr, 64, C.byref(n))
+        if st not in (OK, ERR_CAPACITY):
+            raise DPEError(st, "dpe_ctx_get_kernel_stats")
+        return {arr[i].name.decode(): dict(launches=int(arr[i].launches), ms=float(arr[i].ms),
+                                           strong_ncc_evals=int(arr[i].strong_ncc_evals),
+                                           weak_ncc_evals=int(arr[i].weak_ncc_evals)) for i in range(min(n.value, 64))}
+
+    def fp32_peak_tflops(self) -> float:
+        v = C.c_double()
+        st = self.lib.dpe_fp32_peak(self.handle, C.byref(v))
+        if st != OK:
+            raise DPEError(st, "dpe_fp32_peak")
+        return float(v.value)
+
     # ------------------------------------------------------------------ PatchMatch
     def pm_run(self, images, cameras, params: Params, *, out=None, want_costs=True, **kw) -> Dict:
         """One per-view call on host arrays (memory=MEM_HOST) or device tensors (memory=MEM_DEVICE)."""
@@ -224,7 +282,7 @@ class Context:
 
     # ------------------------------------------------------------------ fusion
     def fuse(self, views: List[Dict], mode: int = FUSE_FP64, capacity: Optional[int] = None,
-             memory: int = MEM_HOST) -> Dict:
+             memory: int = MEM_HOST, min_consistent: int = 1) -> Dict:
         arr = (FusionView * len(views))()
         keep = []
         total = 0
@@ -248,7 +306,7 @@ class Context:
         bgr = np.zeros((max(cap, 1), 3), np.uint8)
         origin = np.zeros((max(cap, 1), 2), np.int32)
         ncons = np.zeros(max(cap, 1), np.uint8)
-        fin = FusionIn(len(views), arr, mode, memory)
+        fin = FusionIn(len(views), arr, mode, memory, min_consistent)
         fo = FusionOut()
         fo.capacity = cap
         fo.xyz, fo.bgr, fo.origin, fo.num_consistent = _ptr(xyz), _ptr(bgr), _ptr(origin), _ptr(ncons)
@@ -257,6 +315,62 @@ class Context:
             raise DPEError(st, "dpe_fuse")
         n = int(fo.count)
         return dict(count=n, xyz=xyz[:n], bgr=bgr[:n], origin=origin[:n], num_consistent=ncons[:n], gpu_ms=fo.gpu_ms)
+
+    # ------------------------------------------------------------------ whole scene
+    def scene_run(self, gray, bgr, cameras, srcs, edges=None, labels=None, *, num_levels=0, refine_calls=3,
+                  max_iterations=3, fuse_mode=FUSE_FP64, min_consistent=1, seed=1, memory=MEM_HOST,
+                  want_maps=True, point_capacity=None) -> Dict:
+        """The reference's full schedule over all views (dpe_scene_run).  gray[v]: (H, W) uint8,
+        bgr[v]: (H, W, 3) uint8, cameras[v]: full-resolution camera dicts, srcs[v]: source view
+        indices, edges[v][level] / labels[v][level]: per-level maps (level 0 = coarsest)."""
+        V = len(gray)
+        H, W = int(gray[0].shape[0]), int(gray[0].shape[1])
+        arr = (SceneView * V)()
+        keep = []
+        for v in range(V):
+            sv = arr[v]
+            sv.gray = _ptr(gray[v])
+            sv.bgr = _ptr(bgr[v]) if bgr is not None else None
+            sv.camera = make_camera(cameras[v])
+            src = np.ascontiguousarray(np.asarray(srcs[v], dtype=np.int32))
+            keep.append(src)
+            sv.num_src = len(src)
+            sv.src_views = _ptr(src)
+            if edges is not None:
+                ea = (C.c_void_p * len(edges[v]))(*[_ptr(e) for e in edges[v]])
+                keep.append(ea)
+                sv.edges = C.cast(ea, C.POINTER(C.c_void_p))
+            if labels is not None:
+                la = (C.c_void_p * len(labels[v]))(*[_ptr(x) for x in labels[v]])
+                keep.append(la)
+                sv.labels = C.cast(la, C.POINTER(C.c_void_p))
+        sc = SceneIn(V, W, H, arr, memory)
+        sch = Schedule(num_levels, refine_calls, max_iterations, fuse_mode if fuse_mode is not None else -1,
+                       min_consistent, seed)
+        so = SceneOut()
+        so.out_memory = MEM_HOST
+        res = {}
+        if want_maps:
+            res["depth"] = [np.zeros((H, W), np.float32) for _ in range(V)]
+            res["normal"] = [np.zeros((H, W, 3), np.float32) for _ in range(V)]
+            res["weak"] = [np.zeros((H, W), np.uint8) for _ in range(V)]
+            res["views"] = [np.zeros((H, W), np.uint32) for _ in range(V)]
+            for key, field in (("depth", "depth"), ("normal", "normal"), ("weak", "weak"), ("views", "selected_views")):
+                pa = (C.c_void_p * V)(*[_ptr(x) for x in res[key]])
+                keep.append(pa)
+                setattr(so, field, C.cast(pa, C.POINTER(C.c_void_p)))
+        cap = V * H * W if point_capacity is None else point_capacity
+        xyz = np.zeros((max(cap, 1), 3), np.float32)
+        rgb = np.zeros((max(cap, 1), 3), np.uint8)
+        so.fusion.capacity = cap
+        so.fusion.xyz, so.fusion.bgr = _ptr(xyz), _ptr(rgb)
+        st = self.lib.dpe_scene_run(self.handle, C.byref(sc), C.byref(sch), C.byref(so))
+        if st != OK:
+            raise DPEError(st, "dpe_scene_run")
+        n = int(so.fusion.count)
+        res.update(points=n, xyz=xyz[:n], bgr=rgb[:n], gpu_ms=so.gpu_ms, fusion_ms=so.fusion_ms,
+                   num_levels=so.num_levels, calls=so.calls)
+        return res
 
     # ------------------------------------------------------------------ NCC queries
     def ncc_eval(self, images, cameras, params: Params, px, py, src, planes) -> np.ndarray:

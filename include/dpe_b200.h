@@ -140,6 +140,8 @@ typedef struct dpe_fusion_in {
   const dpe_fusion_view *views;  /* host array, in pair.txt order */
   int mode;                      /* DPE_FUSE_FP64 or DPE_FUSE_FLOAT */
   int memory;                    /* where depth/normal/weak/bgr/block_mask live */
+  int min_consistent;            /* consistent sources a point needs; <= 1 is the reference rule
+                                    num_consistent >= 1 (DPE.cpp:1520) */
 } dpe_fusion_in;
 
 typedef struct dpe_fusion_out {
@@ -166,6 +168,56 @@ typedef struct dpe_ncc_query {
   const int32_t *src;     /* count source index 1..num_images-1 */
   const float *plane;     /* count*4 plane in reference-camera coordinates (n, distance) */
 } dpe_ncc_query;
+
+/* ---- whole-scene schedule (the pyramid / call loop of main.cpp:321-466, without file I/O) ---- */
+typedef struct dpe_scene_view {
+  const uint8_t *gray;            /* W*H gray image at full resolution (imread GRAYSCALE)           */
+  const uint8_t *bgr;             /* W*H*3 colour image for fusion; NULL when not fusing            */
+  dpe_camera camera;              /* as read from cams/ (full resolution)                          */
+  int num_src;
+  const int *src_views;           /* host array: view indices (pair.txt sources with score > 0)    */
+  const uint8_t *const *edges;    /* host array, one map per level (level 0 = coarsest), or NULL   */
+  const int32_t *const *labels;   /* host array, one map per level, or NULL                         */
+} dpe_scene_view;
+
+typedef struct dpe_schedule {
+  int num_levels;       /* 0: the reference rule, halve max(W,H) until <= 800 (main.cpp:223-238) */
+  int refine_calls;     /* geom-consistency REFINE_ITER calls per level (main.cpp:422: 3)        */
+  int max_iterations;   /* red/black iterations per call (main.cpp:418, 444: 3)                  */
+  int fuse_mode;        /* DPE_FUSE_FP64 / DPE_FUSE_FLOAT, or -1 for no fusion                   */
+  int min_consistent;   /* fusion: consistent sources per point (<= 1: the reference rule)        */
+  uint64_t seed;        /* base of the per-call random streams                                    */
+} dpe_schedule;
+
+typedef struct dpe_scene {
+  int num_views;
+  int width;                      /* full resolution, equal for every view (CheckImages)          */
+  int height;
+  const dpe_scene_view *views;    /* host array, pair.txt order                                    */
+  int memory;                     /* where gray / bgr / edges / labels live                        */
+} dpe_scene;
+
+/* per kernel class statistics (dpe_ctx_get_kernel_stats) */
+typedef struct dpe_kernel_stat {
+  char name[32];
+  int64_t launches;           /* launches timed while profiling was on            */
+  double ms;                  /* summed device time of those launches              */
+  uint64_t strong_ncc_evals;  /* strong-window NCC evaluations while counting      */
+  uint64_t weak_ncc_evals;    /* deformable-window NCC evaluations while counting  */
+} dpe_kernel_stat;
+
+typedef struct dpe_scene_out {
+  float **depth;                  /* optional host array of num_views pointers: final W*H depth    */
+  float **normal;                 /* optional: W*H*3 world normals                                 */
+  uint8_t **weak;                 /* optional: W*H pixel states                                    */
+  uint32_t **selected_views;      /* optional: W*H view masks                                      */
+  int out_memory;                 /* memory space the pointers above refer to                      */
+  dpe_fusion_out fusion;          /* fused points (host memory), when fuse_mode >= 0               */
+  float gpu_ms;                   /* device time of the whole schedule including fusion            */
+  float fusion_ms;
+  int num_levels;
+  int calls;                      /* per-view PatchMatch calls run                                 */
+} dpe_scene_out;
 
 /* ---- context ---- */
 typedef struct dpe_ctx dpe_ctx;
@@ -204,6 +256,15 @@ int dpe_pm_run(dpe_ctx *ctx, const dpe_problem *problem, dpe_pm_out *out);
  * (ExportPointCloud, DPE.cpp:532-572). */
 int dpe_fuse(dpe_ctx *ctx, const dpe_fusion_in *in, dpe_fusion_out *out);
 
+/* Replaces main()'s PatchMatch schedule and fusion (main.cpp:385-461) for a whole scene, with every
+ * view's state kept in device memory between calls: per level the float image pyramid
+ * (SceneCache::GetGrayFloatImage, DPE.cpp:720-737), one FIRST_INIT / REFINE_INIT call and
+ * `refine_calls` geom REFINE_ITER calls per view in pair.txt order (Gauss-Seidel across views),
+ * ProcessProblem's result assembly (main.cpp:266-279), nearest-neighbour state rescale between
+ * levels (RescaleMatToTargetSize, DPE.cpp:1313-1335), then RunFusion.  Edge and label maps are
+ * host preprocessing (EdgeSegment) and are passed in. */
+int dpe_scene_run(dpe_ctx *ctx, const dpe_scene *scene, const dpe_schedule *schedule, dpe_scene_out *out);
+
 /* Strong bilateral NCC (ComputeBilateralNCCOld, DPE.cu:696-782) at explicit queries; test and
  * measurement entry point. */
 int dpe_ncc_eval(dpe_ctx *ctx, const dpe_ncc_query *q, float *costs_out);
@@ -212,6 +273,20 @@ int dpe_ncc_eval(dpe_ctx *ctx, const dpe_ncc_query *q, float *costs_out);
  * dpe_pm_out.strong_ncc_evals / weak_ncc_evals (device atomics; off by default).  The reference
  * has no counterpart (it prints stage times only, main.cpp:17-45). */
 int dpe_ctx_set_eval_counting(dpe_ctx *ctx, int on);
+
+/* Per-kernel device timing (an event pair around every launch while on; off by default), the
+ * statistics accumulated since the last reset, and a reset.  No reference counterpart (the
+ * reference times the whole launch sequence with one event pair, DPE.cu:3132-3239). */
+int dpe_ctx_set_profiling(dpe_ctx *ctx, int on);
+int dpe_ctx_reset_kernel_stats(dpe_ctx *ctx);
+int dpe_ctx_get_kernel_stats(dpe_ctx *ctx, dpe_kernel_stat *out, int capacity, int *count);
+
+/* Number of kernels this library has launched in the process (all contexts). */
+uint64_t dpe_launch_count(void);
+
+/* Measured FP32 FMA throughput of the context's device in TFLOP/s (a dependent-chain FMA kernel
+ * over every SM): the roofline denominator of the NCC cost kernels, which are FP32-issue bound. */
+int dpe_fp32_peak(dpe_ctx *ctx, double *tflops);
 
 #ifdef __cplusplus
 }

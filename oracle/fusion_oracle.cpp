@@ -118,8 +118,10 @@ extern "C" int oracle_fuse(const dpe_fusion_in *in, dpe_fusion_out *out) {
           if (ok) { used_c[j] = src_c; used_r[j] = src_r; n_cons++; }
         }
         const float factor = V.weak[pix] == DPE_WEAK ? 0.45f : 0.3f;
-        const bool accept = in->mode == DPE_FUSE_FP64 ? (n_cons >= 1 && dyn_d > (double)factor * n_cons)
-                                                      : (n_cons >= 1 && dyn_f > factor * n_cons);
+        // the reference rule is n >= 1 (DPE.cpp:1520); min_consistent > 1 raises it
+        const int need = in->min_consistent > 1 ? in->min_consistent : 1;
+        const bool accept = in->mode == DPE_FUSE_FP64 ? (n_cons >= need && dyn_d > (double)factor * n_cons)
+                                                      : (n_cons >= need && dyn_f > factor * n_cons);
         if (!accept) continue;
         const uint8_t *rc = &V.bgr[3 * pix];
         float col[3] = {(float)rc[0], (float)rc[1], (float)rc[2]};

@@ -77,7 +77,7 @@ def pm_run(images, cameras, params, threads: int = 0, **kw) -> Dict:
     return out
 
 
-def fuse(views: List[Dict], mode: int = D.FUSE_FP64, capacity: Optional[int] = None) -> Dict:
+def fuse(views: List[Dict], mode: int = D.FUSE_FP64, capacity: Optional[int] = None, min_consistent: int = 1) -> Dict:
     arr = (D.FusionView * len(views))()
     keep = []
     total = 0
@@ -101,7 +101,7 @@ def fuse(views: List[Dict], mode: int = D.FUSE_FP64, capacity: Optional[int] = N
     bgr = np.zeros((max(cap, 1), 3), np.uint8)
     origin = np.zeros((max(cap, 1), 2), np.int32)
     ncons = np.zeros(max(cap, 1), np.uint8)
-    fin = D.FusionIn(len(views), arr, mode, D.MEM_HOST)
+    fin = D.FusionIn(len(views), arr, mode, D.MEM_HOST, min_consistent)
     fo = D.FusionOut()
     fo.capacity = cap
     fo.xyz, fo.bgr, fo.origin, fo.num_consistent = xyz.ctypes.data, bgr.ctypes.data, origin.ctypes.data, ncons.ctypes.data
