@@ -16,6 +16,13 @@
 using std::max;
 using std::min;
 static dim3 blockIdx, threadIdx, blockDim;
+#undef __global__
+#undef __device__
+#undef __host__
+#undef __forceinline__
+#undef __launch_bounds__
+#undef __grid_constant__
+#undef __constant__
 #define __global__
 #define __device__
 #define __host__
@@ -26,6 +33,12 @@ static dim3 blockIdx, threadIdx, blockDim;
 #define __restrict__
 static inline unsigned __umulhi(unsigned a, unsigned b) { return (unsigned)(((unsigned long long)a * b) >> 32); }
 template <class T> static inline T __ldg(const T *p) { return *p; }
+// the device's correctly rounded, never-contracted arithmetic intrinsics
+static inline float __fmul_rn(float a, float b) { volatile float r = a * b; return r; }
+static inline float __fadd_rn(float a, float b) { volatile float r = a + b; return r; }
+static inline float __fsub_rn(float a, float b) { volatile float r = a - b; return r; }
+static inline float __fdiv_rn(float a, float b) { volatile float r = a / b; return r; }
+static inline float __fsqrt_rn(float a) { volatile float r = std::sqrt(a); return r; }
 static inline unsigned long long atomicAdd(unsigned long long *p, unsigned long long v) {
   const unsigned long long o = *p;
   *p += v;
