@@ -1,0 +1,124 @@
+"""The committed golden fixtures (tests/golden/*.npz, made by tests/golden/make_golden.py).
+
+CPU: the oracle reproduces every fixture bit for bit (a change to the oracle that moves any result
+shows up here).  GPU: the kernels, called through the C-ABI, meet the parity bars against the
+fixtures: NCC within 1e-4 of FP64, first-init depth within 0.1 % on >= 99.5 % of pixels, the
+geometric refine call by the statistical bar, fusion bit-exact in FP64 mode.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import dpe_b200 as D
+import helpers as h
+import oracle_py as O
+
+import importlib.util
+
+_spec = importlib.util.spec_from_file_location("make_golden", os.path.join(os.path.dirname(__file__), "golden",
+                                                                           "make_golden.py"))
+G = importlib.util.module_from_spec(_spec)
+_spec.loader.exec_module(G)
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+NCC_TOL = 1e-4
+DEPTH_REL_TOL = 1e-3
+DEPTH_FRACTION = 0.995
+
+
+def _load(name):
+    return np.load(os.path.join(GOLDEN, name))
+
+
+def _ncc_inputs(z):
+    images = [np.ascontiguousarray(g.astype(np.float32)) for g in z["gray"]]
+    return images, G.cams_from_array(z["cams"]), G.params_from_json(z["params"])
+
+
+def _pm_first(z):
+    images = [np.ascontiguousarray(g.astype(np.float32)) for g in z["gray"]]
+    return images, G.cams_from_array(z["cams"]), G.params_from_json(z["params0"]), int(z["seed0"])
+
+
+def _pm_refine_kw(z):
+    depths = [np.ascontiguousarray(d) for d in z["depths"]]
+    return dict(plane_in=np.ascontiguousarray(z["state_in"]), views_in=np.ascontiguousarray(z["views0"]),
+                weak_in=np.ascontiguousarray(z["weak_in"]), edge=np.ascontiguousarray(z["edge"]),
+                edge_low=np.ascontiguousarray(z["edge_low"]), label=np.ascontiguousarray(z["label"]),
+                depths=depths, seed=int(z["seed1"]))
+
+
+# ------------------------------------------------------------------ the oracle against the fixtures (CPU)
+def test_golden_ncc_oracle_reproduces():
+    z = _load("ncc_small.npz")
+    images, cams, p = _ncc_inputs(z)
+    f32 = O.ncc_strong(images, cams, p, z["px"], z["py"], z["src"], z["planes"], fp64=False)
+    f64 = O.ncc_strong(images, cams, p, z["px"], z["py"], z["src"], z["planes"], fp64=True)
+    assert np.array_equal(f32, z["cost_f32"])
+    assert np.array_equal(f64, z["cost_f64"])
+    assert np.abs(f32 - f64).max() <= NCC_TOL
+
+
+def test_golden_pm_oracle_reproduces():
+    z = _load("pm_tiny.npz")
+    images, cams, p0, seed0 = _pm_first(z)
+    o0 = O.pm_run(images, cams, p0, seed=seed0)
+    for k, g in (("plane", "plane0"), ("weak", "weak0"), ("views", "views0"), ("costs", "cost0")):
+        assert np.array_equal(o0[k], z[g], equal_nan=k in ("plane", "costs")), k
+    p1 = G.params_from_json(z["params1"])
+    o1 = O.pm_run(images, cams, p1, **_pm_refine_kw(z))
+    for k, g in (("plane", "plane1"), ("weak", "weak1"), ("views", "views1"), ("costs", "cost1")):
+        assert np.array_equal(o1[k], z[g], equal_nan=k in ("plane", "costs")), k
+
+
+def test_golden_fusion_oracle_reproduces():
+    z = _load("fusion_tiny.npz")
+    views = G.fusion_views_from(z)
+    for tag, mode, mc in (("fp64", D.FUSE_FP64, 1), ("float", D.FUSE_FLOAT, 1), ("fp64_min2", D.FUSE_FP64, 2)):
+        r = O.fuse(views, mode, min_consistent=mc)
+        assert r["count"] == int(z[f"{tag}_count"]), tag
+        for k in ("xyz", "bgr", "origin", "num_consistent"):
+            assert np.array_equal(r[k], z[f"{tag}_{k}"]), (tag, k)
+
+
+# ------------------------------------------------------------------ the kernels against the fixtures (GPU)
+@pytest.mark.gpu
+def test_golden_ncc_gpu(ctx):
+    z = _load("ncc_small.npz")
+    images, cams, p = _ncc_inputs(z)
+    g = ctx.ncc_eval(images, cams, p, z["px"], z["py"], z["src"], z["planes"])
+    err = np.abs(g.astype(np.float64) - z["cost_f64"])
+    print(f"golden NCC: max |gpu - fp64| {err.max():.3e}")
+    assert err.max() <= NCC_TOL
+
+
+@pytest.mark.gpu
+def test_golden_pm_gpu(ctx):
+    z = _load("pm_tiny.npz")
+    images, cams, p0, seed0 = _pm_first(z)
+    g0 = ctx.pm_run(images, cams, p0, seed=seed0)
+    agree0 = h.rel_depth_agreement(g0["plane"][..., 3], z["plane0"][..., 3], DEPTH_REL_TOL)
+    p1 = G.params_from_json(z["params1"])
+    g1 = ctx.pm_run(images, cams, p1, **_pm_refine_kw(z))
+    agree1 = h.rel_depth_agreement(g1["plane"][..., 3], z["plane1"][..., 3], DEPTH_REL_TOL)
+    weak1 = float((g1["weak"] == z["weak1"]).mean())
+    print(f"golden pm: first-init agreement {agree0:.5f}, geom refine agreement {agree1:.5f}, states {weak1:.5f}")
+    assert agree0 >= DEPTH_FRACTION
+    assert (g0["weak"] == z["weak0"]).mean() >= 0.99
+    # geometric refine: the statistical bar of the parity tests (FMA contraction decides near-ties)
+    assert agree1 >= 0.95
+    assert weak1 >= 0.98
+
+
+@pytest.mark.gpu
+def test_golden_fusion_gpu(ctx):
+    z = _load("fusion_tiny.npz")
+    views = G.fusion_views_from(z)
+    for tag, mc in (("fp64", 1), ("fp64_min2", 2)):
+        r = ctx.fuse(views, D.FUSE_FP64, min_consistent=mc)
+        assert r["count"] == int(z[f"{tag}_count"]), tag
+        for k in ("xyz", "bgr", "origin", "num_consistent"):
+            assert np.array_equal(r[k], z[f"{tag}_{k}"]), (tag, k)
+    r = ctx.fuse(views, D.FUSE_FLOAT)
+    assert abs(r["count"] - int(z["float_count"])) <= 2
