@@ -9,6 +9,7 @@
 #include <atomic>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -419,11 +420,18 @@ extern "C" int dpe_pm_run(dpe_ctx *ctx, const dpe_problem *p, dpe_pm_out *out) {
 
 // ------------------------------------------------------------------ dpe_ncc_eval
 namespace {
+// kDeviceCheck: queries in device memory, which the host cannot validate, are checked here; a
+// query outside the problem gets NaN.
+template <bool kDeviceCheck>
 __global__ void k_ncc_queries(const PMArgs *__restrict__ pa, int64_t n, const int32_t *px, const int32_t *py,
                               const int32_t *src, const float4 *pl, float *out) {
   const PMArgs &a = *pa;
   const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
+  if (kDeviceCheck && (src[k] < 1 || src[k] >= a.N || px[k] < 0 || px[k] >= a.W || py[k] < 0 || py[k] >= a.H)) {
+    out[k] = __int_as_float(0x7fffffff);
+    return;
+  }
   RefWindow rw;
   build_ref_window(a, px[k], py[k], rw, KID_NCC_QUERY);
   out[k] = ncc_strong(a, px[k], py[k], src[k], pl[k], rw);
@@ -470,7 +478,7 @@ extern "C" int dpe_ncc_eval(dpe_ctx *ctx, const dpe_ncc_query *q, float *costs_o
   PMArgs *d_args = A.get<PMArgs>("pm_args", 1);
   if (!d_args) return DPE_ERR_OUT_OF_MEMORY;
   DPE_TRY(cudaMemcpyAsync(d_args, &a, sizeof(PMArgs), cudaMemcpyHostToDevice, s));
-  DPE_TIMED(ctx, KID_NCC_QUERY, s, k_ncc_queries<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(d_args, n, dpx, dpy, dsrc, dpl, dout));
+  DPE_TIMED(ctx, KID_NCC_QUERY, s, k_ncc_queries<false><<<(unsigned)((n + 127) / 128), 128, 0, s>>>(d_args, n, dpx, dpy, dsrc, dpl, dout));
   PM_LAUNCHED("k_ncc_queries", s);
   DPE_TRY(cudaMemcpyAsync(costs_out, dout, n * 4, cudaMemcpyDeviceToHost, s));
   DPE_TRY(cudaStreamSynchronize(s));
@@ -512,6 +520,81 @@ extern "C" int dpe_kernel_info(char *buf, int len) {
   std::snprintf(line, sizeof(line), "stack limit %zu B\n", stack);
   s += line;
   std::snprintf(buf, (size_t)len, "%s", s.c_str());
+  return DPE_OK;
+}
+
+// ------------------------------------------------------------------ allocation-free NCC queries
+namespace {
+// Scratch of dpe_ncc_eval_noalloc: the per-call argument block followed by the clamp-padded
+// images.  Every GPU that loads the library holds these 16 MiB until the process exits.  Nothing
+// in it needs to start at zero: each call writes the whole argument block and every padded texel
+// it reads before the query kernel runs.
+constexpr size_t kStaticScratchBytes = size_t(16) << 20;
+static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
+constexpr int kMaxDevices = 64;
+std::mutex g_static_mu;
+unsigned char *g_static_addr[kMaxDevices] = {};
+
+size_t round256(size_t b) { return (b + 255) & ~size_t(255); }
+}  // namespace
+
+extern "C" int dpe_ncc_eval_noalloc(const dpe_ncc_query *q, float *costs_out, void *stream) {
+  if (!q || !costs_out || q->count < 0) return DPE_ERR_INVALID_ARGUMENT;
+  if (q->num_images < 2 || q->num_images > DPE_MAX_IMAGES || q->width < 16 || q->height < 16) return DPE_ERR_INVALID_ARGUMENT;
+  if (q->params.strong_increment <= 0 || q->params.strong_radius < 0 ||
+      (2 * q->params.strong_radius) / q->params.strong_increment + 1 > kMaxWin)
+    return DPE_ERR_INVALID_ARGUMENT;
+  const int W = q->width, H = q->height, N = q->num_images;
+  for (int i = 0; i < N; ++i)
+    if (!q->images[i]) return DPE_ERR_INVALID_ARGUMENT;
+  if (q->count > 0 && (!q->px || !q->py || !q->src || !q->plane)) return DPE_ERR_INVALID_ARGUMENT;
+  const size_t PL = (size_t)(W + 2) * (H + 2);
+  const size_t img_bytes = round256(PL * sizeof(float));
+  const size_t need = round256(sizeof(PMArgs)) + (size_t)N * img_bytes;
+  if (need > kStaticScratchBytes) {
+    char buf[200];
+    std::snprintf(buf, sizeof(buf), "dpe_ncc_eval_noalloc: %d padded %dx%d images need %zu bytes of scratch; the "
+                  "static array holds %zu", N, W + 2, H + 2, need, kStaticScratchBytes);
+    g_last_error = buf;
+    return DPE_ERR_CAPACITY;
+  }
+  if (q->count == 0) return DPE_OK;
+  int dev = 0;
+  DPE_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) return DPE_ERR_NO_DEVICE;
+  unsigned char *base = nullptr;
+  {
+    // one-time set-up per device, with that device current: the device address of the array
+    std::lock_guard<std::mutex> lock(g_static_mu);
+    if (!g_static_addr[dev]) {
+      void *ptr = nullptr;
+      DPE_TRY(cudaGetSymbolAddress(&ptr, g_static_scratch));
+      g_static_addr[dev] = static_cast<unsigned char *>(ptr);
+    }
+    base = g_static_addr[dev];
+  }
+  PMArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.W = W; a.H = H; a.N = N; a.pad_w = W + 2;
+  a.P = q->params;
+  a.P.num_images = N;
+  for (int i = 0; i < N; ++i) a.cam[i] = q->cameras[i];
+  for (int i = 1; i < N; ++i) relative_pose(a.cam[0], a.cam[i], a.Rrel[i], a.trel[i]);
+  unsigned char *img_base = base + round256(sizeof(PMArgs));
+  for (int i = 0; i < N; ++i) a.img[i] = reinterpret_cast<const float *>(img_base + (size_t)i * img_bytes);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  DPE_TRY(cudaMemcpyAsync(base, &a, sizeof(PMArgs), cudaMemcpyHostToDevice, s));
+  for (int i = 0; i < N; ++i) {
+    k_pad_image<<<dim3((W + 2 + 31) / 32, (H + 2 + 7) / 8), dim3(32, 8), 0, s>>>(
+        q->images[i], reinterpret_cast<float *>(img_base + (size_t)i * img_bytes), W, H);
+    DPE_LAUNCHED("k_pad_image", s);
+  }
+  const int64_t n = q->count;
+  k_ncc_queries<true><<<(unsigned)((n + 127) / 128), 128, 0, s>>>(reinterpret_cast<const PMArgs *>(base), n, q->px,
+                                                                    q->py, q->src,
+                                                                    reinterpret_cast<const float4 *>(q->plane),
+                                                                    costs_out);
+  DPE_LAUNCHED("k_ncc_queries", s);
   return DPE_OK;
 }
 

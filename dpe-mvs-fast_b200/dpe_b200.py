@@ -108,7 +108,8 @@ class Limits(C.Structure):
 
 EXPORTED = ["dpe_status_string", "dpe_last_error", "dpe_params_default", "dpe_ctx_create", "dpe_ctx_destroy", "dpe_pm_run",
             "dpe_fuse", "dpe_ncc_eval", "dpe_ctx_set_eval_counting", "dpe_scene_run", "dpe_ctx_set_profiling",
-            "dpe_ctx_reset_kernel_stats", "dpe_ctx_get_kernel_stats", "dpe_launch_count", "dpe_fp32_peak"]
+            "dpe_ctx_reset_kernel_stats", "dpe_ctx_get_kernel_stats", "dpe_launch_count", "dpe_fp32_peak",
+            "dpe_ncc_eval_noalloc"]
 
 _lib = None
 
@@ -140,6 +141,7 @@ def load_library(path: Optional[str] = None) -> C.CDLL:
     lib.dpe_launch_count.restype = C.c_uint64
     lib.dpe_launch_count.argtypes = []
     lib.dpe_fp32_peak.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+    lib.dpe_ncc_eval_noalloc.argtypes = [C.POINTER(NCCQuery), C.c_void_p, C.c_void_p]
     if path is None:
         _lib = lib
     return lib
@@ -380,6 +382,34 @@ class Context:
         if st != OK:
             raise DPEError(st, "dpe_ncc_eval")
         return out
+
+
+def ncc_eval_noalloc(images, cameras, params: Params, px, py, src, planes, costs_out, stream=None, lib=None):
+    """dpe_ncc_eval_noalloc: every array a CUDA tensor on the current device (images float32 (H, W),
+    px/py/src int32 (n,), planes float32 (n, 4), costs_out float32 (n,)).  The work is enqueued on
+    `stream` (a torch.cuda.Stream, default: torch's current stream) and not waited for."""
+    import torch
+
+    lib = lib or load_library()
+    q = NCCQuery()
+    q.height, q.width = int(images[0].shape[0]), int(images[0].shape[1])
+    q.num_images = len(images)
+    for i, im in enumerate(images):
+        if not (im.is_cuda and im.dtype == torch.float32 and im.is_contiguous()):
+            raise ValueError("images must be contiguous float32 CUDA tensors")
+        q.images[i] = im.data_ptr()
+        q.cameras[i] = make_camera(cameras[i])
+    q.params = params
+    for t, dt in ((px, torch.int32), (py, torch.int32), (src, torch.int32), (planes, torch.float32),
+                  (costs_out, torch.float32)):
+        if not (t.is_cuda and t.dtype == dt and t.is_contiguous()):
+            raise ValueError("queries and output must be contiguous CUDA tensors of the documented types")
+    q.count = int(px.numel())
+    q.px, q.py, q.src, q.plane = px.data_ptr(), py.data_ptr(), src.data_ptr(), planes.data_ptr()
+    s = (stream or torch.cuda.current_stream()).cuda_stream
+    st = lib.dpe_ncc_eval_noalloc(C.byref(q), C.c_void_p(costs_out.data_ptr()), C.c_void_p(s))
+    if st != OK:
+        raise DPEError(st, "dpe_ncc_eval_noalloc")
 
 
 class _Query:

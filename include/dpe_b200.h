@@ -269,6 +269,29 @@ int dpe_scene_run(dpe_ctx *ctx, const dpe_scene *scene, const dpe_schedule *sche
  * measurement entry point. */
 int dpe_ncc_eval(dpe_ctx *ctx, const dpe_ncc_query *q, float *costs_out);
 
+/* Allocation-free variant of dpe_ncc_eval for callers that cannot allocate device memory: code
+ * hosted by a framework that owns and budgets all device memory through its own allocator (a
+ * private cudaMalloc there would bypass its accounting), and real-time paths that must not pay
+ * for cudaMalloc / cudaFree, which may synchronise the device.  It has no counterpart in the
+ * reference.
+ *
+ * Every pointer in `q` (images, px, py, src, plane) and `costs_out` is DEVICE memory owned by the
+ * caller; `plane` is 16-byte aligned.  The call needs no dpe_ctx: it enqueues its work on `stream`
+ * (a cudaStream_t; NULL is the default stream) of the calling thread's current device and returns
+ * before the work completes -- synchronise the stream before reading `costs_out`.  Queries whose
+ * pixel or source index lies outside the problem get NaN.
+ *
+ * Scratch (the argument block and the clamp-padded images) lives in one statically allocated
+ * 16 MiB array in device memory, which every GPU that loads this library holds until the process
+ * exits.  A problem is accepted when 256-byte-rounded sizeof(argument block) plus num_images x
+ * 256-byte-rounded (width + 2) x (height + 2) x 4 bytes fits in 16 MiB (e.g. up to 12 images of
+ * 640x480); larger ones return DPE_ERR_CAPACITY with the sizes in dpe_last_error().  The first
+ * call on a device resolves the array's device address (cudaGetSymbolAddress) with that device
+ * current; make that first call before any stream capture.  All calls share the one array and
+ * it keeps the previous call's contents, so calls that overlap on the GPU (different streams or
+ * host threads without ordering between them) race and corrupt each other's results. */
+int dpe_ncc_eval_noalloc(const dpe_ncc_query *q, float *costs_out, void *stream);
+
 /* Statistics switch: when on, dpe_pm_run counts its NCC evaluations into
  * dpe_pm_out.strong_ncc_evals / weak_ncc_evals (device atomics; off by default).  The reference
  * has no counterpart (it prints stage times only, main.cpp:17-45). */
