@@ -1,6 +1,11 @@
 // fusion_oracle.cpp -- CPU restatement of RunFusion (DPE.cpp:1387-1548), ETH variant.
 //
-// TEST INFRASTRUCTURE ONLY: the checker for the fusion kernels.  The loop order is the
+// TEST INFRASTRUCTURE ONLY: the checker for the fusion kernels.
+// PARITY UNPINNED: the reference ships no tests or known-answer vectors for this path, and its
+// sources need the OpenCV and Boost C++ libraries, which are not available to build it, so
+// this restatement is checked against its own FP64 mode and the committed golden fixtures, not
+// against outputs of the reference itself.
+// The loop order is the
 // reference's: views in pair.txt order, pixels in raster order, sources in list order, with the
 // consumed-pixel masks updated as points are accepted, so the result depends on that order
 // exactly as the reference's does.  Two arithmetic modes:
