@@ -4,6 +4,7 @@
 // (DPE.cpp:1071-1252, DPE.cu:3130-3262).  The context owns a grow-only device arena (replacing
 // the process-wide GpuWorkspace, DPE.cpp:775-837), one stream and timing events.
 #include <cub/cub.cuh>
+#include <thrust/iterator/counting_iterator.h>
 
 #include <algorithm>
 #include <atomic>
@@ -11,6 +12,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "ctx.h"
@@ -40,6 +42,7 @@ int check_problem(const dpe_problem *p) {
   if (P.strong_radius < 0 || P.strong_increment <= 0 || P.weak_increment <= 0 || P.weak_radius < 0)
     return DPE_ERR_INVALID_ARGUMENT;
   if ((2 * P.strong_radius) / P.strong_increment + 1 > kMaxWin) return DPE_ERR_INVALID_ARGUMENT;
+  if (P.use_APD && (2 * P.weak_radius) / P.weak_increment + 1 > kMaxWin) return DPE_ERR_INVALID_ARGUMENT;
   if (P.rotate_time < 1 || P.rotate_time > 4 || P.top_k < 0 || P.max_iterations < 0) return DPE_ERR_INVALID_ARGUMENT;
   return DPE_OK;
 }
@@ -161,6 +164,11 @@ extern "C" int dpe_ctx_create(int device, const dpe_limits *limits, dpe_ctx **ou
     return DPE_ERR_CUDA;
   }
   (void)limits;
+  if (cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) {
+    cudaGetLastError();
+    dpe_ctx_destroy(c);
+    return DPE_ERR_CUDA;
+  }
   if (const char *v = std::getenv("DPE_STACK_LIMIT")) {
     const long long bytes = std::atoll(v);
     if (bytes > 0 && cudaDeviceSetLimit(cudaLimitStackSize, (size_t)bytes) != cudaSuccess) {
@@ -193,6 +201,38 @@ const dim3 kFullBlock(16, 8);
 dim3 half_grid(int W, int H) { return dim3((W + 31) / 32, ((H + 1) / 2 + 3) / 4); }
 const dim3 kHalfBlock(32, 4);
 
+// Blocks of 128 threads for a strided work list of up to `items` entries: enough to fill every
+// multiprocessor, no more than the list needs.
+unsigned list_grid(const dpe_ctx *ctx, long long items) {
+  const long long need = (items + 127) / 128;
+  const long long fill = (long long)ctx->sms * 16;
+  return (unsigned)std::max(1LL, std::min(need, fill));
+}
+
+// Calls f(std::integral_constant<int, staging>) so that f can launch the instance of a cost kernel
+// built for the call's staging (DPE_STAGE_*).
+template <class F> void with_stage(int staging, F &&f) {
+  if (staging == DPE_STAGE_FP16) f(std::integral_constant<int, DPE_STAGE_FP16>{});
+  else if (staging == DPE_STAGE_BF16) f(std::integral_constant<int, DPE_STAGE_BF16>{});
+  else f(std::integral_constant<int, DPE_STAGE_FP32>{});
+}
+
+void launch_strong_update(int staging, bool gn, dim3 grid, cudaStream_t s, const PMArgs *args, int it, int parity) {
+  with_stage(staging, [&](auto st) {
+    if (gn) k_strong_update<decltype(st)::value, true><<<grid, kHalfBlock, 0, s>>>(args, it, parity);
+    else k_strong_update<decltype(st)::value, false><<<grid, kHalfBlock, 0, s>>>(args, it, parity);
+  });
+}
+
+// WEAK pixels of one red/black colour, (x + y) & 1 == parity.
+struct WeakOfColour {
+  const uint8_t *weak;
+  int W, parity;
+  __host__ __device__ __forceinline__ bool operator()(const int &p) const {
+    return weak[p] == DPE_WEAK && (((p % W) + (p / W)) & 1) == parity;
+  }
+};
+
 }  // namespace
 
 extern "C" int dpe_pm_run(dpe_ctx *ctx, const dpe_problem *p, dpe_pm_out *out) {
@@ -218,9 +258,13 @@ extern "C" int dpe_pm_run(dpe_ctx *ctx, const dpe_problem *p, dpe_pm_out *out) {
   for (int i = 1; i < N; ++i) relative_pose(a.cam[0], a.cam[i], a.Rrel[i], a.trel[i]);
   a.key[0] = (uint32_t)p->seed;
   a.key[1] = (uint32_t)(p->seed >> 32);
+  a.stage = ctx->opt.staging;
+  a.gn = ctx->opt.gn_refine;
 
   // ---- device buffers
   float *img_pad = A.get<float>("img_pad", PL * N);
+  const int staging = ctx->opt.staging;
+  uint32_t *img_pairs = staging != DPE_STAGE_FP32 ? A.get<uint32_t>("img_pairs", PL * N) : nullptr;
   float *stage = A.get<float>("img_stage", L * N);
   a.plane = A.get<float4>("plane", L);
   a.plane_snap = A.get<float4>("plane_snap", L);
@@ -240,6 +284,25 @@ extern "C" int dpe_pm_run(dpe_ctx *ctx, const dpe_problem *p, dpe_pm_out *out) {
   a.lab_bound = A.get<short2>("lab_bound", L * 8);
   a.edge_neigh = A.get<short2>("edge_neigh", L * 8);
   a.nearest = A.get<short2>("nearest", L);
+  const size_t wcap = (L + 1) / 2;  // pixels of one colour
+  if (a.P.use_APD) {
+    const int n = N - 1;
+    const int side = (2 * a.P.weak_radius) / a.P.weak_increment + 1;
+    a.wtaps = side * side;
+    a.wtab_stride = kMaxWin * kMaxWin + 8 * a.wtaps;
+    int *wl = A.get<int>("weak_list", 2 * wcap);
+    a.wlist[0] = wl;
+    a.wlist[1] = wl ? wl + wcap : nullptr;
+    a.wcount = A.get<int>("weak_count", 2);
+    a.wtab = A.get<float2>("weak_tab", wcap * a.wtab_stride);
+    a.wwin = A.get<float4>("weak_win", wcap * kNeighbours);
+    a.wcost = A.get<float>("weak_cost", wcap * 10 * n);
+    a.wgeom = A.get<float>("weak_geom", wcap * 10 * n);
+    a.whyp = A.get<float4>("weak_hyp", wcap * 5);
+    a.wcost_r = A.get<float>("weak_cost_r", wcap * 5 * n);
+    a.wgeom_r = A.get<float>("weak_geom_r", wcap * 5 * n);
+    a.wstate = A.get<float4>("weak_state", wcap * 2);
+  }
   if (!A.ok()) return DPE_ERR_OUT_OF_MEMORY;
 
   const float4 *plane_in = nullptr;
@@ -312,6 +375,15 @@ extern "C" int dpe_pm_run(dpe_ctx *ctx, const dpe_problem *p, dpe_pm_out *out) {
     }
     a.img[i] = img_pad + PL * i;
     k_pad_image<<<dim3((W + 2 + 31) / 32, (H + 2 + 7) / 8), dim3(32, 8), 0, s>>>(src, img_pad + PL * i, W, H);
+    PM_LAUNCHED("k_pad_image", s);
+    if (i > 0 && staging != DPE_STAGE_FP32) {
+      a.pair[i] = img_pairs + PL * i;
+      if (staging == DPE_STAGE_BF16)
+        k_stage_pairs<true><<<(unsigned)((PL + 255) / 256), 256, 0, s>>>(img_pad + PL * i, img_pairs + PL * i, (long long)PL);
+      else
+        k_stage_pairs<false><<<(unsigned)((PL + 255) / 256), 256, 0, s>>>(img_pad + PL * i, img_pairs + PL * i, (long long)PL);
+      PM_LAUNCHED("k_stage_pairs", s);
+    }
   }
   unsigned long long *counters = A.get<unsigned long long>("counters", 2 * KID_COUNT);
   if (!counters) return DPE_ERR_OUT_OF_MEMORY;
@@ -319,7 +391,6 @@ extern "C" int dpe_pm_run(dpe_ctx *ctx, const dpe_problem *p, dpe_pm_out *out) {
   if (ctx->count_evals) DPE_TRY(cudaMemsetAsync(counters, 0, 16 * KID_COUNT, s));
 
   // ---- kernel sequence (DPE.cu:3157-3234)
-  PM_LAUNCHED("k_pad_image", s);
   PMArgs *d_args = A.get<PMArgs>("pm_args", 1);
   if (!d_args) return DPE_ERR_OUT_OF_MEMORY;
   DPE_TRY(cudaMemcpyAsync(d_args, &a, sizeof(PMArgs), cudaMemcpyHostToDevice, s));
@@ -362,7 +433,19 @@ extern "C" int dpe_pm_run(dpe_ctx *ctx, const dpe_problem *p, dpe_pm_out *out) {
   PM_LAUNCHED("k_gen_neighbours", s);
   DPE_TIMED(ctx, KID_NEIGHBOUR_UPDATE, s, k_neighbour_update<<<fg, kFullBlock, 0, s>>>(d_args));
   PM_LAUNCHED("k_neighbour_update", s);
-  DPE_TIMED(ctx, KID_RANDOM_INIT, s, k_random_init<<<fg, kFullBlock, 0, s>>>(d_args));
+  if (a.P.use_APD) {
+    // WEAK pixels per colour, in raster order; the states are final for the iterations
+    size_t sel_bytes = 0;
+    thrust::counting_iterator<int> first(0);
+    cub::DeviceSelect::If(nullptr, sel_bytes, first, const_cast<int *>(a.wlist[0]), const_cast<int *>(a.wcount),
+                          (int)L, WeakOfColour{a.weak, W, 0}, s);
+    void *sel_tmp = A.get<uint8_t>("select_tmp", sel_bytes + 16);
+    if (!sel_tmp) return DPE_ERR_OUT_OF_MEMORY;
+    for (int parity = 0; parity < 2; ++parity)
+      DPE_TRY(cub::DeviceSelect::If(sel_tmp, sel_bytes, first, const_cast<int *>(a.wlist[parity]),
+                                    const_cast<int *>(a.wcount) + parity, (int)L, WeakOfColour{a.weak, W, parity}, s));
+  }
+  DPE_TIMED(ctx, KID_RANDOM_INIT, s, with_stage(staging, [&](auto st) { k_random_init<decltype(st)::value><<<fg, kFullBlock, 0, s>>>(d_args); }));
   PM_LAUNCHED("k_random_init", s);
   for (int it = 0; it < a.P.max_iterations; ++it) {
     for (int parity = 0; parity < 2; ++parity) {
@@ -370,15 +453,25 @@ extern "C" int dpe_pm_run(dpe_ctx *ctx, const dpe_problem *p, dpe_pm_out *out) {
         DPE_TRY(cudaMemcpyAsync(a.plane_snap, a.plane, L * sizeof(float4), cudaMemcpyDeviceToDevice, s));
         DPE_TRY(cudaMemcpyAsync(a.cost_snap, a.cost, L * 4, cudaMemcpyDeviceToDevice, s));
       }
-      DPE_TIMED(ctx, KID_STRONG_UPDATE, s, k_strong_update<<<hg, kHalfBlock, 0, s>>>(d_args, it, parity));
+      DPE_TIMED(ctx, KID_STRONG_UPDATE, s, launch_strong_update(staging, a.gn != 0, hg, s, d_args, it, parity));
       PM_LAUNCHED("k_strong_update", s);
     }
     DPE_TIMED(ctx, KID_RANSAC, s, k_ransac_fit_plane<<<fg, kFullBlock, 0, s>>>(d_args));
     PM_LAUNCHED("k_ransac_fit_plane", s);
     if (a.P.use_APD)
       for (int parity = 0; parity < 2; ++parity) {
-        DPE_TIMED(ctx, KID_WEAK_UPDATE, s, k_weak_update<<<hg, kHalfBlock, 0, s>>>(d_args, it, parity));
-        PM_LAUNCHED("k_weak_update", s);
+        const unsigned gp = list_grid(ctx, (long long)wcap);
+        const unsigned ge = list_grid(ctx, (long long)wcap * 10 * (N - 1));
+        DPE_TIMED(ctx, KID_WEAK_PREPARE, s, k_weak_prepare<<<gp, 128, 0, s>>>(d_args, parity));
+        PM_LAUNCHED("k_weak_prepare", s);
+        DPE_TIMED(ctx, KID_WEAK_EVAL, s, with_stage(staging, [&](auto st) { k_weak_eval<false, decltype(st)::value><<<ge, 128, 0, s>>>(d_args, parity); }));
+        PM_LAUNCHED("k_weak_eval", s);
+        DPE_TIMED(ctx, KID_WEAK_DECIDE, s, k_weak_decide<<<gp, 128, 0, s>>>(d_args, it, parity));
+        PM_LAUNCHED("k_weak_decide", s);
+        DPE_TIMED(ctx, KID_WEAK_EVAL, s, with_stage(staging, [&](auto st) { k_weak_eval<true, decltype(st)::value><<<ge, 128, 0, s>>>(d_args, parity); }));
+        PM_LAUNCHED("k_weak_eval", s);
+        DPE_TIMED(ctx, KID_WEAK_FINISH, s, with_stage(staging, [&](auto st) { k_weak_finish<decltype(st)::value><<<gp, 128, 0, s>>>(d_args, parity); }));
+        PM_LAUNCHED("k_weak_finish", s);
       }
   }
   DPE_TIMED(ctx, KID_DEPTH_NORMAL, s, k_get_depth_normal<<<fg, kFullBlock, 0, s>>>(d_args));
@@ -387,9 +480,9 @@ extern "C" int dpe_pm_run(dpe_ctx *ctx, const dpe_problem *p, dpe_pm_out *out) {
     DPE_TIMED(ctx, KID_FILTER, s, k_filter_strong<<<hg, kHalfBlock, 0, s>>>(d_args, parity));
     PM_LAUNCHED("k_filter_strong", s);
   }
-  DPE_TIMED(ctx, KID_DEPTH_TO_WEAK, s, k_depth_to_weak<<<fg, kFullBlock, 0, s>>>(d_args, a.weak));
+  DPE_TIMED(ctx, KID_DEPTH_TO_WEAK, s, with_stage(staging, [&](auto st) { k_depth_to_weak<decltype(st)::value><<<fg, kFullBlock, 0, s>>>(d_args, a.weak); }));
   PM_LAUNCHED("k_depth_to_weak", s);
-  DPE_TIMED(ctx, KID_LOCAL_REFINE, s, k_local_refine<<<fg, kFullBlock, 0, s>>>(d_args));
+  DPE_TIMED(ctx, KID_LOCAL_REFINE, s, with_stage(staging, [&](auto st) { k_local_refine<decltype(st)::value><<<fg, kFullBlock, 0, s>>>(d_args); }));
   PM_LAUNCHED("k_local_refine", s);
   DPE_TRY(cudaEventRecord(ctx->ev1, s));
 
@@ -438,17 +531,29 @@ __global__ void k_ncc_queries(const PMArgs *__restrict__ pa, int64_t n, const in
 }
 }  // namespace
 
-extern "C" int dpe_ncc_eval(dpe_ctx *ctx, const dpe_ncc_query *q, float *costs_out) {
-  if (!ctx || !q || !costs_out || q->count < 0) return DPE_ERR_INVALID_ARGUMENT;
+namespace {
+// Host-side checks and the upload shared by the NCC query entry points: padded images, the
+// argument block and the query arrays in the context's arena.
+struct QueryUpload {
+  PMArgs *d_args = nullptr;
+  int32_t *px = nullptr, *py = nullptr, *src = nullptr;
+  float4 *plane = nullptr;
+};
+int check_queries(const dpe_ncc_query *q) {
+  if (!q || q->count < 0) return DPE_ERR_INVALID_ARGUMENT;
   if (q->num_images < 2 || q->num_images > DPE_MAX_IMAGES || q->width < 16 || q->height < 16) return DPE_ERR_INVALID_ARGUMENT;
-  if ((2 * q->params.strong_radius) / q->params.strong_increment + 1 > kMaxWin) return DPE_ERR_INVALID_ARGUMENT;
-  const int W = q->width, H = q->height, N = q->num_images;
+  if (q->params.strong_increment <= 0 || q->params.strong_radius < 0 ||
+      (2 * q->params.strong_radius) / q->params.strong_increment + 1 > kMaxWin)
+    return DPE_ERR_INVALID_ARGUMENT;
   for (int64_t k = 0; k < q->count; ++k)
-    if (q->src[k] < 1 || q->src[k] >= N || q->px[k] < 0 || q->px[k] >= W || q->py[k] < 0 || q->py[k] >= H)
+    if (q->src[k] < 1 || q->src[k] >= q->num_images || q->px[k] < 0 || q->px[k] >= q->width || q->py[k] < 0 ||
+        q->py[k] >= q->height)
       return DPE_ERR_INVALID_ARGUMENT;
-  if (q->count == 0) return DPE_OK;
-  DPE_TRY(cudaSetDevice(ctx->device));
+  return DPE_OK;
+}
+int upload_queries(dpe_ctx *ctx, const dpe_ncc_query *q, QueryUpload *u) {
   cudaStream_t s = ctx->stream;
+  const int W = q->width, H = q->height, N = q->num_images;
   const size_t L = (size_t)W * H, PL = (size_t)(W + 2) * (H + 2);
   Arena &A = ctx->arena;
   PMArgs a;
@@ -461,9 +566,11 @@ extern "C" int dpe_ncc_eval(dpe_ctx *ctx, const dpe_ncc_query *q, float *costs_o
   float *img_pad = A.get<float>("img_pad", PL * N);
   float *stage = A.get<float>("img_stage", L * N);
   const int64_t n = q->count;
-  int32_t *dpx = A.get<int32_t>("q_px", n), *dpy = A.get<int32_t>("q_py", n), *dsrc = A.get<int32_t>("q_src", n);
-  float4 *dpl = A.get<float4>("q_plane", n);
-  float *dout = A.get<float>("q_out", n);
+  u->px = A.get<int32_t>("q_px", n);
+  u->py = A.get<int32_t>("q_py", n);
+  u->src = A.get<int32_t>("q_src", n);
+  u->plane = A.get<float4>("q_plane", n);
+  u->d_args = A.get<PMArgs>("pm_args", 1);
   if (!A.ok()) return DPE_ERR_OUT_OF_MEMORY;
   for (int i = 0; i < N; ++i) {
     DPE_TRY(cudaMemcpyAsync(stage + L * i, q->images[i], L * 4, cudaMemcpyHostToDevice, s));
@@ -471,16 +578,85 @@ extern "C" int dpe_ncc_eval(dpe_ctx *ctx, const dpe_ncc_query *q, float *costs_o
     k_pad_image<<<dim3((W + 2 + 31) / 32, (H + 2 + 7) / 8), dim3(32, 8), 0, s>>>(stage + L * i, img_pad + PL * i, W, H);
     PM_LAUNCHED("k_pad_image", s);
   }
-  DPE_TRY(cudaMemcpyAsync(dpx, q->px, n * 4, cudaMemcpyHostToDevice, s));
-  DPE_TRY(cudaMemcpyAsync(dpy, q->py, n * 4, cudaMemcpyHostToDevice, s));
-  DPE_TRY(cudaMemcpyAsync(dsrc, q->src, n * 4, cudaMemcpyHostToDevice, s));
-  DPE_TRY(cudaMemcpyAsync(dpl, q->plane, n * 16, cudaMemcpyHostToDevice, s));
-  PMArgs *d_args = A.get<PMArgs>("pm_args", 1);
-  if (!d_args) return DPE_ERR_OUT_OF_MEMORY;
-  DPE_TRY(cudaMemcpyAsync(d_args, &a, sizeof(PMArgs), cudaMemcpyHostToDevice, s));
-  DPE_TIMED(ctx, KID_NCC_QUERY, s, k_ncc_queries<false><<<(unsigned)((n + 127) / 128), 128, 0, s>>>(d_args, n, dpx, dpy, dsrc, dpl, dout));
+  DPE_TRY(cudaMemcpyAsync(u->px, q->px, n * 4, cudaMemcpyHostToDevice, s));
+  DPE_TRY(cudaMemcpyAsync(u->py, q->py, n * 4, cudaMemcpyHostToDevice, s));
+  DPE_TRY(cudaMemcpyAsync(u->src, q->src, n * 4, cudaMemcpyHostToDevice, s));
+  DPE_TRY(cudaMemcpyAsync(u->plane, q->plane, n * 16, cudaMemcpyHostToDevice, s));
+  DPE_TRY(cudaMemcpyAsync(u->d_args, &a, sizeof(PMArgs), cudaMemcpyHostToDevice, s));
+  return DPE_OK;
+}
+
+// Cost and gradients of each query (the adjoint of k_ncc_queries).  gdn: dC/d(depth, nx, ny, nz)
+// with the depth at the pixel held instead of the plane offset w = -depth * (n . ray).
+__global__ void k_ncc_grad(const PMArgs *__restrict__ pa, int64_t n, const int32_t *px, const int32_t *py,
+                           const int32_t *src, const float4 *pl, float *cost, float4 *gplane, float4 *gdn,
+                           float *gimg) {
+  const PMArgs &a = *pa;
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  RefWindow rw;
+  build_ref_window(a, px[k], py[k], rw, KID_NCC_QUERY);
+  float g[4];
+  const int s = src[k];
+  const float4 p = pl[k];
+  cost[k] = ncc_strong_adjoint(a, px[k], py[k], s, p, rw, g, gimg ? gimg + (size_t)(s - 1) * a.W * a.H : nullptr);
+  gplane[k] = make_float4(g[0], g[1], g[2], g[3]);
+  // w = -depth * (n . ray), ray = Kr^-1 (x, y, 1): dC/ddepth = g_w * -(n . ray); dC/dn|depth = g_n + g_w * -depth * ray
+  const dpe_camera &c = a.cam[0];
+  const float ray[3] = {((float)px[k] - c.K[2]) / c.K[0], ((float)py[k] - c.K[5]) / c.K[4], 1.0f};
+  const float nr = p.x * ray[0] + p.y * ray[1] + p.z * ray[2];
+  const float depth = nr != 0.0f ? -p.w / nr : 0.0f;
+  gdn[k] = make_float4(-g[3] * nr, g[0] - g[3] * depth * ray[0], g[1] - g[3] * depth * ray[1], g[2] - g[3] * depth * ray[2]);
+}
+}  // namespace
+
+extern "C" int dpe_ncc_eval(dpe_ctx *ctx, const dpe_ncc_query *q, float *costs_out) {
+  if (!ctx || !costs_out) return DPE_ERR_INVALID_ARGUMENT;
+  int st = check_queries(q);
+  if (st) return st;
+  if (q->count == 0) return DPE_OK;
+  DPE_TRY(cudaSetDevice(ctx->device));
+  cudaStream_t s = ctx->stream;
+  QueryUpload u;
+  if ((st = upload_queries(ctx, q, &u))) return st;
+  const int64_t n = q->count;
+  float *dout = ctx->arena.get<float>("q_out", n);
+  if (!dout) return DPE_ERR_OUT_OF_MEMORY;
+  DPE_TIMED(ctx, KID_NCC_QUERY, s, k_ncc_queries<false><<<(unsigned)((n + 127) / 128), 128, 0, s>>>(u.d_args, n, u.px, u.py, u.src, u.plane, dout));
   PM_LAUNCHED("k_ncc_queries", s);
   DPE_TRY(cudaMemcpyAsync(costs_out, dout, n * 4, cudaMemcpyDeviceToHost, s));
+  DPE_TRY(cudaStreamSynchronize(s));
+  ctx->collect();
+  return DPE_OK;
+}
+
+extern "C" int dpe_ncc_grad(dpe_ctx *ctx, const dpe_ncc_query *q, float *costs_out, float *grad_plane_out,
+                            float *grad_depth_normal_out, float *const *grad_images_out) {
+  if (!ctx || !costs_out || !grad_plane_out) return DPE_ERR_INVALID_ARGUMENT;
+  int st = check_queries(q);
+  if (st) return st;
+  if (q->count == 0) return DPE_OK;
+  DPE_TRY(cudaSetDevice(ctx->device));
+  cudaStream_t s = ctx->stream;
+  QueryUpload u;
+  if ((st = upload_queries(ctx, q, &u))) return st;
+  const int64_t n = q->count;
+  const size_t L = (size_t)q->width * q->height;
+  Arena &A = ctx->arena;
+  float *dcost = A.get<float>("q_out", n);
+  float4 *dgp = A.get<float4>("q_gplane", n), *dgd = A.get<float4>("q_gdn", n);
+  float *dgimg = grad_images_out ? A.get<float>("q_gimg", L * (q->num_images - 1)) : nullptr;
+  if (!A.ok()) return DPE_ERR_OUT_OF_MEMORY;
+  if (dgimg) DPE_TRY(cudaMemsetAsync(dgimg, 0, L * (q->num_images - 1) * 4, s));
+  DPE_TIMED(ctx, KID_NCC_QUERY, s, k_ncc_grad<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(u.d_args, n, u.px, u.py, u.src, u.plane, dcost, dgp, dgd, dgimg));
+  PM_LAUNCHED("k_ncc_grad", s);
+  DPE_TRY(cudaMemcpyAsync(costs_out, dcost, n * 4, cudaMemcpyDeviceToHost, s));
+  DPE_TRY(cudaMemcpyAsync(grad_plane_out, dgp, n * 16, cudaMemcpyDeviceToHost, s));
+  if (grad_depth_normal_out) DPE_TRY(cudaMemcpyAsync(grad_depth_normal_out, dgd, n * 16, cudaMemcpyDeviceToHost, s));
+  if (dgimg)
+    for (int i = 1; i < q->num_images; ++i)
+      if (grad_images_out[i])
+        DPE_TRY(cudaMemcpyAsync(grad_images_out[i], dgimg + L * (i - 1), L * 4, cudaMemcpyDeviceToHost, s));
   DPE_TRY(cudaStreamSynchronize(s));
   ctx->collect();
   return DPE_OK;
@@ -507,13 +683,16 @@ extern "C" int dpe_kernel_info(char *buf, int len) {
   add("k_gen_edge_inform", (const void *)k_gen_edge_inform);
   add("k_find_nearest_strong", (const void *)k_find_nearest_strong);
   add("k_gen_neighbours", (const void *)k_gen_neighbours);
-  add("k_random_init", (const void *)k_random_init);
-  add("k_strong_update", (const void *)k_strong_update);
+  add("k_random_init", (const void *)k_random_init<DPE_STAGE_FP32>);
+  add("k_strong_update", (const void *)k_strong_update<DPE_STAGE_FP32, false>);
   add("k_ransac_fit_plane", (const void *)k_ransac_fit_plane);
-  add("k_weak_update", (const void *)k_weak_update);
+  add("k_weak_prepare", (const void *)k_weak_prepare);
+  add("k_weak_eval", (const void *)k_weak_eval<false, DPE_STAGE_FP32>);
+  add("k_weak_decide", (const void *)k_weak_decide);
+  add("k_weak_finish", (const void *)k_weak_finish<DPE_STAGE_FP32>);
   add("k_filter_strong", (const void *)k_filter_strong);
-  add("k_depth_to_weak", (const void *)k_depth_to_weak);
-  add("k_local_refine", (const void *)k_local_refine);
+  add("k_depth_to_weak", (const void *)k_depth_to_weak<DPE_STAGE_FP32>);
+  add("k_local_refine", (const void *)k_local_refine<DPE_STAGE_FP32>);
   size_t stack = 0;
   cudaDeviceGetLimit(&stack, cudaLimitStackSize);
   char line[96];
@@ -599,6 +778,15 @@ extern "C" int dpe_ncc_eval_noalloc(const dpe_ncc_query *q, float *costs_out, vo
 }
 
 // ------------------------------------------------------------------ statistics
+extern "C" int dpe_ctx_set_options(dpe_ctx *ctx, const dpe_options *opt) {
+  if (!ctx || !opt) return DPE_ERR_INVALID_ARGUMENT;
+  if (opt->staging != DPE_STAGE_FP32 && opt->staging != DPE_STAGE_FP16 && opt->staging != DPE_STAGE_BF16)
+    return DPE_ERR_INVALID_ARGUMENT;
+  if (opt->gn_refine != 0 && opt->gn_refine != 1) return DPE_ERR_INVALID_ARGUMENT;
+  ctx->opt = *opt;
+  return DPE_OK;
+}
+
 extern "C" int dpe_ctx_set_profiling(dpe_ctx *ctx, int on) {
   if (!ctx) return DPE_ERR_INVALID_ARGUMENT;
   ctx->profile = on != 0;

@@ -89,6 +89,8 @@ class Arena {
 
 struct dpe_ctx {
   int device = 0;
+  int sms = 148;  // multiprocessors of the device: grid size of the work-list kernels
+  dpe_options opt = {DPE_STAGE_FP32, 0};
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   bool count_evals = false;

@@ -7,6 +7,8 @@
 
 #include <cfloat>
 #include <cstdint>
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include "../../include/dpe_b200.h"
@@ -29,6 +31,11 @@ struct PMArgs {
   float trel[kMaxImages][3];  // source translation relative to the reference (DPE.cu:480-485)
   uint32_t key[2];
   const float *img[kMaxImages];  // padded (W+2)*(H+2) float images
+  // Staged source images (dpe_options::staging FP16 / BF16): pair[s][o] holds the padded texels
+  // P[o] and P[o+1] as two 16-bit values in one 32-bit word, so a bilinear footprint is two loads.
+  const uint32_t *pair[kMaxImages];
+  int stage;  // DPE_STAGE_*: storage the cost kernels sample the source images from
+  int gn;     // 1: Gauss-Newton plane hypothesis in the strong update (dpe_options::gn_refine)
   const float *dep[kMaxImages];  // W*H depth maps (geom consistency)
   // state
   float4 *plane;
@@ -52,6 +59,21 @@ struct PMArgs {
   short2 *edge_neigh;
   short2 *nearest;
   unsigned long long *counters;  // per kernel class: [2k] strong NCC evals, [2k+1] weak (counting runs)
+  // Weak-texture pass.  The WEAK pixels of each colour are listed once per call (wlist, wcount,
+  // raster order); a listed pixel's position in its list is its slot in the scratch below, which
+  // every colour pass reuses.
+  const int *wlist[2];
+  const int *wcount;  // [2]
+  int wtab_stride;    // table entries per slot: kMaxWin^2 for the centre window + 8 deformable windows
+  int wtaps;          // taps of one deformable window
+  float2 *wtab;       // [slot][tap] bilateral weight w and w * (r - c) of every window tap
+  float4 *wwin;       // [slot][9] reference sums (s_w, s_r, s_rr) of each window
+  float *wcost;       // [slot][10][N-1] deformable NCC: 8 candidates, the current plane, the fit plane
+  float *wgeom;       // [slot][10][N-1] geometric cost of the same hypotheses
+  float4 *whyp;       // [slot][5] random refinement hypotheses
+  float *wcost_r;     // [slot][5][N-1] deformable NCC of the random hypotheses
+  float *wgeom_r;     // [slot][5][N-1] geometric cost of the random hypotheses
+  float4 *wstate;     // [slot][2] plane after the candidate and fit-plane steps; (depth, cost, cost0, wn)
 };
 
 // Relative pose of source s with respect to the reference, computed once per call on the host
@@ -162,6 +184,82 @@ __device__ __forceinline__ float bilinear(const float *__restrict__ img, int pad
   const float bot = (1.0f - ax) * v01 + ax * v11;
   return (1.0f - ay) * top + ay * bot;
 }
+// ------------------------------------------------------------------ source samplers
+// A source image as the cost kernels sample it.  fetch(o) returns the 2x2 texel footprint of
+// padded offset o, (P[o], P[o+1], P[o+pw], P[o+pw+1]), in FP32; the interpolation is shared, so
+// samplers differ only in storage.  FP32 samples equal bilinear() above exactly.
+struct SrcF32 {
+  const float *p;
+  int pw;
+  long long n;
+  __device__ __forceinline__ float4 fetch(int o) const {
+    return make_float4(img_ld(p, o, n, 102), img_ld(p, o + 1, n, 103), img_ld(p, o + pw, n, 104),
+                       img_ld(p, o + pw + 1, n, 105));
+  }
+};
+__device__ __forceinline__ uint32_t pair_ld(const uint32_t *p, long long off, long long n, int tag) {
+#ifdef DPE_CHECKED
+  return *dpe_chk(p, off, n, tag);
+#else
+  return __ldg(p + off);
+#endif
+}
+// FP16 pairs: low half P[o], high half P[o+1].
+struct SrcF16 {
+  const uint32_t *p;
+  int pw;
+  long long n;
+  __device__ __forceinline__ float4 fetch(int o) const {
+    const uint32_t t = pair_ld(p, o, n, 108), b = pair_ld(p, o + pw, n, 109);
+    return make_float4(__half2float(__ushort_as_half((unsigned short)(t & 0xFFFFu))),
+                       __half2float(__ushort_as_half((unsigned short)(t >> 16))),
+                       __half2float(__ushort_as_half((unsigned short)(b & 0xFFFFu))),
+                       __half2float(__ushort_as_half((unsigned short)(b >> 16))));
+  }
+};
+// BF16 pairs: a bfloat16 is the top half of an FP32 word, so widening is a shift.
+struct SrcBF16 {
+  const uint32_t *p;
+  int pw;
+  long long n;
+  __device__ __forceinline__ float4 fetch(int o) const {
+    const uint32_t t = pair_ld(p, o, n, 110), b = pair_ld(p, o + pw, n, 111);
+    return make_float4(__uint_as_float(t << 16), __uint_as_float(t & 0xFFFF0000u), __uint_as_float(b << 16),
+                       __uint_as_float(b & 0xFFFF0000u));
+  }
+};
+template <class Src>
+__device__ __forceinline__ float bilinear_s(const Src &src, int W, int H, float x, float y) {
+  const float xc = fminf(fmaxf(x, -1.0f), (float)(W - 1));
+  const float yc = fminf(fmaxf(y, -1.0f), (float)(H - 1));
+  const float fx = floorf(xc), fy = floorf(yc);
+  const float ax = xc - fx, ay = yc - fy;
+  const float4 v = src.fetch(((int)fy + 1) * src.pw + ((int)fx + 1));
+  const float top = (1.0f - ax) * v.x + ax * v.y;
+  const float bot = (1.0f - ax) * v.z + ax * v.w;
+  return (1.0f - ay) * top + ay * bot;
+}
+__device__ __forceinline__ SrcF32 src_f32(const PMArgs &a, int s) {
+  return SrcF32{a.img[s], a.pad_w, (long long)a.pad_w * (a.H + 2)};
+}
+__device__ __forceinline__ SrcF16 src_f16(const PMArgs &a, int s) {
+  return SrcF16{a.pair[s], a.pad_w, (long long)a.pad_w * (a.H + 2)};
+}
+__device__ __forceinline__ SrcBF16 src_bf16(const PMArgs &a, int s) {
+  return SrcBF16{a.pair[s], a.pad_w, (long long)a.pad_w * (a.H + 2)};
+}
+// The sampler of a staging (DPE_STAGE_*), chosen at compile time: each cost kernel is built once
+// per staging, so a kernel carries only its own tap loop.
+template <int kStage> struct SrcOf;
+template <> struct SrcOf<DPE_STAGE_FP32> {
+  static __device__ __forceinline__ SrcF32 make(const PMArgs &a, int s) { return src_f32(a, s); }
+};
+template <> struct SrcOf<DPE_STAGE_FP16> {
+  static __device__ __forceinline__ SrcF16 make(const PMArgs &a, int s) { return src_f16(a, s); }
+};
+template <> struct SrcOf<DPE_STAGE_BF16> {
+  static __device__ __forceinline__ SrcBF16 make(const PMArgs &a, int s) { return src_bf16(a, s); }
+};
 
 // ------------------------------------------------------------------ geometry (DPE.cu:313-546)
 __device__ __forceinline__ void point3d(const dpe_camera &c, int x, int y, float depth, float X[3]) {
@@ -317,16 +415,12 @@ __device__ __forceinline__ void build_ref_window(const PMArgs &a, int px, int py
   rw.var_r = swrr * rw.inv_wsum - rw.mean_r * rw.mean_r;
 }
 
-// ComputeBilateralNCCOld (DPE.cu:696-782) with the reference window precomputed.
-__device__ __forceinline__ float ncc_strong(const PMArgs &a, int px, int py, int s, float4 pl, const RefWindow &rw) {
-  float H[9];
-  homography(a, s, pl, H);
-  const float2 pt = project(H, px, py);
-  const dpe_camera &sc = a.cam[s];
-  if (pt.x >= sc.width || pt.x < 0.0f || pt.y >= sc.height || pt.y < 0.0f) return 2.0f;
-  if (rw.cnt) atomicAdd(rw.cnt, 1ull);
+// ComputeBilateralNCCOld (DPE.cu:696-782) with the reference window precomputed; the window loop
+// for one source sampler.
+template <class Src>
+__device__ __forceinline__ float ncc_strong_src(const PMArgs &a, int px, int py, const float H[9], const Src &src,
+                                                const RefWindow &rw) {
   const int r = a.P.strong_radius, inc = a.P.strong_increment;
-  const float *__restrict__ img = a.img[s];
   float s_s = 0.f, s_ss = 0.f, s_rs = 0.f;
   int k = 0;
   for (int i = -r; i <= r; i += inc) {
@@ -337,7 +431,7 @@ __device__ __forceinline__ float ncc_strong(const PMArgs &a, int px, int py, int
       const float y = (float)(py + j);
       const float X = H[1] * y + bx, Y = H[4] * y + by, Z = H[7] * y + bz;
       const float iz = 1.0f / Z;
-      const float sv = bilinear(img, a.pad_w, a.W, a.H, X * iz, Y * iz) - rw.center;
+      const float sv = bilinear_s(src, a.W, a.H, X * iz, Y * iz) - rw.center;
       const float ws = G(rw.w, k, kMaxWin * kMaxWin, 322) * sv;
       s_s += ws;
       s_ss += ws * sv;
@@ -351,26 +445,193 @@ __device__ __forceinline__ float ncc_strong(const PMArgs &a, int px, int py, int
   const float cov = s_rs * rw.inv_wsum - rw.mean_r * m_s;
   return fmaxf(0.0f, fminf(2.0f, 1.0f - cov / sqrtf(rw.var_r * var_s)));
 }
+template <int kStage = DPE_STAGE_FP32>
+__device__ __forceinline__ float ncc_strong(const PMArgs &a, int px, int py, int s, float4 pl, const RefWindow &rw) {
+  float H[9];
+  homography(a, s, pl, H);
+  const float2 pt = project(H, px, py);
+  const dpe_camera &sc = a.cam[s];
+  if (pt.x >= sc.width || pt.x < 0.0f || pt.y >= sc.height || pt.y < 0.0f) return 2.0f;
+  if (rw.cnt) atomicAdd(rw.cnt, 1ull);
+  return ncc_strong_src(a, px, py, H, SrcOf<kStage>::make(a, s), rw);
+}
 
-// Window NCC with the window built on the fly (deformable weak window, DPE.cu:628-672), with the
-// same compensated moments (shift by the reference centre value).
-__device__ __forceinline__ float window_ncc(const PMArgs &a, const float H[9], int s, int cx, int cy, int radius, int inc,
-                                            float ref_center) {
+// ------------------------------------------------------------------ strong NCC adjoint
+// Cost and gradient of the strong NCC with respect to the plane (nx, ny, nz, w), and optionally
+// with respect to the source image's pixels (accumulated into gimg, W*H, with atomics).  Two passes
+// over the window, the second recomputing the projections instead of storing the patch:
+//   pass 1: the moments and the cost, exactly as ncc_strong;
+//   pass 2: per tap, dC/ds (s = bilinear sample) from the moments, through the bilinear slope to
+//           the projected point, through the projection to the homography entries.
+// dC/dH then goes through H = K_s (R - t n^T / w) K_r^-1 to the plane.  Where the cost is the
+// constant 2 (centre outside the source, flat window) or clamped to [0, 2], the gradient is zero.
+__device__ __forceinline__ float ncc_strong_adjoint(const PMArgs &a, int px, int py, int s, float4 pl,
+                                                    const RefWindow &rw, float g[4], float *gimg) {
+  g[0] = g[1] = g[2] = g[3] = 0.0f;
+  float H[9];
+  homography(a, s, pl, H);
+  const float2 pt = project(H, px, py);
+  const dpe_camera &sc = a.cam[s];
+  if (pt.x >= sc.width || pt.x < 0.0f || pt.y >= sc.height || pt.y < 0.0f) return 2.0f;
+  const int r = a.P.strong_radius, inc = a.P.strong_increment;
   const float *__restrict__ img = a.img[s];
-  float s_r = 0, s_rr = 0, s_s = 0, s_ss = 0, s_rs = 0, s_w = 0;
-  for (int i = -radius; i <= radius; i += inc) {
-    float r_r = 0, r_rr = 0, r_s = 0, r_ss = 0, r_rs = 0, r_w = 0;
-    for (int j = -radius; j <= radius; j += inc) {
-      const int rx = cx + i, ry = cy + j;
-      const float rp = texel(a, 0, rx, ry);
-      const float2 sp = project(H, rx, ry);
-      const float sv = bilinear(img, a.pad_w, a.W, a.H, sp.x, sp.y) - ref_center;
-      const float w = bilateral_weight((float)i, (float)j, rp, ref_center, a.P.sigma_spatial, a.P.sigma_color);
-      const float rc = rp - ref_center;
-      r_r += w * rc; r_rr += w * rc * rc; r_s += w * sv; r_ss += w * sv * sv; r_rs += w * rc * sv; r_w += w;
+  float s_s = 0.f, s_ss = 0.f, s_rs = 0.f;
+  int k = 0;
+  for (int i = -r; i <= r; i += inc) {
+    const float x = (float)(px + i);
+    const float bx = H[0] * x + H[2], by = H[3] * x + H[5], bz = H[6] * x + H[8];
+    for (int j = -r; j <= r; j += inc) {
+      const float y = (float)(py + j);
+      const float X = H[1] * y + bx, Y = H[4] * y + by, Z = H[7] * y + bz;
+      const float iz = 1.0f / Z;
+      const float sv = bilinear(img, a.pad_w, a.W, a.H, X * iz, Y * iz) - rw.center;
+      const float ws = rw.w[k] * sv;
+      s_s += ws;
+      s_ss += ws * sv;
+      s_rs += rw.wr[k] * sv;
+      ++k;
     }
-    s_r += r_r; s_rr += r_rr; s_s += r_s; s_ss += r_ss; s_rs += r_rs; s_w += r_w;
   }
+  const float m_s = s_s * rw.inv_wsum;
+  const float var_s = s_ss * rw.inv_wsum - m_s * m_s;
+  if (rw.var_r < 1e-5f || var_s < 1e-5f) return 2.0f;
+  const float cov = s_rs * rw.inv_wsum - rw.mean_r * m_s;
+  const float sq = sqrtf(rw.var_r * var_s);
+  const float cost = 1.0f - cov / sq;
+  if (!(cost > 0.0f && cost < 2.0f)) return fmaxf(0.0f, fminf(2.0f, cost));
+  if (rw.cnt) atomicAdd(rw.cnt, 2ull);  // two passes over the window
+  // dC/ds_k = w_k / sum(w) * (-(r_k - mean_r) / sq + cov * (s_k - m_s) / (var_s * sq))
+  const float ka = -rw.inv_wsum / sq, kb = rw.inv_wsum * cov / (var_s * sq);
+  float gH[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  const int W = a.W, Hh = a.H, pw = a.pad_w;
+  k = 0;
+  for (int i = -r; i <= r; i += inc) {
+    const float x = (float)(px + i);
+    const float bx = H[0] * x + H[2], by = H[3] * x + H[5], bz = H[6] * x + H[8];
+    for (int j = -r; j <= r; j += inc) {
+      const float y = (float)(py + j);
+      const float X = H[1] * y + bx, Y = H[4] * y + by, Z = H[7] * y + bz;
+      const float iz = 1.0f / Z;
+      const float u = X * iz, v = Y * iz;
+      const float xc = fminf(fmaxf(u, -1.0f), (float)(W - 1)), yc = fminf(fmaxf(v, -1.0f), (float)(Hh - 1));
+      const float fx = floorf(xc), fy = floorf(yc);
+      const float ax = xc - fx, ay = yc - fy;
+      const int o = ((int)fy + 1) * pw + ((int)fx + 1);
+      const float v00 = img[o], v10 = img[o + 1], v01 = img[o + pw], v11 = img[o + pw + 1];
+      const float sv = (1.0f - ay) * ((1.0f - ax) * v00 + ax * v10) + ay * ((1.0f - ax) * v01 + ax * v11) - rw.center;
+      const float rc = texel(a, 0, px + i, py + j) - rw.center;  // r_k - c
+      const float dc = rw.w[k] * (ka * (rc - rw.mean_r) + kb * (sv - m_s));
+      // slope of the sample; zero along a clamped coordinate
+      const float dsx = (u > -1.0f && u < (float)(W - 1)) ? (1.0f - ay) * (v10 - v00) + ay * (v11 - v01) : 0.0f;
+      const float dsy = (v > -1.0f && v < (float)(Hh - 1)) ? (1.0f - ax) * (v01 - v00) + ax * (v11 - v10) : 0.0f;
+      const float gu = dc * dsx * iz, gv = dc * dsy * iz;
+      gH[0] += gu * x; gH[1] += gu * y; gH[2] += gu;
+      gH[3] += gv * x; gH[4] += gv * y; gH[5] += gv;
+      const float gz = -(gu * u + gv * v);
+      gH[6] += gz * x; gH[7] += gz * y; gH[8] += gz;
+      if (gimg) {
+        const int x0 = (int)fx, y0 = (int)fy;
+        const int xa = min(max(x0, 0), W - 1), xb = min(max(x0 + 1, 0), W - 1);
+        const int ya = min(max(y0, 0), Hh - 1), yb = min(max(y0 + 1, 0), Hh - 1);
+        atomicAdd(&gimg[(size_t)ya * W + xa], dc * (1.0f - ax) * (1.0f - ay));
+        atomicAdd(&gimg[(size_t)ya * W + xb], dc * ax * (1.0f - ay));
+        atomicAdd(&gimg[(size_t)yb * W + xa], dc * (1.0f - ax) * ay);
+        atomicAdd(&gimg[(size_t)yb * W + xb], dc * ax * ay);
+      }
+      ++k;
+    }
+  }
+  // H = Ks T, Ks = [[K0 0 K2] [0 K4 K5] [0 0 K8]]: gT = Ks^T gH
+  const dpe_camera &rc0 = a.cam[0];
+  float gT[9];
+  for (int b = 0; b < 3; ++b) {
+    gT[b] = sc.K[0] * gH[b];
+    gT[3 + b] = sc.K[4] * gH[3 + b];
+    gT[6 + b] = sc.K[2] * gH[b] + sc.K[5] * gH[3 + b] + sc.K[8] * gH[6 + b];
+  }
+  // T = M Kr^-1 (rows: T0 = M0 / f, T1 = M1 / fy, T2 = M2 - M0 cx / f - M1 cy / fy): gM
+  float gM[9];
+  for (int ra = 0; ra < 3; ++ra) {
+    gM[3 * ra] = (gT[3 * ra] - gT[3 * ra + 2] * rc0.K[2]) / rc0.K[0];
+    gM[3 * ra + 1] = (gT[3 * ra + 1] - gT[3 * ra + 2] * rc0.K[5]) / rc0.K[4];
+    gM[3 * ra + 2] = gT[3 * ra + 2];
+  }
+  // M = Rrel - t n^T / w
+  const float n3[3] = {pl.x, pl.y, pl.z};
+  const float *t = a.trel[s];
+  float gw = 0.0f;
+  for (int b = 0; b < 3; ++b) {
+    float gn = 0.0f;
+    for (int ra = 0; ra < 3; ++ra) {
+      gn += gM[3 * ra + b] * t[ra];
+      gw += gM[3 * ra + b] * t[ra] * n3[b];
+    }
+    g[b] = -gn / pl.w;
+  }
+  g[3] = gw / (pl.w * pl.w);
+  return cost;
+}
+
+// Strong costs of plane pl against every source: out[j] = cost against source j + 1.
+template <int kStage>
+__device__ __forceinline__ void ncc_all_sources(const PMArgs &a, int px, int py, float4 pl, const RefWindow &rw,
+                                                float *out) {
+  for (int j = 0; j < a.N - 1; ++j) out[j] = ncc_strong<kStage>(a, px, py, j + 1, pl, rw);
+}
+// Sum over the listed sources act[0..na) (ascending) of vw[j] * cost(j), in list order.
+template <int kStage>
+__device__ __forceinline__ float weighted_ncc(const PMArgs &a, int px, int py, float4 pl, const RefWindow &rw,
+                                             const int *act, int na, const uint8_t *vw) {
+  float tc = 0.0f;
+  for (int q = 0; q < na; ++q) tc += vw[act[q]] * ncc_strong<kStage>(a, px, py, act[q] + 1, pl, rw);
+  return tc;
+}
+
+__device__ __forceinline__ short2 neighbour(const PMArgs &a, int center, int k) {
+  return a.neigh[(size_t)a.nmap[center] * kNeighbours + k];
+}
+
+// ------------------------------------------------------------------ deformable (weak) NCC
+// ComputeBilateralNCCNew (DPE.cu:561-694): a centre window around the pixel plus eight small
+// windows around its stored strong neighbours, all compared through the same homography.  The
+// reference side of every window (bilateral weights, w * (r - c), the sums of w, w*(r-c) and
+// w*(r-c)^2) does not depend on the hypothesis; k_weak_prepare tabulates it once per pixel and
+// pass, and each evaluation reads the table.  Sums are accumulated in the same blocked order
+// (per window column, then over columns) in both places.
+
+// Window k's radius and step: the adaptive centre window (k = 0) or a fixed weak window.
+__device__ __forceinline__ void weak_window_shape(const PMArgs &a, int center, int k, int *radius, int *inc) {
+  int r = k == 0 ? a.P.strong_radius : a.P.weak_radius;
+  int s = k == 0 ? a.P.strong_increment : a.P.weak_increment;
+  if (a.P.use_radius && k == 0) {
+    r = a.radius[center];
+    s = cvmax(2, (int)(2.0 * r / 5.0));
+  }
+  *radius = r;
+  *inc = s;
+}
+__device__ __forceinline__ int weak_window_base(const PMArgs &a, int k) {
+  return k == 0 ? 0 : kMaxWin * kMaxWin + (k - 1) * a.wtaps;
+}
+
+// The hypothesis-dependent half of one window: sums of w*s, w*s^2, w*(r-c)*s over the taps.
+template <class Src>
+__device__ __forceinline__ float window_ncc_tab(const PMArgs &a, const float H[9], const Src &src, int cx, int cy,
+                                                int radius, int inc, float ref_center, const float2 *__restrict__ tab,
+                                                float4 win) {
+  float s_s = 0, s_ss = 0, s_rs = 0;
+  int t = 0;
+  for (int i = -radius; i <= radius; i += inc) {
+    float r_s = 0, r_ss = 0, r_rs = 0;
+    for (int j = -radius; j <= radius; j += inc) {
+      const float2 sp = project(H, cx + i, cy + j);
+      const float sv = bilinear_s(src, a.W, a.H, sp.x, sp.y) - ref_center;
+      const float2 e = tab[t++];
+      r_s += e.x * sv; r_ss += e.x * sv * sv; r_rs += e.y * sv;
+    }
+    s_s += r_s; s_ss += r_ss; s_rs += r_rs;
+  }
+  float s_w = win.x, s_r = win.y, s_rr = win.z;
   const float inv = 1.0f / s_w;
   s_r *= inv; s_rr *= inv; s_s *= inv; s_ss *= inv; s_rs *= inv;
   const float var_r = s_rr - s_r * s_r;
@@ -380,20 +641,18 @@ __device__ __forceinline__ float window_ncc(const PMArgs &a, const float H[9], i
   return fmaxf(0.0f, fminf(2.0f, 1.0f - cov / sqrtf(var_r * var_s)));
 }
 
-__device__ __forceinline__ short2 neighbour(const PMArgs &a, int center, int k) {
-  return a.neigh[(size_t)a.nmap[center] * kNeighbours + k];
-}
-
-// ComputeBilateralNCCNew (DPE.cu:561-694)
-__device__ __forceinline__ float ncc_weak(const PMArgs &a, int px, int py, int s, float4 pl) {
+// The deformable cost of hypothesis pl against source s for the pixel in `slot`.
+template <int kStage>
+__device__ __forceinline__ float ncc_weak_tab(const PMArgs &a, int slot, int center, int px, int py, int s, float4 pl,
+                                              int kid) {
   float H[9];
   homography(a, s, pl, H);
   const float2 pt = project(H, px, py);
   const dpe_camera &sc = a.cam[s];
   if (pt.x >= sc.width || pt.x < 0.0f || pt.y >= sc.height || pt.y < 0.0f) return 2.0f;
-  if (a.counters) atomicAdd(&a.counters[2 * KID_WEAK_UPDATE + 1], 1ull);
-  const int center = px + py * a.W;
+  if (a.counters) atomicAdd(&a.counters[2 * kid + 1], 1ull);
   const float ref_center = texel(a, 0, px, py);
+  const float2 *tab = a.wtab + (size_t)slot * a.wtab_stride;
   float center_cost = 0.0f, strong_cost = 0.0f;
   int strong_count = 0;
   for (int k = 0; k < kNeighbours; ++k) {
@@ -409,13 +668,11 @@ __device__ __forceinline__ float ncc_weak(const PMArgs &a, int px, int py, int s
       }
       return 2.0f;
     }
-    int radius = k == 0 ? a.P.strong_radius : a.P.weak_radius;
-    int inc = k == 0 ? a.P.strong_increment : a.P.weak_increment;
-    if (a.P.use_radius && k == 0) {
-      radius = a.radius[center];
-      inc = cvmax(2, (int)(2.0 * radius / 5.0));
-    }
-    const float t = window_ncc(a, H, s, nb.x, nb.y, radius, inc, ref_center);
+    int radius, inc;
+    weak_window_shape(a, center, k, &radius, &inc);
+    const float2 *wt = tab + weak_window_base(a, k);
+    const float4 win = a.wwin[(size_t)slot * kNeighbours + k];
+    const float t = window_ncc_tab(a, H, SrcOf<kStage>::make(a, s), nb.x, nb.y, radius, inc, ref_center, wt, win);
     if (k == 0) center_cost = t;
     else { strong_cost += t; strong_count++; }
   }

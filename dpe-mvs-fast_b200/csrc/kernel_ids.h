@@ -10,7 +10,10 @@ enum KernelId {
   KID_RANDOM_INIT,
   KID_STRONG_UPDATE,
   KID_RANSAC,
-  KID_WEAK_UPDATE,
+  KID_WEAK_PREPARE,
+  KID_WEAK_EVAL,
+  KID_WEAK_DECIDE,
+  KID_WEAK_FINISH,
   KID_DEPTH_NORMAL,
   KID_FILTER,
   KID_DEPTH_TO_WEAK,
@@ -26,6 +29,7 @@ enum KernelId {
 
 static const char *const kKernelNames[KID_COUNT] = {
     "k_init_state",    "k_gen_edge_inform", "k_find_nearest_strong", "k_gen_neighbours", "k_neighbour_update",
-    "k_random_init",   "k_strong_update",   "k_ransac_fit_plane",    "k_weak_update",    "k_get_depth_normal",
+    "k_random_init",   "k_strong_update",   "k_ransac_fit_plane",    "k_weak_prepare",   "k_weak_eval",
+    "k_weak_decide",   "k_weak_finish",     "k_get_depth_normal",
     "k_filter_strong", "k_depth_to_weak",   "k_local_refine",        "k_pad_image",      "k_ncc_queries",
     "k_fuse_entries",  "k_fuse_waves",      "k_fuse_emit",           "k_scene_misc"};

@@ -44,6 +44,24 @@ __global__ void k_pad_image(const float *__restrict__ src, float *__restrict__ d
   dst[(size_t)(y + 1) * (W + 2) + (x + 1)] = src[(size_t)sy * W + sx];
 }
 
+// Staged copy of one padded source image (PMArgs::pair): word o packs P[o] (low 16 bits) and
+// P[o+1] (high 16 bits) as FP16 or BF16, rounded to nearest-even.  The last word repeats P[o].
+template <bool kBF16>
+__global__ void k_stage_pairs(const float *__restrict__ pad, uint32_t *__restrict__ out, long long n) {
+  const long long o = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (o >= n) return;
+  const float lo = pad[o], hi = pad[o + 1 < n ? o + 1 : o];
+  uint32_t a, b;
+  if (kBF16) {
+    a = __bfloat16_as_ushort(__float2bfloat16_rn(lo));
+    b = __bfloat16_as_ushort(__float2bfloat16_rn(hi));
+  } else {
+    a = __half_as_ushort(__float2half_rn(lo));
+    b = __half_as_ushort(__float2half_rn(hi));
+  }
+  out[o] = a | (b << 16);
+}
+
 __global__ void k_init_state(const PMArgs *__restrict__ pa, const float4 *plane_in, const uint32_t *views_in,
                              const uint8_t *weak_in, int *weak_flag) {
   const PMArgs &a = *pa;
@@ -449,6 +467,7 @@ __global__ void k_neighbour_update(const PMArgs *__restrict__ pa) {
 }
 
 // ------------------------------------------------------------------ RandomInitialization (DPE.cu:1039-1067, 784-861)
+template <int kStage>
 __global__ void __launch_bounds__(128) k_random_init(const PMArgs *__restrict__ pa) {
   const PMArgs &a = *pa;
   int px, py;
@@ -467,9 +486,10 @@ __global__ void __launch_bounds__(128) k_random_init(const PMArgs *__restrict__ 
     a.plane[center] = pl;
     float cv[kMaxSrc], srt[kMaxSrc];
     int valid = 0;
+    ncc_all_sources<kStage>(a, px, py, pl, rw, cv);
     for (int i = 0; i < n; ++i) {
-      const float v = ncc_strong(a, px, py, i + 1, pl, rw);
-      cv[i] = v; srt[i] = v;
+      const float v = cv[i];
+      srt[i] = v;
       if (v < 2.0f) valid++;
     }
     sort_small(srt, n);
@@ -496,7 +516,7 @@ __global__ void __launch_bounds__(128) k_random_init(const PMArgs *__restrict__ 
     float cost = 0.0f;
     for (int i = 1; i < a.N; ++i) {
       if (isSet(views, i - 1)) {
-        const float v = ncc_strong(a, px, py, i, pl, rw);
+        const float v = ncc_strong<kStage>(a, px, py, i, pl, rw);
         if (v < 2.0f) { cnt++; cost += v; }
         else unSetBit(&views, i - 1);
       }
@@ -508,7 +528,8 @@ __global__ void __launch_bounds__(128) k_random_init(const PMArgs *__restrict__ 
 
 // ------------------------------------------------------------------ shared pieces of the propagation kernels
 // Multi-hypothesis joint view selection (DPE.cu:1551-1619 / 1714-1783).
-__device__ __forceinline__ float sample_views(const PMArgs &a, Rng &rng, int iter, const float (*cost_array)[kMaxSrc],
+// cost_array: 8 candidate rows of per-source costs, `stride` floats apart.
+__device__ __forceinline__ float sample_views(const PMArgs &a, Rng &rng, int iter, const float *cost_array, int stride,
                                               const float *priors, uint8_t *vw, uint32_t *temp_sel, float *probs) {
   const int n = a.N - 1;
   for (int i = 0; i < 32; ++i) vw[i] = 0;
@@ -519,7 +540,7 @@ __device__ __forceinline__ float sample_views(const PMArgs &a, Rng &rng, int ite
     int count_false = 0;
     float tmpw = 0;
     for (int j = 0; j < 8; ++j) {
-      const float v = cost_array[j][i];
+      const float v = cost_array[j * stride + i];
       if (v < thr) { tmpw += expf(v * v / (-0.18f)); count++; }
       if (v > 1.2f) count_false++;
     }
@@ -554,7 +575,71 @@ __device__ __forceinline__ int find_min_cost_index(const float *c, int n) {
   return idx;
 }
 
+// ------------------------------------------------------------------ Gauss-Newton plane hypothesis
+// The differentiation form's refinement step (no reference counterpart; dpe_options::gn_refine).
+// Around the current plane (n, depth) it takes the cost of each sampled source j and its gradient
+// (ncc_strong_adjoint) in the local parameters theta = (d depth, d a1, d a2), the normal tilted
+// within its tangent plane (n' = normalize(n + a1 e1 + a2 e2)), and solves the damped normal
+// equations  (J^T V J + lambda diag(J^T V J)) theta = -J^T V c  (V = the sample counts).  The
+// resulting plane is a hypothesis like the random ones: kept only when its cost is lower and its
+// depth lies in range.  It draws no random numbers, so the rest of the update is unchanged.
+template <int kStage>
+__device__ __forceinline__ void gn_hypothesis(const PMArgs &a, int px, int py, const RefWindow &rw, const int *act,
+                                              int na, const uint8_t *vw, float wn, float4 *pl_now, float *depth_now,
+                                              float *cost_now) {
+  const dpe_camera &rc = a.cam[0];
+  const float4 p = *pl_now;
+  const float ray0 = ((float)px - rc.K[2]) / rc.K[0], ray1 = ((float)py - rc.K[5]) / rc.K[4];
+  const float nr = p.x * ray0 + p.y * ray1 + p.z;
+  const float d0 = *depth_now;
+  // tangent basis of the normal
+  float e1x, e1y, e1z;
+  if (fabsf(p.x) < 0.9f) { e1x = 0.0f; e1y = p.z; e1z = -p.y; }  // n x (1, 0, 0)
+  else { e1x = -p.z; e1y = 0.0f; e1z = p.x; }                    // n x (0, 1, 0)
+  const float e1n = 1.0f / sqrtf(e1x * e1x + e1y * e1y + e1z * e1z);
+  e1x *= e1n; e1y *= e1n; e1z *= e1n;
+  const float e2x = p.y * e1z - p.z * e1y, e2y = p.z * e1x - p.x * e1z, e2z = p.x * e1y - p.y * e1x;
+  const float e1r = e1x * ray0 + e1y * ray1 + e1z, e2r = e2x * ray0 + e2y * ray1 + e2z;
+  float A00 = 0, A01 = 0, A02 = 0, A11 = 0, A12 = 0, A22 = 0, b0 = 0, b1 = 0, b2 = 0;
+  for (int q = 0; q < na; ++q) {
+    const int j = act[q];
+    float g[4];
+    const float c = ncc_strong_adjoint(a, px, py, j + 1, p, rw, g, nullptr);
+    if (!(c > 0.0f && c < 2.0f)) continue;
+    // w = -depth (n . ray): dC/ddepth = g_w (-(n . ray)); tilting n moves w by -depth (e . ray)
+    const float jd = -g[3] * nr;
+    const float j1 = g[0] * e1x + g[1] * e1y + g[2] * e1z - g[3] * d0 * e1r;
+    const float j2 = g[0] * e2x + g[1] * e2y + g[2] * e2z - g[3] * d0 * e2r;
+    const float v = (float)vw[j];
+    A00 += v * jd * jd; A01 += v * jd * j1; A02 += v * jd * j2;
+    A11 += v * j1 * j1; A12 += v * j1 * j2; A22 += v * j2 * j2;
+    b0 -= v * jd * c; b1 -= v * j1 * c; b2 -= v * j2 * c;
+  }
+  const float lambda = 0.1f;
+  A00 *= 1.0f + lambda; A11 *= 1.0f + lambda; A22 *= 1.0f + lambda;
+  const float c00 = A11 * A22 - A12 * A12, c01 = A02 * A12 - A01 * A22, c02 = A01 * A12 - A02 * A11;
+  const float det = A00 * c00 + A01 * c01 + A02 * c02;
+  if (!(fabsf(det) > 1e-30f) || !isfinite(det)) return;
+  const float c11 = A00 * A22 - A02 * A02, c12 = A01 * A02 - A00 * A12, c22 = A00 * A11 - A01 * A01;
+  const float inv = 1.0f / det;
+  const float td = (c00 * b0 + c01 * b1 + c02 * b2) * inv;
+  const float t1 = (c01 * b0 + c11 * b1 + c12 * b2) * inv;
+  const float t2 = (c02 * b0 + c12 * b1 + c22 * b2) * inv;
+  float nx = p.x + t1 * e1x + t2 * e2x, ny = p.y + t1 * e1y + t2 * e2y, nz = p.z + t1 * e1z + t2 * e2z;
+  const float nn = 1.0f / sqrtf(nx * nx + ny * ny + nz * nz);
+  nx *= nn; ny *= nn; nz *= nn;
+  if (!(nx * ray0 + ny * ray1 + nz < 0.0f)) return;  // the plane must face the camera
+  const float dn = d0 + td;
+  if (!(dn >= a.P.depth_min && dn <= a.P.depth_max)) return;
+  float4 t = make_float4(nx, ny, nz, 0.0f);
+  t.w = dist_to_origin(rc, px, py, dn, t);
+  const float tc = weighted_ncc<kStage>(a, px, py, t, rw, act, na, vw) / wn;
+  const float db = depth_from_plane(rc, t, px, py);
+  if (db >= a.P.depth_min && db <= a.P.depth_max && tc < *cost_now) { *depth_now = db; *pl_now = t; *cost_now = tc; }
+}
+
 // ------------------------------------------------------------------ strong update (DPE.cu:1218-1670, 1069-1122)
+template <int kStage, bool kGN>
 __global__ void __launch_bounds__(128) k_strong_update(const PMArgs *__restrict__ pa, int iter, int parity) {
   const PMArgs &a = *pa;
   int px, py;
@@ -610,7 +695,7 @@ __global__ void __launch_bounds__(128) k_strong_update(const PMArgs *__restrict_
         flag[d] = true;
         positions[d] = mp;
         const float4 cp = G(cand_plane, mp, L, 205);
-        for (int j = 0; j < n; ++j) cost_array[d][j] = ncc_strong(a, px, py, j + 1, cp, rw);
+        ncc_all_sources<kStage>(a, px, py, cp, rw, cost_array[d]);
       }
     }
     if (!on_edge) {
@@ -634,7 +719,7 @@ __global__ void __launch_bounds__(128) k_strong_update(const PMArgs *__restrict_
           flag[d] = true;
           float tca[kMaxSrc];
           const float4 cp = G(cand_plane, mp, L, 205);
-          for (int j = 0; j < n; ++j) tca[j] = ncc_strong(a, px, py, j + 1, cp, rw);
+          ncc_all_sources<kStage>(a, px, py, cp, rw, tca);
           int g0 = 0, g1 = 0, b0 = 0, b1 = 0;
           for (int j = 0; j < n; ++j) {
             if (cost_array[d][j] < good_thr) g0++;
@@ -706,7 +791,7 @@ __global__ void __launch_bounds__(128) k_strong_update(const PMArgs *__restrict_
     for (int d = 0; d < 8; ++d) {
       if (!flag[d]) continue;
       const float4 cp = G(a.plane, positions[d], L, 210);
-      for (int j = 0; j < n; ++j) cost_array[d][j] = ncc_strong(a, px, py, j + 1, cp, rw);
+      ncc_all_sources<kStage>(a, px, py, cp, rw, cost_array[d]);
     }
   }
 #ifdef DPE_CHECKED
@@ -730,7 +815,7 @@ __global__ void __launch_bounds__(128) k_strong_update(const PMArgs *__restrict_
   Rng rng = make_rng(a, center);
   uint8_t vw[32];
   uint32_t temp_sel = 0;
-  const float wn = sample_views(a, rng, iter, cost_array, priors, vw, &temp_sel, probs);
+  const float wn = sample_views(a, rng, iter, &cost_array[0][0], kMaxSrc, priors, vw, &temp_sel, probs);
 #ifdef DPE_CHECKED
   for (int d = 0; d < 8; ++d)
     if (flag[d]) (void)G(a.plane, positions[d], L, 341 + d);
@@ -753,11 +838,12 @@ __global__ void __launch_bounds__(128) k_strong_update(const PMArgs *__restrict_
     if (flag[d]) (void)G(a.plane, positions[d], L, 301 + d);
 #endif
   const float4 pl_cur = G(a.plane, center, L, 212);
-  float cost_now = 0.0f;
-  for (int i = 0; i < n; ++i) {
-    // views with no samples contribute 0 * cost, and every cost is finite
-    if (vw[i] > 0) cost_now += vw[i] * ncc_strong(a, px, py, i + 1, pl_cur, rw);
-  }
+  // sampled sources in ascending order: views with no samples contribute 0 * (finite cost)
+  int act[kMaxSrc];
+  int na = 0;
+  for (int i = 0; i < n; ++i)
+    if (vw[i] > 0) act[na++] = i;
+  float cost_now = weighted_ncc<kStage>(a, px, py, pl_cur, rw, act, na, vw);
   cost_now /= wn;
   const float cost_written = cost_now;
   float depth_now = depth_from_plane(rc, pl_cur, px, py);
@@ -784,14 +870,13 @@ __global__ void __launch_bounds__(128) k_strong_update(const PMArgs *__restrict_
     for (int h = 0; h < 5; ++h) {
       float4 t = normals[h];
       t.w = dist_to_origin(rc, px, py, depths[h], t);
-      float tc = 0.0f;
-      for (int j = 0; j < n; ++j)
-        if (vw[j] > 0) tc += vw[j] * ncc_strong(a, px, py, j + 1, t, rw);
+      float tc = weighted_ncc<kStage>(a, px, py, t, rw, act, na, vw);
       tc /= wn;
       const float db = depth_from_plane(rc, t, px, py);
       if (db >= dmin && db <= dmax && tc < cost_now) { depth_now = db; pl_now = t; cost_now = tc; }
     }
   }
+  if (kGN && na > 0) gn_hypothesis<kStage>(a, px, py, rw, act, na, vw, wn, &pl_now, &depth_now, &cost_now);
   G(a.rng_ctr, center, L, 215) = rng.ctr;
   G(a.views, center, L, 216) = views_new;
   store_vweight(&G(a.vweight, center, L, 217), vw);
@@ -945,137 +1030,259 @@ __global__ void __launch_bounds__(128) k_ransac_fit_plane(const PMArgs *__restri
 }
 
 // ------------------------------------------------------------------ weak update (DPE.cu:1672-1866, 1124-1216)
-__device__ __forceinline__ void cost_vector_weak(const PMArgs &a, int px, int py, float4 pl, float *cv) {
-  for (int i = 1; i < a.N; ++i) cv[i - 1] = ncc_weak(a, px, py, i, pl);
+// CheckerboardPropagationWeak + PlaneHypothesisRefinementWeak for the WEAK pixels of one colour,
+// split into work lists so that every lane has work:
+//   k_weak_prepare      per pixel: the reference side of its nine windows (table, sums);
+//   k_weak_eval<false>  per (pixel, hypothesis, source): the 8 strong-neighbour candidates, the
+//                       current plane and the fitted plane;
+//   k_weak_decide       per pixel: view sampling, candidate choice, fitted-plane test, and the five
+//                       random refinement hypotheses (all random draws of the pixel);
+//   k_weak_eval<true>   per (pixel, random hypothesis, sampled source);
+//   k_weak_finish       per pixel: the random-hypothesis test, the REFINE_INIT rule, the write-back
+//                       and the final strong-window re-cost.
+// Each cost is the one the fused per-pixel form computes, and every sum runs in the same order.
+// Pixels of one colour read only STRONG neighbours and their own state, so the order of the
+// list does not matter.  Work items are strided over a grid sized for the GPU; the list lengths
+// stay on the device.
+
+__global__ void __launch_bounds__(128) k_weak_prepare(const PMArgs *__restrict__ pa, int parity) {
+  const PMArgs &a = *pa;
+  const int count = a.wcount[parity];
+  const int *list = a.wlist[parity];
+  for (int slot = blockIdx.x * blockDim.x + threadIdx.x; slot < count; slot += gridDim.x * blockDim.x) {
+    const int center = list[slot];
+    const int px = center % a.W, py = center / a.W;
+    const float ref_center = texel(a, 0, px, py);
+    float2 *tab = a.wtab + (size_t)slot * a.wtab_stride;
+    for (int k = 0; k < kNeighbours; ++k) {
+      const short2 nb = neighbour(a, center, k);
+      float4 win = make_float4(0, 0, 0, 0);
+      if (nb.x != -1 && nb.y != -1) {
+        int radius, inc;
+        weak_window_shape(a, center, k, &radius, &inc);
+        int t = weak_window_base(a, k);
+        float s_r = 0, s_rr = 0, s_w = 0;
+        for (int i = -radius; i <= radius; i += inc) {
+          float r_r = 0, r_rr = 0, r_w = 0;
+          for (int j = -radius; j <= radius; j += inc) {
+            const float rp = texel(a, 0, nb.x + i, nb.y + j);
+            const float w = bilateral_weight((float)i, (float)j, rp, ref_center, a.P.sigma_spatial, a.P.sigma_color);
+            const float rc = rp - ref_center;
+            tab[t++] = make_float2(w, w * rc);
+            r_r += w * rc; r_rr += w * rc * rc; r_w += w;
+          }
+          s_r += r_r; s_rr += r_rr; s_w += r_w;
+        }
+        win = make_float4(s_w, s_r, s_rr, 0.0f);
+      }
+      a.wwin[(size_t)slot * kNeighbours + k] = win;
+    }
+  }
 }
 
-__global__ void __launch_bounds__(128) k_weak_update(const PMArgs *__restrict__ pa, int iter, int parity) {
+// kRandom = false: hypotheses 0..7 are the candidates (the planes of the strong neighbours 1..8),
+// 8 the current plane, 9 the fitted plane.  kRandom = true: the five random hypotheses, for the
+// sources the pixel sampled.  Unevaluated candidates keep the fused form's initial costs (0, and 2
+// for the first candidate's first source: quirk Q2).
+template <bool kRandom, int kStage>
+__global__ void __launch_bounds__(128) k_weak_eval(const PMArgs *__restrict__ pa, int parity) {
   const PMArgs &a = *pa;
-  int px, py;
-  if (!colour_pixel(a, parity, &px, &py)) return;
-  const int W = a.W, n = a.N - 1;
-  const int center = py * W + px;
-  if (a.weak[center] != DPE_WEAK) return;
+  const int n = a.N - 1;
+  const int hyps = kRandom ? 5 : 10;
+  const long long per = (long long)hyps * n;
+  const long long total = (long long)a.wcount[parity] * per;
+  const int *list = a.wlist[parity];
+  const bool geom = a.P.geom_consistency != 0;
+  float *costs = kRandom ? a.wcost_r : a.wcost;
+  float *geoms = kRandom ? a.wgeom_r : a.wgeom;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int slot = (int)(t / per);
+    const int r = (int)(t - (long long)slot * per);
+    const int h = r / n, j = r - h * n;
+    const int center = list[slot];
+    const int px = center % a.W, py = center / a.W;
+    float4 pl;
+    if (kRandom) {
+      const float4 fp = a.fit_plane[center];
+      if (fp.x == 0 && fp.y == 0 && fp.z == 0) continue;  // no random refinement for this pixel
+      if (vweight_at(a.vweight[center], j) == 0) continue;
+      pl = a.whyp[(size_t)slot * 5 + h];
+    } else if (h < 8) {
+      const short2 nb = neighbour(a, center, h + 1);
+      if (nb.x == -1 || nb.y == -1 || a.weak[nb.x + nb.y * a.W] != DPE_STRONG) {
+        costs[t] = (h == 0 && j == 0) ? 2.0f : 0.0f;
+        geoms[t] = 0.0f;
+        continue;
+      }
+      pl = a.plane[nb.x + nb.y * a.W];
+    } else if (h == 8) {
+      pl = a.plane[center];
+    } else {
+      pl = a.fit_plane[center];
+      if (pl.x == 0 && pl.y == 0 && pl.z == 0) continue;  // unused: refinement skipped
+    }
+    costs[t] = ncc_weak_tab<kStage>(a, slot, center, px, py, j + 1, pl, KID_WEAK_EVAL);
+    geoms[t] = geom ? geom_cost(a, px, py, j + 1, pl) : 0.0f;
+  }
+}
+
+__global__ void __launch_bounds__(128) k_weak_decide(const PMArgs *__restrict__ pa, int iter, int parity) {
+  const PMArgs &a = *pa;
+  const int n = a.N - 1, W = a.W;
+  const int count = a.wcount[parity];
+  const int *list = a.wlist[parity];
   const dpe_camera &rc = a.cam[0];
   const bool geom = a.P.geom_consistency != 0;
   const float gf = a.P.geom_factor;
-  float cost_array[8][kMaxSrc];
-  for (int d = 0; d < 8; ++d)
-    for (int j = 0; j < n; ++j) cost_array[d][j] = 0.0f;
-  cost_array[0][0] = 2.0f;
+  const float dmin = a.P.depth_min, dmax = a.P.depth_max;
+  float priors[kMaxSrc], probs[kMaxSrc];
+  uint8_t vw[32];
+  float final_costs[8];
   bool flag[8];
   float4 cand[8];
-  for (int i = 0; i < 8; ++i) {
-    flag[i] = false;
-    cand[i] = make_float4(0, 0, 0, 0);
-    const short2 nb = neighbour(a, center, i + 1);
-    if (nb.x == -1 || nb.y == -1 || a.weak[nb.x + nb.y * W] != DPE_STRONG) continue;
-    flag[i] = true;
-    cand[i] = a.plane[nb.x + nb.y * W];
-    cost_vector_weak(a, px, py, cand[i], cost_array[i]);
-  }
-  float priors[kMaxSrc], probs[kMaxSrc];
-  for (int j = 0; j < n; ++j) priors[j] = 0.0f;
-  for (int i = 0; i < 8; ++i) {
-    const short2 nb = neighbour(a, center, i + 1);
-    if (nb.x == -1 || nb.y == -1) continue;
-    const uint32_t sv = a.views[nb.x + nb.y * W];
-    for (int j = 0; j < n; ++j) priors[j] += isSet(sv, j) == 1 ? 0.9f : 0.1f;
-  }
-  Rng rng = make_rng(a, center);
-  uint8_t vw[32];
-  uint32_t temp_sel = 0;
-  const float wn = sample_views(a, rng, iter, cost_array, priors, vw, &temp_sel, probs);
-  float final_costs[8];
-  for (int i = 0; i < 8; ++i) {
-    float fc = 0.0f;
-    for (int j = 0; j < n; ++j)
-      if (vw[j] > 0) {
-        if (geom) fc += vw[j] * (cost_array[i][j] + gf * (flag[i] ? geom_cost(a, px, py, j + 1, cand[i]) : 3.0f));
-        else fc += vw[j] * cost_array[i][j];
-      }
-    final_costs[i] = fc / wn;
-  }
-  const int mi = find_min_cost_index(final_costs, 8);
-  const float4 pl_cur = a.plane[center];
-  float cost_now = 0.0f;
-  for (int i = 0; i < n; ++i) {
-    if (vw[i] == 0) continue;  // 0 * (finite cost) contributes nothing
-    const float c = ncc_weak(a, px, py, i + 1, pl_cur);
-    if (geom) cost_now += vw[i] * (c + gf * geom_cost(a, px, py, i + 1, pl_cur));
-    else cost_now += vw[i] * c;
-  }
-  cost_now /= wn;
-  const float cost_written = cost_now;
-  float depth_now = depth_from_plane(rc, pl_cur, px, py);
-  float4 pl_now = pl_cur;
-  uint32_t views_new = a.views[center];
-  if (flag[mi]) {
-    const float db = depth_from_plane(rc, cand[mi], px, py);
-    if (db >= a.P.depth_min && db <= a.P.depth_max && final_costs[mi] < cost_now) {
-      depth_now = db; pl_now = cand[mi]; cost_now = final_costs[mi];
-      views_new = temp_sel;
+  for (int slot = blockIdx.x * blockDim.x + threadIdx.x; slot < count; slot += gridDim.x * blockDim.x) {
+    const int center = list[slot];
+    const int px = center % W, py = center / W;
+    const float *ca = a.wcost + (size_t)slot * 10 * n;
+    const float *ga = a.wgeom + (size_t)slot * 10 * n;
+    for (int i = 0; i < 8; ++i) {
+      const short2 nb = neighbour(a, center, i + 1);
+      flag[i] = !(nb.x == -1 || nb.y == -1 || a.weak[nb.x + nb.y * W] != DPE_STRONG);
+      cand[i] = flag[i] ? a.plane[nb.x + nb.y * W] : make_float4(0, 0, 0, 0);
     }
-  }
-  // PlaneHypothesisRefinementWeak: the fitted plane, then five random hypotheses.  A zero fitted
-  // plane ends the refinement before the random hypotheses (DPE.cu:1146-1148).
-  const float dmin = a.P.depth_min, dmax = a.P.depth_max;
-  const float4 fp = a.fit_plane[center];
-  const bool refine = !(fp.x == 0 && fp.y == 0 && fp.z == 0);
-  if (refine) {
-    {
+    for (int j = 0; j < n; ++j) priors[j] = 0.0f;
+    for (int i = 0; i < 8; ++i) {
+      const short2 nb = neighbour(a, center, i + 1);
+      if (nb.x == -1 || nb.y == -1) continue;
+      const uint32_t sv = a.views[nb.x + nb.y * W];
+      for (int j = 0; j < n; ++j) priors[j] += isSet(sv, j) == 1 ? 0.9f : 0.1f;
+    }
+    Rng rng = make_rng(a, center);
+    uint32_t temp_sel = 0;
+    const float wn = sample_views(a, rng, iter, ca, n, priors, vw, &temp_sel, probs);
+    for (int i = 0; i < 8; ++i) {
+      float fc = 0.0f;
+      for (int j = 0; j < n; ++j)
+        if (vw[j] > 0) {
+          if (geom) fc += vw[j] * (ca[i * n + j] + gf * (flag[i] ? ga[i * n + j] : 3.0f));
+          else fc += vw[j] * ca[i * n + j];
+        }
+      final_costs[i] = fc / wn;
+    }
+    const int mi = find_min_cost_index(final_costs, 8);
+    const float4 pl_cur = a.plane[center];
+    float cost_now = 0.0f;
+    for (int i = 0; i < n; ++i) {
+      if (vw[i] == 0) continue;  // 0 * (finite cost) contributes nothing
+      const float c = ca[8 * n + i];
+      if (geom) cost_now += vw[i] * (c + gf * ga[8 * n + i]);
+      else cost_now += vw[i] * c;
+    }
+    cost_now /= wn;
+    const float cost_written = cost_now;
+    float depth_now = depth_from_plane(rc, pl_cur, px, py);
+    float4 pl_now = pl_cur;
+    uint32_t views_new = a.views[center];
+    if (flag[mi]) {
+      const float db = depth_from_plane(rc, cand[mi], px, py);
+      if (db >= dmin && db <= dmax && final_costs[mi] < cost_now) {
+        depth_now = db; pl_now = cand[mi]; cost_now = final_costs[mi];
+        views_new = temp_sel;
+      }
+    }
+    // PlaneHypothesisRefinementWeak: the fitted plane, then five random hypotheses.  A zero fitted
+    // plane ends the refinement before the random hypotheses (DPE.cu:1146-1148).
+    const float4 fp = a.fit_plane[center];
+    if (!(fp.x == 0 && fp.y == 0 && fp.z == 0)) {
       float tc = 0.0f;
       for (int j = 0; j < n; ++j)
         if (vw[j] > 0) {
-          const float c = ncc_weak(a, px, py, j + 1, fp);
-          if (geom) tc += vw[j] * (c + gf * geom_cost(a, px, py, j + 1, fp));
+          const float c = ca[9 * n + j];
+          if (geom) tc += vw[j] * (c + gf * ga[9 * n + j]);
           else tc += vw[j] * c;
         }
       tc /= wn;
       const float db = depth_from_plane(rc, fp, px, py);
       if (db >= dmin && db <= dmax && tc < cost_now) { depth_now = db; pl_now = fp; cost_now = tc; }
+      const float depth_rand = rng.uniform() * (dmax - dmin) + dmin;
+      const float4 n_rand = random_normal(rc, px, py, rng, depth_now);
+      const float lo = (1 - 0.02f) * depth_now, hi = (1 + 0.02f) * depth_now;
+      const float depth_pert = rng.uniform() * (hi - lo) + lo;
+      const float4 n_pert = perturbed_normal(rc, px, py, pl_now, rng, (float)(0.02f * 3.14159265358979323846));
+      const float depths[5] = {depth_rand, depth_now, depth_rand, depth_now, depth_pert};
+      const float4 normals[5] = {pl_now, n_rand, n_rand, n_pert, pl_now};
+      for (int h = 0; h < 5; ++h) {
+        float4 t = normals[h];
+        t.w = dist_to_origin(rc, px, py, depths[h], t);
+        a.whyp[(size_t)slot * 5 + h] = t;
+      }
     }
+    a.rng_ctr[center] = rng.ctr;
+    a.views[center] = views_new;
+    store_vweight(&a.vweight[center], vw);
+    a.wstate[(size_t)slot * 2] = pl_now;
+    a.wstate[(size_t)slot * 2 + 1] = make_float4(depth_now, cost_now, cost_written, wn);
   }
-  if (refine) {
-    const float depth_rand = rng.uniform() * (dmax - dmin) + dmin;
-    const float4 n_rand = random_normal(rc, px, py, rng, depth_now);
-    const float lo = (1 - 0.02f) * depth_now, hi = (1 + 0.02f) * depth_now;
-    const float depth_pert = rng.uniform() * (hi - lo) + lo;
-    const float4 n_pert = perturbed_normal(rc, px, py, pl_now, rng, (float)(0.02f * 3.14159265358979323846));
-    const float depths[5] = {depth_rand, depth_now, depth_rand, depth_now, depth_pert};
-    const float4 normals[5] = {pl_now, n_rand, n_rand, n_pert, pl_now};
-    for (int h = 0; h < 5; ++h) {
-      float4 t = normals[h];
-      t.w = dist_to_origin(rc, px, py, depths[h], t);
-      float tc = 0.0f;
-      for (int j = 0; j < n; ++j)
-        if (vw[j] > 0) {
-          const float c = ncc_weak(a, px, py, j + 1, t);
-          if (geom) tc += vw[j] * (c + gf * geom_cost(a, px, py, j + 1, t));
-          else tc += vw[j] * c;
+}
+
+template <int kStage>
+__global__ void __launch_bounds__(128) k_weak_finish(const PMArgs *__restrict__ pa, int parity) {
+  const PMArgs &a = *pa;
+  const int n = a.N - 1, W = a.W;
+  const int count = a.wcount[parity];
+  const int *list = a.wlist[parity];
+  const dpe_camera &rc = a.cam[0];
+  const bool geom = a.P.geom_consistency != 0;
+  const float gf = a.P.geom_factor;
+  const float dmin = a.P.depth_min, dmax = a.P.depth_max;
+  for (int slot = blockIdx.x * blockDim.x + threadIdx.x; slot < count; slot += gridDim.x * blockDim.x) {
+    const int center = list[slot];
+    const int px = center % W, py = center / W;
+    float4 pl_now = a.wstate[(size_t)slot * 2];
+    const float4 st = a.wstate[(size_t)slot * 2 + 1];
+    float cost_now = st.y;
+    const float cost_written = st.z, wn = st.w;
+    const uint4 vwp = a.vweight[center];
+    const float4 fp = a.fit_plane[center];
+    if (!(fp.x == 0 && fp.y == 0 && fp.z == 0)) {
+      const float *cr = a.wcost_r + (size_t)slot * 5 * n;
+      const float *gr = a.wgeom_r + (size_t)slot * 5 * n;
+      for (int h = 0; h < 5; ++h) {
+        const float4 t = a.whyp[(size_t)slot * 5 + h];
+        float tc = 0.0f;
+        for (int j = 0; j < n; ++j) {
+          const int v = vweight_at(vwp, j);
+          if (v > 0) {
+            const float c = cr[h * n + j];
+            if (geom) tc += v * (c + gf * gr[h * n + j]);
+            else tc += v * c;
+          }
         }
-      tc /= wn;
-      const float db = depth_from_plane(rc, t, px, py);
-      if (db >= dmin && db <= dmax && tc < cost_now) { depth_now = db; pl_now = t; cost_now = tc; }
+        tc /= wn;
+        const float db = depth_from_plane(rc, t, px, py);
+        if (db >= dmin && db <= dmax && tc < cost_now) { pl_now = t; cost_now = tc; }
+      }
     }
+    float4 pl_final = a.plane[center];
+    if (a.P.state == DPE_REFINE_INIT) {
+      if ((double)cost_now < (double)cost_written - 0.1) pl_final = pl_now;
+    } else {
+      pl_final = pl_now;
+    }
+    a.plane[center] = pl_final;
+    // final re-cost with the strong window (DPE.cu:1849-1865); the radius swap there has no effect
+    RefWindow rw;
+    build_ref_window(a, px, py, rw, KID_WEAK_FINISH);
+    uint8_t vw[32];
+    int act[kMaxSrc];
+    int na = 0;
+    for (int i = 0; i < n; ++i) {
+      vw[i] = (uint8_t)vweight_at(vwp, i);
+      if (vw[i] > 0) act[na++] = i;
+    }
+    a.cost[center] = weighted_ncc<kStage>(a, px, py, pl_final, rw, act, na, vw) / wn;
   }
-  a.rng_ctr[center] = rng.ctr;
-  a.views[center] = views_new;
-  store_vweight(&a.vweight[center], vw);
-  float4 pl_final = pl_cur;
-  if (a.P.state == DPE_REFINE_INIT) {
-    if ((double)cost_now < (double)cost_written - 0.1) pl_final = pl_now;
-  } else {
-    pl_final = pl_now;
-  }
-  a.plane[center] = pl_final;
-  // final re-cost with the strong window (DPE.cu:1849-1865); the radius swap there has no effect
-  RefWindow rw;
-  build_ref_window(a, px, py, rw, KID_WEAK_UPDATE);
-  float cn = 0.0f;
-  for (int i = 0; i < n; ++i)
-    if (vw[i] > 0) cn += vw[i] * ncc_strong(a, px, py, i + 1, pl_final, rw);
-  a.cost[center] = cn / wn;
 }
 
 // ------------------------------------------------------------------ post passes
@@ -1123,6 +1330,7 @@ struct Sweep {
   uint32_t views;
   uint4 vw;
 };
+template <int kStage>
 __device__ __forceinline__ void sweep_setup(const PMArgs &a, int px, int py, const RefWindow &rw, Sweep &s) {
   const int center = px + py * a.W;
   s.pl = normal_to_ref(a.cam[0], a.plane[center]);
@@ -1136,7 +1344,7 @@ __device__ __forceinline__ void sweep_setup(const PMArgs &a, int px, int py, con
     if (!isSet(s.views, vi)) continue;
     float4 t = s.pl;
     t.w = dist_to_origin(a.cam[0], px, py, s.depth, t);
-    float tc = ncc_strong(a, px, py, si, t, rw);
+    float tc = ncc_strong<kStage>(a, px, py, si, t, rw);
     if (a.P.geom_consistency) tc += a.P.geom_factor * geom_cost(a, px, py, si, t);
     const int w = vweight_at(s.vw, vi);
     s.cost_now += tc * w;
@@ -1149,6 +1357,7 @@ __device__ __forceinline__ void sweep_setup(const PMArgs &a, int px, int py, con
 }
 
 // DepthToWeak (DPE.cu:2597-2751)
+template <int kStage>
 __global__ void __launch_bounds__(128) k_depth_to_weak(const PMArgs *__restrict__ pa, uint8_t *weak_out) {
   const PMArgs &a = *pa;
   int px, py;
@@ -1159,11 +1368,15 @@ __global__ void __launch_bounds__(128) k_depth_to_weak(const PMArgs *__restrict_
   RefWindow rw;
   build_ref_window(a, px, py, rw, KID_DEPTH_TO_WEAK);
   Sweep s;
-  sweep_setup(a, px, py, rw, s);
+  sweep_setup<kStage>(a, px, py, rw, s);
   if (s.depth == 0 || s.valid == 0) { weak_out[center] = DPE_UNKNOWN; return; }
   s.cost_now /= s.weight_normal;
   s.base_line /= s.valid;
   const float disp = rc.K[0] * s.base_line / s.depth;
+  int act[kMaxSrc];  // selected sources, ascending
+  int na = 0;
+  for (int vi = 0; vi < a.N - 1; ++vi)
+    if (isSet(s.views, vi)) act[na++] = vi;
   constexpr int R = 30, NS = 61;
   float pc[NS];
   for (int pd = -R; pd <= R; ++pd) {
@@ -1172,13 +1385,10 @@ __global__ void __launch_bounds__(128) k_depth_to_weak(const PMArgs *__restrict_
     float4 t = s.pl;
     t.w = dist_to_origin(rc, px, py, pdep, t);
     float cost = 0.0f;
-    for (int si = 1; si < a.N; ++si) {
-      const int vi = si - 1;
-      if (isSet(s.views, vi)) {
-        float tc = ncc_strong(a, px, py, si, t, rw);
-        if (a.P.geom_consistency) tc += a.P.geom_factor * geom_cost(a, px, py, si, t);
-        cost += tc * vweight_at(s.vw, vi);
-      }
+    for (int q = 0; q < na; ++q) {
+      float tc = ncc_strong<kStage>(a, px, py, act[q] + 1, t, rw);
+      if (a.P.geom_consistency) tc += a.P.geom_factor * geom_cost(a, px, py, act[q] + 1, t);
+      cost += tc * vweight_at(s.vw, act[q]);
     }
     cost /= s.weight_normal;
     pc[pd + R] = cvmin(2.0f, cost);
@@ -1206,6 +1416,7 @@ __global__ void __launch_bounds__(128) k_depth_to_weak(const PMArgs *__restrict_
 }
 
 // LocalRefine (DPE.cu:2753-2839)
+template <int kStage>
 __global__ void __launch_bounds__(128) k_local_refine(const PMArgs *__restrict__ pa) {
   const PMArgs &a = *pa;
   int px, py;
@@ -1215,12 +1426,16 @@ __global__ void __launch_bounds__(128) k_local_refine(const PMArgs *__restrict__
   RefWindow rw;
   build_ref_window(a, px, py, rw, KID_LOCAL_REFINE);
   Sweep s;
-  sweep_setup(a, px, py, rw, s);
+  sweep_setup<kStage>(a, px, py, rw, s);
   if (s.depth == 0) return;
   if (s.weight_normal == 0 || s.valid == 0) return;
   s.cost_now /= s.weight_normal;
   s.base_line /= s.valid;
   const float disp = rc.K[0] * s.base_line / s.depth;
+  int act[kMaxSrc];  // selected sources, ascending
+  int na = 0;
+  for (int vi = 0; vi < a.N - 1; ++vi)
+    if (isSet(s.views, vi)) act[na++] = vi;
   float min_cost = 2.0f, best = s.depth;
   for (int pd = -5; pd <= 5; ++pd) {
     const float pdep = rc.K[0] * s.base_line / (disp + pd);
@@ -1228,13 +1443,11 @@ __global__ void __launch_bounds__(128) k_local_refine(const PMArgs *__restrict__
     float4 t = s.pl;
     t.w = dist_to_origin(rc, px, py, pdep, t);
     float tc = 0.0f;
-    for (int si = 1; si < a.N; ++si) {
-      const int vi = si - 1;
-      if (isSet(s.views, vi)) {
-        const int w = vweight_at(s.vw, vi);
-        tc += ncc_strong(a, px, py, si, t, rw) * w;
-        if (a.P.geom_consistency) tc += a.P.geom_factor * geom_cost(a, px, py, si, t) * w;
-      }
+    for (int q = 0; q < na; ++q) {
+      const int vi = act[q];
+      const int w = vweight_at(s.vw, vi);
+      tc += ncc_strong<kStage>(a, px, py, vi + 1, t, rw) * w;
+      if (a.P.geom_consistency) tc += a.P.geom_factor * geom_cost(a, px, py, vi + 1, t) * w;
     }
     tc /= s.weight_normal;
     if (tc < min_cost) { min_cost = tc; best = pdep; }

@@ -23,6 +23,7 @@ WEAK, STRONG, UNKNOWN = 0, 1, 2
 FIRST_INIT, REFINE_INIT, REFINE_ITER = 0, 1, 2
 MEM_HOST, MEM_DEVICE = 0, 1
 FUSE_FP64, FUSE_FLOAT = 0, 1
+STAGE_FP32, STAGE_FP16, STAGE_BF16 = 0, 1, 2
 
 
 class Camera(C.Structure):
@@ -102,6 +103,10 @@ class SceneOut(C.Structure):
                 ("gpu_ms", C.c_float), ("fusion_ms", C.c_float), ("num_levels", C.c_int), ("calls", C.c_int)]
 
 
+class Options(C.Structure):
+    _fields_ = [("staging", C.c_int), ("gn_refine", C.c_int)]
+
+
 class Limits(C.Structure):
     _fields_ = [("max_width", C.c_int), ("max_height", C.c_int), ("max_images", C.c_int)]
 
@@ -109,7 +114,7 @@ class Limits(C.Structure):
 EXPORTED = ["dpe_status_string", "dpe_last_error", "dpe_params_default", "dpe_ctx_create", "dpe_ctx_destroy", "dpe_pm_run",
             "dpe_fuse", "dpe_ncc_eval", "dpe_ctx_set_eval_counting", "dpe_scene_run", "dpe_ctx_set_profiling",
             "dpe_ctx_reset_kernel_stats", "dpe_ctx_get_kernel_stats", "dpe_launch_count", "dpe_fp32_peak",
-            "dpe_ncc_eval_noalloc"]
+            "dpe_ncc_eval_noalloc", "dpe_ncc_grad", "dpe_ctx_set_options"]
 
 _lib = None
 
@@ -142,6 +147,8 @@ def load_library(path: Optional[str] = None) -> C.CDLL:
     lib.dpe_launch_count.argtypes = []
     lib.dpe_fp32_peak.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
     lib.dpe_ncc_eval_noalloc.argtypes = [C.POINTER(NCCQuery), C.c_void_p, C.c_void_p]
+    lib.dpe_ctx_set_options.argtypes = [C.c_void_p, C.POINTER(Options)]
+    lib.dpe_ncc_grad.argtypes = [C.c_void_p, C.POINTER(NCCQuery), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     if path is None:
         _lib = lib
     return lib
@@ -375,6 +382,29 @@ class Context:
         return res
 
     # ------------------------------------------------------------------ NCC queries
+    def set_options(self, staging: int = STAGE_FP32, gn_refine: int = 0) -> None:
+        """dpe_ctx_set_options: source-image staging (STAGE_*) and the Gauss-Newton hypothesis."""
+        st = self.lib.dpe_ctx_set_options(self.handle, C.byref(Options(staging, gn_refine)))
+        if st != OK:
+            raise DPEError(st, "dpe_ctx_set_options")
+
+    def ncc_grad(self, images, cameras, params: Params, px, py, src, planes, want_images: bool = False):
+        """dpe_ncc_grad: (cost (n,), dC/d(n, w) (n, 4), dC/d(depth, n) (n, 4), image gradients or None)."""
+        q = make_query(images, cameras, params, px, py, src, planes)
+        n = len(q.keep[0])
+        cost = np.zeros(n, np.float32)
+        gp = np.zeros((n, 4), np.float32)
+        gd = np.zeros((n, 4), np.float32)
+        gimg, ptrs = None, None
+        if want_images:
+            H, W = images[0].shape
+            gimg = [None] + [np.zeros((H, W), np.float32) for _ in images[1:]]
+            ptrs = (C.c_void_p * len(images))(*([None] + [g.ctypes.data for g in gimg[1:]]))
+        st = self.lib.dpe_ncc_grad(self.handle, C.byref(q.struct), _ptr(cost), _ptr(gp), _ptr(gd), ptrs)
+        if st != OK:
+            raise DPEError(st, "dpe_ncc_grad")
+        return cost, gp, gd, gimg
+
     def ncc_eval(self, images, cameras, params: Params, px, py, src, planes) -> np.ndarray:
         q = make_query(images, cameras, params, px, py, src, planes)
         out = np.zeros(len(q.keep[0]), np.float32)

@@ -269,6 +269,21 @@ int dpe_scene_run(dpe_ctx *ctx, const dpe_scene *scene, const dpe_schedule *sche
  * measurement entry point. */
 int dpe_ncc_eval(dpe_ctx *ctx, const dpe_ncc_query *q, float *costs_out);
 
+/* Adjoint of dpe_ncc_eval: the strong NCC and its gradient at explicit queries (host buffers).
+ * The reference has no gradient; this is the differentiable form of ComputeBilateralNCCOld
+ * (DPE.cu:696-782) for plane refinement and autograd harnesses.
+ *   grad_plane_out        [count][4] dC/d(nx, ny, nz, w) of the query's plane (n, w) in
+ *                         reference-camera coordinates (the layout of dpe_ncc_query::plane);
+ *   grad_depth_normal_out [count][4] dC/d(depth, nx, ny, nz) with the pixel's depth held fixed
+ *                         instead of w (w = -depth * n . Kr^-1 (x, y, 1)); may be NULL;
+ *   grad_images_out       NULL, or num_images pointers (entry 0 unused, NULL entries skipped) to
+ *                         width x height float buffers receiving d(sum of all query costs) /
+ *                         d(source image pixel).
+ * The gradient is zero where the cost is the constant 2 (centre outside the source, flat window)
+ * or clamped to [0, 2]. */
+int dpe_ncc_grad(dpe_ctx *ctx, const dpe_ncc_query *q, float *costs_out, float *grad_plane_out,
+                 float *grad_depth_normal_out, float *const *grad_images_out);
+
 /* Allocation-free variant of dpe_ncc_eval for callers that cannot allocate device memory: code
  * hosted by a framework that owns and budgets all device memory through its own allocator (a
  * private cudaMalloc there would bypass its accounting), and real-time paths that must not pay
@@ -291,6 +306,24 @@ int dpe_ncc_eval(dpe_ctx *ctx, const dpe_ncc_query *q, float *costs_out);
  * it keeps the previous call's contents, so calls that overlap on the GPU (different streams or
  * host threads without ordering between them) race and corrupt each other's results. */
 int dpe_ncc_eval_noalloc(const dpe_ncc_query *q, float *costs_out, void *stream);
+
+/* ---- options: the precision and differentiation forms of the path (no reference counterpart) */
+enum { DPE_STAGE_FP32 = 0, DPE_STAGE_FP16 = 1, DPE_STAGE_BF16 = 2 };
+typedef struct dpe_options {
+  /* Storage of the source images the cost kernels sample (DPE_STAGE_*).  FP16 / BF16 keep each
+   * padded texel and its right neighbour in one 32-bit word; the bilinear interpolation, the
+   * moments and the NCC stay FP32, as do the reference image and the window weights.  Images of
+   * 8-bit integers are exact in both (the finest pyramid level); interpolated pyramid levels are
+   * rounded.  Default DPE_STAGE_FP32. */
+  int staging;
+  /* 1: every strong-update iteration adds one Gauss-Newton plane hypothesis, built from the
+   * adjoint of the strong NCC (dpe_ncc_grad) over the pixel's sampled sources, and keeps it when
+   * it lowers the pixel's cost like the reference's random hypotheses.  Default 0: the
+   * reference's refinement only. */
+  int gn_refine;
+} dpe_options;
+/* Applies to the following dpe_pm_run / dpe_scene_run calls of the context. */
+int dpe_ctx_set_options(dpe_ctx *ctx, const dpe_options *opt);
 
 /* Statistics switch: when on, dpe_pm_run counts its NCC evaluations into
  * dpe_pm_out.strong_ncc_evals / weak_ncc_evals (device atomics; off by default).  The reference

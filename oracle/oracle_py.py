@@ -39,6 +39,7 @@ def load() -> C.CDLL:
     lib.oracle_pm_run.argtypes = [C.POINTER(D.Problem), C.POINTER(D.PMOut), C.c_int]
     lib.oracle_fuse.argtypes = [C.POINTER(D.FusionIn), C.POINTER(D.FusionOut)]
     lib.oracle_set_raw_moments.argtypes = [C.c_int]
+    lib.oracle_ncc_strong_grad.argtypes = [C.POINTER(D.NCCQuery), C.c_void_p, C.c_void_p, C.c_void_p]
     _lib = lib
     return lib
 
@@ -61,6 +62,23 @@ def ncc_strong(images, cameras, params, px, py, src, planes, fp64: bool) -> np.n
     out = np.zeros(len(q.keep[0]), np.float64)
     load().oracle_ncc_strong(C.byref(q.struct), 1 if fp64 else 0, out.ctypes.data)
     return out
+
+
+def ncc_strong_grad(images, cameras, params, px, py, src, planes, want_images: bool = False):
+    """FP64 strong NCC and its gradient: (cost (n,), dC/d(nx, ny, nz, w) (n, 4), and with
+    want_images the gradient of the summed cost w.r.t. each image's pixels (list, entry 0 None))."""
+    q = D.make_query(images, cameras, params, px, py, src, planes)
+    n = len(q.keep[0])
+    cost = np.zeros(n, np.float64)
+    grad = np.zeros((n, 4), np.float64)
+    gimg = None
+    ptrs = None
+    if want_images:
+        H, W = images[0].shape
+        gimg = [None] + [np.zeros((H, W), np.float64) for _ in images[1:]]
+        ptrs = (C.c_void_p * len(images))(*([None] + [g.ctypes.data for g in gimg[1:]]))
+    load().oracle_ncc_strong_grad(C.byref(q.struct), cost.ctypes.data, grad.ctypes.data, ptrs)
+    return cost, grad, gimg
 
 
 def pm_run(images, cameras, params, threads: int = 0, **kw) -> Dict:

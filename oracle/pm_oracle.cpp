@@ -1567,6 +1567,152 @@ void oracle_ncc_strong(const dpe_ncc_query *q, int fp64, double *out) {
   }
 }
 
+// ----------------------------------------------------------------------------- FP64 gradient
+// Reference gradient of the strong NCC (ComputeBilateralNCCOld, DPE.cu:696-782, evaluated as
+// above in double) for checking the adjoint kernel.  The plane derivatives come from forward-mode
+// dual numbers over (nx, ny, nz, w), independent of any hand-derived adjoint; the source-image
+// derivative follows from dC/ds_k (the cost's sensitivity to each bilinear sample) times the
+// bilinear weights of the sample's four texels (clamped to the image like the sample itself).
+namespace {
+struct D4 {
+  double v = 0, d[4] = {0, 0, 0, 0};
+  D4() = default;
+  D4(double x) : v(x) {}
+};
+inline D4 operator+(const D4 &a, const D4 &b) { D4 r(a.v + b.v); for (int i = 0; i < 4; ++i) r.d[i] = a.d[i] + b.d[i]; return r; }
+inline D4 operator-(const D4 &a, const D4 &b) { D4 r(a.v - b.v); for (int i = 0; i < 4; ++i) r.d[i] = a.d[i] - b.d[i]; return r; }
+inline D4 operator*(const D4 &a, const D4 &b) {
+  D4 r(a.v * b.v);
+  for (int i = 0; i < 4; ++i) r.d[i] = a.d[i] * b.v + a.v * b.d[i];
+  return r;
+}
+inline D4 operator/(const D4 &a, const D4 &b) {
+  D4 r(a.v / b.v);
+  for (int i = 0; i < 4; ++i) r.d[i] = (a.d[i] * b.v - a.v * b.d[i]) / (b.v * b.v);
+  return r;
+}
+inline D4 dsqrt(const D4 &a) {
+  D4 r(std::sqrt(a.v));
+  for (int i = 0; i < 4; ++i) r.d[i] = a.d[i] / (2.0 * r.v);
+  return r;
+}
+}  // namespace
+
+// cost_out[k] and grad_plane[4k..4k+3] = dC/d(nx, ny, nz, w) per query.  grad_images, when not
+// null, holds num_images pointers (entry 0 unused) to W*H double buffers that receive the
+// gradient of the SUM of all query costs with respect to that source image's pixels.
+void oracle_ncc_strong_grad(const dpe_ncc_query *q, double *cost_out, double *grad_plane, double **grad_images) {
+  Ctx c;
+  c.W = q->width; c.H = q->height; c.N = q->num_images; c.P = q->params;
+  for (int i = 0; i < c.N; ++i) { c.cam[i] = q->cameras[i]; c.img[i].data = q->images[i]; c.img[i].w = c.W; c.img[i].h = c.H; }
+  const int r = c.P.strong_radius, inc = c.P.strong_increment;
+#pragma omp parallel for schedule(static) if (!grad_images)
+  for (int64_t k = 0; k < q->count; ++k) {
+    const int px = q->px[k], py = q->py[k], s = q->src[k];
+    const dpe_camera &rc = c.cam[0], &sc = c.cam[s];
+    double *g = grad_plane + 4 * k;
+    g[0] = g[1] = g[2] = g[3] = 0.0;
+    cost_out[k] = 2.0;
+    double rC[3], sC[3], Rr[9], Cr[3], tr[3];
+    for (int i = 0; i < 3; ++i) {
+      rC[i] = -((double)rc.R[i] * rc.t[0] + (double)rc.R[3 + i] * rc.t[1] + (double)rc.R[6 + i] * rc.t[2]);
+      sC[i] = -((double)sc.R[i] * sc.t[0] + (double)sc.R[3 + i] * sc.t[1] + (double)sc.R[6 + i] * sc.t[2]);
+    }
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b)
+        Rr[3 * a + b] = (double)sc.R[3 * a] * rc.R[3 * b] + (double)sc.R[3 * a + 1] * rc.R[3 * b + 1] + (double)sc.R[3 * a + 2] * rc.R[3 * b + 2];
+    for (int i = 0; i < 3; ++i) Cr[i] = rC[i] - sC[i];
+    for (int a = 0; a < 3; ++a) tr[a] = (double)sc.R[3 * a] * Cr[0] + (double)sc.R[3 * a + 1] * Cr[1] + (double)sc.R[3 * a + 2] * Cr[2];
+    D4 n[3], w;
+    for (int b = 0; b < 3; ++b) { n[b] = D4(q->plane[4 * k + b]); n[b].d[b] = 1.0; }
+    w = D4(q->plane[4 * k + 3]); w.d[3] = 1.0;
+    D4 H[9], T[9];
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b) H[3 * a + b] = D4(Rr[3 * a + b]) - D4(tr[a]) * n[b] / w;
+    for (int a = 0; a < 3; ++a) {
+      T[3 * a] = H[3 * a] / D4(rc.K[0]);
+      T[3 * a + 1] = H[3 * a + 1] / D4(rc.K[4]);
+      T[3 * a + 2] = D4(0.0) - H[3 * a] * D4((double)rc.K[2] / rc.K[0]) - H[3 * a + 1] * D4((double)rc.K[5] / rc.K[4]) +
+                     H[3 * a + 2];
+    }
+    for (int b = 0; b < 3; ++b) {
+      H[b] = D4(sc.K[0]) * T[b] + D4(sc.K[2]) * T[6 + b];
+      H[3 + b] = D4(sc.K[4]) * T[3 + b] + D4(sc.K[5]) * T[6 + b];
+      H[6 + b] = D4(sc.K[8]) * T[6 + b];
+    }
+    auto proj = [&](double x, double y, D4 *ox, D4 *oy) {
+      const D4 X = H[0] * D4(x) + H[1] * D4(y) + H[2], Y = H[3] * D4(x) + H[4] * D4(y) + H[5];
+      const D4 Z = H[6] * D4(x) + H[7] * D4(y) + H[8];
+      *ox = X / Z; *oy = Y / Z;
+    };
+    D4 cx, cy;
+    proj(px, py, &cx, &cy);
+    if (cx.v >= sc.width || cx.v < 0.0 || cy.v >= sc.height || cy.v < 0.0) continue;
+    const double center = c.img[0].texel(px, py);
+    constexpr int kMaxTaps = 256;
+    double wk[kMaxTaps], rk[kMaxTaps], svk[kMaxTaps];
+    int tx0[kMaxTaps], ty0[kMaxTaps];
+    double tax[kMaxTaps], tay[kMaxTaps];
+    int nt = 0;
+    D4 s_s(0.0), s_ss(0.0), s_rs(0.0);
+    double s_r = 0, s_rr = 0, s_w = 0;
+    for (int i = -r; i <= r; i += inc)
+      for (int j = -r; j <= r; j += inc) {
+        const double rp = c.img[0].texel(px + i, py + j);
+        D4 sx, sy;
+        proj(px + i, py + j, &sx, &sy);
+        const Image &im = c.img[s];
+        // bilinear with clamp-to-edge: a clamped coordinate does not move the sample
+        D4 xc = sx, yc = sy;
+        if (sx.v < -1.0) xc = D4(-1.0);
+        if (sx.v > (double)(im.w - 1)) xc = D4((double)(im.w - 1));
+        if (sy.v < -1.0) yc = D4(-1.0);
+        if (sy.v > (double)(im.h - 1)) yc = D4((double)(im.h - 1));
+        const double fx = std::floor(xc.v), fy = std::floor(yc.v);
+        const int x0 = (int)fx, y0 = (int)fy;
+        D4 ax = xc - D4(fx), ay = yc - D4(fy);
+        const double v00 = im.texel(x0, y0), v10 = im.texel(x0 + 1, y0);
+        const double v01 = im.texel(x0, y0 + 1), v11 = im.texel(x0 + 1, y0 + 1);
+        const D4 top = (D4(1.0) - ax) * D4(v00) + ax * D4(v10);
+        const D4 bot = (D4(1.0) - ax) * D4(v01) + ax * D4(v11);
+        const D4 sv = (D4(1.0) - ay) * top + ay * bot;
+        const double wt = std::exp(-std::sqrt((double)(i * i + j * j)) / (2.0 * c.P.sigma_spatial * c.P.sigma_spatial) -
+                                   std::fabs(rp - center) / (2.0 * c.P.sigma_color * c.P.sigma_color));
+        s_r += wt * rp; s_rr += wt * rp * rp; s_w += wt;
+        s_s = s_s + D4(wt) * sv; s_ss = s_ss + D4(wt) * sv * sv; s_rs = s_rs + D4(wt * rp) * sv;
+        if (nt < kMaxTaps) {
+          wk[nt] = wt; rk[nt] = rp; svk[nt] = sv.v; tx0[nt] = x0; ty0[nt] = y0; tax[nt] = ax.v; tay[nt] = ay.v;
+          nt++;
+        }
+      }
+    s_r /= s_w; s_rr /= s_w;
+    const D4 ms = s_s / D4(s_w), mss = s_ss / D4(s_w), mrs = s_rs / D4(s_w);
+    const double vr = s_rr - s_r * s_r;
+    const D4 vs = mss - ms * ms;
+    if (vr < 1e-5 || vs.v < 1e-5) continue;
+    const D4 cov = mrs - D4(s_r) * ms;
+    const D4 cst = D4(1.0) - cov / dsqrt(D4(vr) * vs);
+    cost_out[k] = std::fmax(0.0, std::fmin(2.0, cst.v));
+    if (cst.v <= 0.0 || cst.v >= 2.0) continue;  // clamped: flat
+    for (int i = 0; i < 4; ++i) g[i] = cst.d[i];
+    if (grad_images && grad_images[s]) {
+      const double sq = std::sqrt(vr * vs.v);
+      for (int t = 0; t < nt; ++t) {
+        const double dcov = wk[t] * (rk[t] - s_r) / s_w;
+        const double dvs = 2.0 * wk[t] * (svk[t] - ms.v) / s_w;
+        const double dc = -dcov / sq + cov.v * dvs / (2.0 * vs.v * sq);
+        const int xs[2] = {tx0[t], tx0[t] + 1}, ys[2] = {ty0[t], ty0[t] + 1};
+        const double bx[2] = {1.0 - tax[t], tax[t]}, by[2] = {1.0 - tay[t], tay[t]};
+        for (int yy = 0; yy < 2; ++yy)
+          for (int xx = 0; xx < 2; ++xx) {
+            const int X = std::min(std::max(xs[xx], 0), c.W - 1), Y = std::min(std::max(ys[yy], 0), c.H - 1);
+            grad_images[s][(size_t)Y * c.W + X] += dc * bx[xx] * by[yy];
+          }
+      }
+    }
+  }
+}
+
 // One per-view PatchMatch call with the kernel order of DPE::RunPatchMatch (DPE.cu:3157-3234).
 // Host memory only.  Returns 0 on success.
 int oracle_pm_run(const dpe_problem *pr, dpe_pm_out *out, int threads) {

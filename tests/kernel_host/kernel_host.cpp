@@ -15,7 +15,7 @@
 
 using std::max;
 using std::min;
-static dim3 blockIdx, threadIdx, blockDim;
+static dim3 blockIdx, threadIdx, blockDim, gridDim;
 #undef __global__
 #undef __device__
 #undef __host__
@@ -44,12 +44,24 @@ static inline unsigned long long atomicAdd(unsigned long long *p, unsigned long 
   *p += v;
   return o;
 }
+static inline float __uint_as_float(unsigned int u) {
+  float f;
+  std::memcpy(&f, &u, 4);
+  return f;
+}
+static inline float atomicAdd(float *p, float v) {
+  const float o = *p;
+  *p += v;
+  return o;
+}
 using std::isnan;
+using std::isfinite;
 #include "../../dpe-mvs-fast_b200/csrc/pm_kernels.cuh"
 using namespace dpe;
 
 template <class K, class... Args> static void launch(dim3 grid, dim3 block, K k, Args... args) {
   blockDim = block;
+  gridDim = grid;
   for (unsigned by = 0; by < grid.y; ++by)
     for (unsigned bx = 0; bx < grid.x; ++bx)
       for (unsigned ty = 0; ty < block.y; ++ty)
@@ -80,6 +92,7 @@ extern "C" int host_pm_run(const dpe_problem *p, dpe_pm_out *out) {
     launch(dim3((W + 2 + 31) / 32, (H + 2 + 7) / 8), dim3(32, 8), k_pad_image, p->images[i], d, W, H);
     a.img[i] = d;
     imgs.push_back(d);
+
     if (a.P.geom_consistency) a.dep[i] = p->depths[i];
   }
   a.plane = alloc<float4>(L); a.plane_snap = alloc<float4>(L); a.fit_plane = alloc<float4>(L);
@@ -99,20 +112,48 @@ extern "C" int host_pm_run(const dpe_problem *p, dpe_pm_out *out) {
   launch(fg, fb, k_find_nearest_strong, &a);
   launch(fg, fb, k_gen_neighbours, &a);
   launch(fg, fb, k_neighbour_update, &a);
-  launch(fg, fb, k_random_init, &a);
+  // WEAK pixels per colour in raster order (the cub select of dpe_pm_run)
+  const size_t wcap = (L + 1) / 2;
+  std::vector<int> wlist(2 * wcap), wcount(2, 0);
+  std::vector<float2> wtab;
+  std::vector<float4> wwin, whyp, wstate;
+  std::vector<float> wcost, wgeom, wcost_r, wgeom_r;
+  if (a.P.use_APD) {
+    for (size_t i = 0; i < L; ++i) {
+      const int x = (int)(i % W), y = (int)(i / W), c = (x + y) & 1;
+      if (a.weak[i] == DPE_WEAK) wlist[c * wcap + wcount[c]++] = (int)i;
+    }
+    const int n = N - 1, side = (2 * a.P.weak_radius) / a.P.weak_increment + 1;
+    a.wtaps = side * side;
+    a.wtab_stride = kMaxWin * kMaxWin + 8 * a.wtaps;
+    wtab.resize(wcap * a.wtab_stride); wwin.resize(wcap * kNeighbours); whyp.resize(wcap * 5);
+    wstate.resize(wcap * 2); wcost.resize(wcap * 10 * n); wgeom.resize(wcap * 10 * n);
+    wcost_r.resize(wcap * 5 * n); wgeom_r.resize(wcap * 5 * n);
+    a.wlist[0] = wlist.data(); a.wlist[1] = wlist.data() + wcap; a.wcount = wcount.data();
+    a.wtab = wtab.data(); a.wwin = wwin.data(); a.whyp = whyp.data(); a.wstate = wstate.data();
+    a.wcost = wcost.data(); a.wgeom = wgeom.data(); a.wcost_r = wcost_r.data(); a.wgeom_r = wgeom_r.data();
+  }
+  launch(fg, fb, k_random_init<DPE_STAGE_FP32>, &a);
   for (int it = 0; it < a.P.max_iterations; ++it) {
     for (int parity = 0; parity < 2; ++parity) {
       if (a.P.use_edge) { memcpy(a.plane_snap, a.plane, L * 16); memcpy(a.cost_snap, a.cost, L * 4); }
-      launch(hg, hb, k_strong_update, &a, it, parity);
+      launch(hg, hb, k_strong_update<DPE_STAGE_FP32, false>, &a, it, parity);
     }
     launch(fg, fb, k_ransac_fit_plane, &a);
     if (a.P.use_APD)
-      for (int parity = 0; parity < 2; ++parity) launch(hg, hb, k_weak_update, &a, it, parity);
+      for (int parity = 0; parity < 2; ++parity) {
+        const dim3 lg(7), lb(32);  // strided work lists: any grid covers them
+        launch(lg, lb, k_weak_prepare, &a, parity);
+        launch(lg, lb, k_weak_eval<false, DPE_STAGE_FP32>, &a, parity);
+        launch(lg, lb, k_weak_decide, &a, it, parity);
+        launch(lg, lb, k_weak_eval<true, DPE_STAGE_FP32>, &a, parity);
+        launch(lg, lb, k_weak_finish<DPE_STAGE_FP32>, &a, parity);
+      }
   }
   launch(fg, fb, k_get_depth_normal, &a);
   for (int parity = 0; parity < 2; ++parity) launch(hg, hb, k_filter_strong, &a, parity);
-  launch(fg, fb, k_depth_to_weak, &a, a.weak);
-  launch(fg, fb, k_local_refine, &a);
+  launch(fg, fb, k_depth_to_weak<DPE_STAGE_FP32>, &a, a.weak);
+  launch(fg, fb, k_local_refine<DPE_STAGE_FP32>, &a);
   memcpy(out->plane, a.plane, L * 16);
   memcpy(out->weak, a.weak, L);
   memcpy(out->selected_views, a.views, L * 4);
