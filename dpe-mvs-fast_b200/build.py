@@ -1,6 +1,9 @@
 """Build the sm_100a shared library libdpe_sm100.so in-tree (nvcc, no torch extension machinery).
 
-Usage: python dpe-mvs-fast_b200/build.py [--force]
+Usage: python dpe-mvs-fast_b200/build.py [--force] [--checked] [--variant NAME -DMACRO=V ...]
+
+--variant builds libdpe_sm100_NAME.so with the given preprocessor definitions (kernel-shape
+experiments selected at run time with DPE_LIBRARY=libdpe_sm100_NAME.so).
 """
 from __future__ import annotations
 
@@ -35,11 +38,15 @@ def _deps() -> list:
     return files
 
 
-def build(force: bool = False, verbose: bool = False, checked: bool = False) -> str:
+def build(force: bool = False, verbose: bool = False, checked: bool = False, variant: str = "",
+          defines: tuple = ()) -> str:
     """Compile csrc/*.cu for sm_100a and link libdpe_sm100.so (checked=True: the bounds-checked
-    debug variant libdpe_sm100_checked.so, built with -DDPE_CHECKED)."""
+    debug variant libdpe_sm100_checked.so, built with -DDPE_CHECKED; variant: a named build with
+    extra -D definitions)."""
     os.makedirs(OBJ, exist_ok=True)
     lib = LIB_CHECKED if checked else LIB
+    if variant:
+        lib = os.path.join(HERE, f"libdpe_sm100_{variant}.so")
     newest = max(os.path.getmtime(f) for f in _deps())
     if not force and os.path.exists(lib) and os.path.getmtime(lib) >= newest:
         return lib
@@ -47,9 +54,10 @@ def build(force: bool = False, verbose: bool = False, checked: bool = False) -> 
     procs = []
     objs = []
     for src, extra in UNITS.items():
-        obj = os.path.join(OBJ, src.replace(".cu", "_checked.o" if checked else ".o"))
+        suffix = f"_{variant}.o" if variant else ("_checked.o" if checked else ".o")
+        obj = os.path.join(OBJ, src.replace(".cu", suffix))
         objs.append(obj)
-        flags = ["-DDPE_CHECKED"] if checked else []
+        flags = (["-DDPE_CHECKED"] if checked else []) + list(defines)
         cmd = [nvcc, *ARCH, *COMMON, *extra, *flags, "-c", os.path.join(CSRC, src), "-o", obj]
         if verbose:
             print(" ".join(cmd), flush=True)
@@ -65,4 +73,7 @@ def build(force: bool = False, verbose: bool = False, checked: bool = False) -> 
 
 
 if __name__ == "__main__":
-    print(build(force="--force" in sys.argv, verbose=True, checked="--checked" in sys.argv))
+    args = sys.argv[1:]
+    name = args[args.index("--variant") + 1] if "--variant" in args else ""
+    defs = tuple(a for a in args if a.startswith("-D"))
+    print(build(force="--force" in args, verbose=True, checked="--checked" in args, variant=name, defines=defs))

@@ -217,7 +217,7 @@ template <class F> void with_stage(int staging, F &&f) {
   else f(std::integral_constant<int, DPE_STAGE_FP32>{});
 }
 
-void launch_strong_update(int staging, bool gn, dim3 grid, cudaStream_t s, const PMArgs *args, int it, int parity) {
+void launch_strong_update(int staging, bool gn, dim3 grid, cudaStream_t s, const Launch args, int it, int parity) {
   with_stage(staging, [&](auto st) {
     if (gn) k_strong_update<decltype(st)::value, true><<<grid, kHalfBlock, 0, s>>>(args, it, parity);
     else k_strong_update<decltype(st)::value, false><<<grid, kHalfBlock, 0, s>>>(args, it, parity);
@@ -235,12 +235,26 @@ struct WeakOfColour {
 
 }  // namespace
 
-extern "C" int dpe_pm_run(dpe_ctx *ctx, const dpe_problem *p, dpe_pm_out *out) {
-  if (!ctx || !out) return DPE_ERR_INVALID_ARGUMENT;
-  int st = check_problem(p);
-  if (st) return st;
-  if (!out->plane || !out->weak || !out->selected_views) return DPE_ERR_INVALID_ARGUMENT;
-  DPE_TRY(cudaSetDevice(ctx->device));
+namespace {
+
+// One problem of a call: its host-side argument block (copied to the device before the kernels)
+// and the inputs the first kernel reads.  Problem i of a batch keeps its buffers under arena
+// names suffixed with its index, so problems never share state.
+struct ProblemState {
+  PMArgs a;
+  const float4 *plane_in = nullptr;
+  const uint32_t *views_in = nullptr;
+  const uint8_t *weak_in = nullptr;
+  int *weak_flag = nullptr;
+  size_t L = 0, wcap = 0;
+};
+
+std::string slot_name(const char *base, int index) {
+  return index == 0 ? std::string(base) : std::string(base) + "#" + std::to_string(index);
+}
+
+// Buffers, uploads and the padded / staged source images of problem `index`.
+int setup_problem(dpe_ctx *ctx, const dpe_problem *p, int index, ProblemState *ps) {
   cudaStream_t s = ctx->stream;
   const int W = p->width, H = p->height, N = p->num_images;
   const size_t L = (size_t)W * H;
@@ -248,8 +262,11 @@ extern "C" int dpe_pm_run(dpe_ctx *ctx, const dpe_problem *p, dpe_pm_out *out) {
   const bool host = p->memory == DPE_MEM_HOST;
   const cudaMemcpyKind h2d = host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
   Arena &A = ctx->arena;
-
-  PMArgs a;
+  auto get = [&](auto *tag, const char *name, size_t count) {
+    using T = std::remove_pointer_t<decltype(tag)>;
+    return A.get<T>(slot_name(name, index).c_str(), count);
+  };
+  PMArgs &a = ps->a;
   std::memset(&a, 0, sizeof(a));
   a.W = W; a.H = H; a.N = N; a.pad_w = W + 2;
   a.P = p->params;
@@ -260,83 +277,82 @@ extern "C" int dpe_pm_run(dpe_ctx *ctx, const dpe_problem *p, dpe_pm_out *out) {
   a.key[1] = (uint32_t)(p->seed >> 32);
   a.stage = ctx->opt.staging;
   a.gn = ctx->opt.gn_refine;
+  ps->L = L;
+  ps->wcap = (L + 1) / 2;  // pixels of one colour
 
   // ---- device buffers
-  float *img_pad = A.get<float>("img_pad", PL * N);
+  float *img_pad = get((float *)0, "img_pad", PL * N);
   const int staging = ctx->opt.staging;
-  uint32_t *img_pairs = staging != DPE_STAGE_FP32 ? A.get<uint32_t>("img_pairs", PL * N) : nullptr;
-  float *stage = A.get<float>("img_stage", L * N);
-  a.plane = A.get<float4>("plane", L);
-  a.plane_snap = A.get<float4>("plane_snap", L);
-  a.fit_plane = A.get<float4>("fit_plane", L);
-  a.cost = A.get<float>("cost", L);
-  a.cost_snap = A.get<float>("cost_snap", L);
-  a.complexity = A.get<float>("complexity", L);
-  a.views = A.get<uint32_t>("views", L);
-  a.rng_ctr = A.get<uint32_t>("rng_ctr", L);
-  a.vweight = A.get<uint4>("vweight", L);
-  a.weak = A.get<uint8_t>("weak", L);
-  a.reliable = A.get<uint8_t>("reliable", L);
-  a.nmap = A.get<int32_t>("nmap", L);
-  a.radius = A.get<int32_t>("radius", L);
-  int *weak_flag = A.get<int32_t>("weak_flag", L);
-  a.neigh = A.get<short2>("neigh", L * kNeighbours);
-  a.lab_bound = A.get<short2>("lab_bound", L * 8);
-  a.edge_neigh = A.get<short2>("edge_neigh", L * 8);
-  a.nearest = A.get<short2>("nearest", L);
-  const size_t wcap = (L + 1) / 2;  // pixels of one colour
+  uint32_t *img_pairs = staging != DPE_STAGE_FP32 ? get((uint32_t *)0, "img_pairs", PL * N) : nullptr;
+  float *stage = host ? get((float *)0, "img_stage", L * N) : nullptr;
+  a.plane = get((float4 *)0, "plane", L);
+  a.plane_snap = get((float4 *)0, "plane_snap", L);
+  a.fit_plane = get((float4 *)0, "fit_plane", L);
+  a.cost = get((float *)0, "cost", L);
+  a.cost_snap = get((float *)0, "cost_snap", L);
+  a.complexity = get((float *)0, "complexity", L);
+  a.views = get((uint32_t *)0, "views", L);
+  a.rng_ctr = get((uint32_t *)0, "rng_ctr", L);
+  a.vweight = get((uint4 *)0, "vweight", L);
+  a.weak = get((uint8_t *)0, "weak", L);
+  a.reliable = get((uint8_t *)0, "reliable", L);
+  a.nmap = get((int32_t *)0, "nmap", L);
+  a.radius = get((int32_t *)0, "radius", L);
+  ps->weak_flag = get((int32_t *)0, "weak_flag", L);
+  a.neigh = get((short2 *)0, "neigh", L * kNeighbours);
+  a.lab_bound = get((short2 *)0, "lab_bound", L * 8);
+  a.edge_neigh = get((short2 *)0, "edge_neigh", L * 8);
+  a.nearest = get((short2 *)0, "nearest", L);
+  const size_t wcap = ps->wcap;
   if (a.P.use_APD) {
     const int n = N - 1;
     const int side = (2 * a.P.weak_radius) / a.P.weak_increment + 1;
     a.wtaps = side * side;
     a.wtab_stride = kMaxWin * kMaxWin + 8 * a.wtaps;
-    int *wl = A.get<int>("weak_list", 2 * wcap);
+    int *wl = get((int *)0, "weak_list", 2 * wcap);
     a.wlist[0] = wl;
     a.wlist[1] = wl ? wl + wcap : nullptr;
-    a.wcount = A.get<int>("weak_count", 2);
-    a.wtab = A.get<float2>("weak_tab", wcap * a.wtab_stride);
-    a.wwin = A.get<float4>("weak_win", wcap * kNeighbours);
-    a.wcost = A.get<float>("weak_cost", wcap * 10 * n);
-    a.wgeom = A.get<float>("weak_geom", wcap * 10 * n);
-    a.whyp = A.get<float4>("weak_hyp", wcap * 5);
-    a.wcost_r = A.get<float>("weak_cost_r", wcap * 5 * n);
-    a.wgeom_r = A.get<float>("weak_geom_r", wcap * 5 * n);
-    a.wstate = A.get<float4>("weak_state", wcap * 2);
+    a.wcount = get((int *)0, "weak_count", 2);
+    a.wtab = get((float2 *)0, "weak_tab", wcap * a.wtab_stride);
+    a.wwin = get((float4 *)0, "weak_win", wcap * kNeighbours);
+    a.wcost = get((float *)0, "weak_cost", wcap * 10 * n);
+    a.wgeom = get((float *)0, "weak_geom", wcap * 10 * n);
+    a.whyp = get((float4 *)0, "weak_hyp", wcap * 5);
+    a.wcost_r = get((float *)0, "weak_cost_r", wcap * 5 * n);
+    a.wgeom_r = get((float *)0, "weak_geom_r", wcap * 5 * n);
+    a.wstate = get((float4 *)0, "weak_state", wcap * 2);
   }
   if (!A.ok()) return DPE_ERR_OUT_OF_MEMORY;
 
-  const float4 *plane_in = nullptr;
-  const uint32_t *views_in = nullptr;
-  const uint8_t *weak_in = nullptr;
   if (host) {
     if (a.P.state != DPE_FIRST_INIT) {
-      float4 *d = A.get<float4>("plane_in", L);
+      float4 *d = get((float4 *)0, "plane_in", L);
       if (!d) return DPE_ERR_OUT_OF_MEMORY;
       DPE_TRY(cudaMemcpyAsync(d, p->plane_in, L * sizeof(float4), h2d, s));
-      plane_in = d;
+      ps->plane_in = d;
       if (p->selected_views_in) {
-        uint32_t *dv = A.get<uint32_t>("views_in", L);
+        uint32_t *dv = get((uint32_t *)0, "views_in", L);
         if (!dv) return DPE_ERR_OUT_OF_MEMORY;
         DPE_TRY(cudaMemcpyAsync(dv, p->selected_views_in, L * 4, h2d, s));
-        views_in = dv;
+        ps->views_in = dv;
       }
     }
     if (a.P.use_APD) {
-      uint8_t *dw = A.get<uint8_t>("weak_in", L);
+      uint8_t *dw = get((uint8_t *)0, "weak_in", L);
       if (!dw) return DPE_ERR_OUT_OF_MEMORY;
       DPE_TRY(cudaMemcpyAsync(dw, p->weak_in, L, h2d, s));
-      weak_in = dw;
+      ps->weak_in = dw;
     }
   } else {
-    plane_in = reinterpret_cast<const float4 *>(p->plane_in);
-    views_in = p->selected_views_in;
-    weak_in = p->weak_in;
+    ps->plane_in = reinterpret_cast<const float4 *>(p->plane_in);
+    ps->views_in = p->selected_views_in;
+    ps->weak_in = p->weak_in;
   }
   if (a.P.use_edge || a.P.use_limit) {
     const size_t LL = (size_t)p->low_width * p->low_height;
     a.lowW = p->low_width; a.lowH = p->low_height;
     if (host) {
-      uint8_t *de = A.get<uint8_t>("edge", L), *dl = A.get<uint8_t>("edge_low", LL);
+      uint8_t *de = get((uint8_t *)0, "edge", L), *dl = get((uint8_t *)0, "edge_low", LL);
       if (!de || !dl) return DPE_ERR_OUT_OF_MEMORY;
       DPE_TRY(cudaMemcpyAsync(de, p->edge, L, h2d, s));
       DPE_TRY(cudaMemcpyAsync(dl, p->edge_low_res, LL, h2d, s));
@@ -347,7 +363,7 @@ extern "C" int dpe_pm_run(dpe_ctx *ctx, const dpe_problem *p, dpe_pm_out *out) {
   }
   if (a.P.use_label) {
     if (host) {
-      int32_t *dl = A.get<int32_t>("label", L);
+      int32_t *dl = get((int32_t *)0, "label", L);
       if (!dl) return DPE_ERR_OUT_OF_MEMORY;
       DPE_TRY(cudaMemcpyAsync(dl, p->label, L * 4, h2d, s));
       a.label = dl;
@@ -356,7 +372,7 @@ extern "C" int dpe_pm_run(dpe_ctx *ctx, const dpe_problem *p, dpe_pm_out *out) {
     }
   }
   if (a.P.geom_consistency) {
-    float *dd = host ? A.get<float>("depths", L * N) : nullptr;
+    float *dd = host ? get((float *)0, "depths", L * N) : nullptr;
     if (host && !dd) return DPE_ERR_OUT_OF_MEMORY;
     for (int i = 0; i < N; ++i) {
       if (host) {
@@ -385,17 +401,146 @@ extern "C" int dpe_pm_run(dpe_ctx *ctx, const dpe_problem *p, dpe_pm_out *out) {
       PM_LAUNCHED("k_stage_pairs", s);
     }
   }
-  unsigned long long *counters = A.get<unsigned long long>("counters", 2 * KID_COUNT);
-  if (!counters) return DPE_ERR_OUT_OF_MEMORY;
-  a.counters = ctx->count_evals ? counters : nullptr;
-  if (ctx->count_evals) DPE_TRY(cudaMemsetAsync(counters, 0, 16 * KID_COUNT, s));
+  return DPE_OK;
+}
 
-  // ---- kernel sequence (DPE.cu:3157-3234)
-  PMArgs *d_args = A.get<PMArgs>("pm_args", 1);
-  if (!d_args) return DPE_ERR_OUT_OF_MEMORY;
-  DPE_TRY(cudaMemcpyAsync(d_args, &a, sizeof(PMArgs), cudaMemcpyHostToDevice, s));
+// Grids of one kernel sequence: for one problem the 2D pixel grids; for a batch one 1D grid per
+// kind over all problems, with the prefix tables the kernels resolve their problem from.
+struct SequenceGrids {
+  Launch full, half, prep, eval;
+  dim3 fg, hg;
+  unsigned gp = 0, ge = 0;
+  const dim3 fb = kFullBlock, hb = kHalfBlock;
+};
+
+// The kernel sequence of DPE::RunPatchMatch (DPE.cu:3157-3234) for n problems that share the
+// schedule flags (state, APD, edges, geometric term, iteration count).
+int run_sequence(dpe_ctx *ctx, ProblemState *ps, int n, const PMArgs *d_args, const SequenceGrids &g) {
+  cudaStream_t s = ctx->stream;
+  Arena &A = ctx->arena;
+  const dpe_params &P = ps[0].a.P;
+  const int staging = ctx->opt.staging;
+  const bool gn = ctx->opt.gn_refine != 0;
+  DPE_TIMED(ctx, KID_INIT_STATE, s, for (int b = 0; b < n; ++b) {
+    // k_init_state takes per-problem inputs: one launch per problem
+    const Launch one{d_args + b, nullptr, 1};
+    k_init_state<<<full_grid(ps[b].a.W, ps[b].a.H), kFullBlock, 0, s>>>(one, ps[b].plane_in, ps[b].views_in,
+                                                                         ps[b].weak_in, ps[b].weak_flag);
+  });
+  PM_LAUNCHED("k_init_state", s);
+  for (int b = 0; b < n; ++b) {
+    const PMArgs &a = ps[b].a;
+    const int L = (int)ps[b].L;
+    if (P.use_APD) {
+      size_t tmp_bytes = 0;
+      cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, ps[b].weak_flag, a.nmap, L, s);
+      void *tmp = A.get<uint8_t>("scan_tmp", tmp_bytes + 16);
+      if (!tmp) return DPE_ERR_OUT_OF_MEMORY;
+      DPE_TRY(cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, ps[b].weak_flag, a.nmap, L, s));
+    } else {
+      DPE_TRY(cudaMemsetAsync(a.nmap, 0, (size_t)L * 4, s));
+    }
+  }
+  DPE_TIMED(ctx, KID_GEN_EDGE_INFORM, s, k_gen_edge_inform<<<g.fg, g.fb, 0, s>>>(g.full));
+  PM_LAUNCHED("k_gen_edge_inform", s);
+  DPE_TIMED(ctx, KID_FIND_NEAREST, s, k_find_nearest_strong<<<g.fg, g.fb, 0, s>>>(g.full));
+  PM_LAUNCHED("k_find_nearest_strong", s);
+  DPE_TIMED(ctx, KID_GEN_NEIGHBOURS, s, k_gen_neighbours<<<g.fg, g.fb, 0, s>>>(g.full));
+  PM_LAUNCHED("k_gen_neighbours", s);
+  DPE_TIMED(ctx, KID_NEIGHBOUR_UPDATE, s, k_neighbour_update<<<g.fg, g.fb, 0, s>>>(g.full));
+  PM_LAUNCHED("k_neighbour_update", s);
+  if (P.use_APD) {
+    // WEAK pixels per colour, in raster order; the states are final for the iterations
+    for (int b = 0; b < n; ++b) {
+      const PMArgs &a = ps[b].a;
+      const int L = (int)ps[b].L;
+      size_t sel_bytes = 0;
+      thrust::counting_iterator<int> first(0);
+      cub::DeviceSelect::If(nullptr, sel_bytes, first, const_cast<int *>(a.wlist[0]), const_cast<int *>(a.wcount), L,
+                            WeakOfColour{a.weak, a.W, 0}, s);
+      void *sel_tmp = A.get<uint8_t>("select_tmp", sel_bytes + 16);
+      if (!sel_tmp) return DPE_ERR_OUT_OF_MEMORY;
+      for (int parity = 0; parity < 2; ++parity)
+        DPE_TRY(cub::DeviceSelect::If(sel_tmp, sel_bytes, first, const_cast<int *>(a.wlist[parity]),
+                                      const_cast<int *>(a.wcount) + parity, L, WeakOfColour{a.weak, a.W, parity}, s));
+    }
+  }
+  DPE_TIMED(ctx, KID_RANDOM_INIT, s, with_stage(staging, [&](auto st) { k_random_init<decltype(st)::value><<<g.fg, g.fb, 0, s>>>(g.full); }));
+  PM_LAUNCHED("k_random_init", s);
+  for (int it = 0; it < P.max_iterations; ++it) {
+    for (int parity = 0; parity < 2; ++parity) {
+      if (P.use_edge)
+        for (int b = 0; b < n; ++b) {
+          const PMArgs &a = ps[b].a;
+          DPE_TRY(cudaMemcpyAsync(a.plane_snap, a.plane, ps[b].L * sizeof(float4), cudaMemcpyDeviceToDevice, s));
+          DPE_TRY(cudaMemcpyAsync(a.cost_snap, a.cost, ps[b].L * 4, cudaMemcpyDeviceToDevice, s));
+        }
+      DPE_TIMED(ctx, KID_STRONG_UPDATE, s, launch_strong_update(staging, gn, g.hg, s, g.half, it, parity));
+      PM_LAUNCHED("k_strong_update", s);
+    }
+    DPE_TIMED(ctx, KID_RANSAC, s, k_ransac_fit_plane<<<g.fg, g.fb, 0, s>>>(g.full));
+    PM_LAUNCHED("k_ransac_fit_plane", s);
+    if (P.use_APD)
+      for (int parity = 0; parity < 2; ++parity) {
+        DPE_TIMED(ctx, KID_WEAK_PREPARE, s, k_weak_prepare<<<g.gp, 128, 0, s>>>(g.prep, parity));
+        PM_LAUNCHED("k_weak_prepare", s);
+        DPE_TIMED(ctx, KID_WEAK_EVAL, s, with_stage(staging, [&](auto st) { k_weak_eval<false, decltype(st)::value><<<g.ge, 128, 0, s>>>(g.eval, parity); }));
+        PM_LAUNCHED("k_weak_eval", s);
+        DPE_TIMED(ctx, KID_WEAK_DECIDE, s, k_weak_decide<<<g.gp, 128, 0, s>>>(g.prep, it, parity));
+        PM_LAUNCHED("k_weak_decide", s);
+        DPE_TIMED(ctx, KID_WEAK_EVAL, s, with_stage(staging, [&](auto st) { k_weak_eval<true, decltype(st)::value><<<g.ge, 128, 0, s>>>(g.eval, parity); }));
+        PM_LAUNCHED("k_weak_eval", s);
+        DPE_TIMED(ctx, KID_WEAK_FINISH, s, with_stage(staging, [&](auto st) { k_weak_finish<decltype(st)::value><<<g.gp, 128, 0, s>>>(g.prep, parity); }));
+        PM_LAUNCHED("k_weak_finish", s);
+      }
+  }
+  DPE_TIMED(ctx, KID_DEPTH_NORMAL, s, k_get_depth_normal<<<g.fg, g.fb, 0, s>>>(g.full));
+  PM_LAUNCHED("k_get_depth_normal", s);
+  for (int parity = 0; parity < 2; ++parity) {
+    DPE_TIMED(ctx, KID_FILTER, s, k_filter_strong<<<g.hg, g.hb, 0, s>>>(g.half, parity));
+    PM_LAUNCHED("k_filter_strong", s);
+  }
+  DPE_TIMED(ctx, KID_DEPTH_TO_WEAK, s, with_stage(staging, [&](auto st) { k_depth_to_weak<decltype(st)::value><<<g.fg, g.fb, 0, s>>>(g.full); }));
+  PM_LAUNCHED("k_depth_to_weak", s);
+  DPE_TIMED(ctx, KID_LOCAL_REFINE, s, with_stage(staging, [&](auto st) { k_local_refine<decltype(st)::value><<<g.fg, g.fb, 0, s>>>(g.full); }));
+  PM_LAUNCHED("k_local_refine", s);
+  return DPE_OK;
+}
+
+int copy_outputs(dpe_ctx *ctx, const ProblemState &ps, const dpe_problem *p, dpe_pm_out *out) {
+  cudaStream_t s = ctx->stream;
+  const PMArgs &a = ps.a;
+  const size_t L = ps.L;
+  const cudaMemcpyKind d2o = p->memory == DPE_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+  DPE_TRY(cudaMemcpyAsync(out->plane, a.plane, L * sizeof(float4), d2o, s));
+  DPE_TRY(cudaMemcpyAsync(out->weak, a.weak, L, d2o, s));
+  DPE_TRY(cudaMemcpyAsync(out->selected_views, a.views, L * 4, d2o, s));
+  if (out->costs) DPE_TRY(cudaMemcpyAsync(out->costs, a.cost, L * 4, d2o, s));
+  return DPE_OK;
+}
+
+// Runs problems ps[0..n) through one kernel sequence and fills outs[0..n).
+int pm_run_problems(dpe_ctx *ctx, const dpe_problem *const *problems, int n, dpe_pm_out *const *outs) {
+  DPE_TRY(cudaSetDevice(ctx->device));
+  cudaStream_t s = ctx->stream;
+  Arena &A = ctx->arena;
+  std::vector<ProblemState> ps(n);
+  unsigned long long *counters = A.get<unsigned long long>("counters", 2 * KID_COUNT);
+  PMArgs *d_args = A.get<PMArgs>("pm_args", n);
+  int *d_start = n > 1 ? A.get<int>("batch_start", 4 * (n + 1)) : nullptr;
+  if (!counters || !d_args || (n > 1 && !d_start)) return DPE_ERR_OUT_OF_MEMORY;
+  if (ctx->count_evals) DPE_TRY(cudaMemsetAsync(counters, 0, 16 * KID_COUNT, s));
+  for (int b = 0; b < n; ++b) {
+    int st = setup_problem(ctx, problems[b], b, &ps[b]);
+    if (st) return st;
+    ps[b].a.counters = ctx->count_evals ? counters : nullptr;
+  }
+  std::vector<PMArgs> host_args(n);
+  for (int b = 0; b < n; ++b) host_args[b] = ps[b].a;
+  DPE_TRY(cudaMemcpyAsync(d_args, host_args.data(), sizeof(PMArgs) * n, cudaMemcpyHostToDevice, s));
 #ifdef DPE_CHECKED
   {
+    const PMArgs &a = ps[0].a;
     long long *echo = A.get<long long>("echo", 8);
     k_echo_args<<<1, 1, 0, s>>>(d_args, echo);
     long long e[8];
@@ -412,86 +557,44 @@ extern "C" int dpe_pm_run(dpe_ctx *ctx, const dpe_problem *p, dpe_pm_out *out) {
       }
   }
 #endif
-  DPE_TRY(cudaEventRecord(ctx->ev0, s));
-  const dim3 fg = full_grid(W, H), hg = half_grid(W, H);
-  DPE_TIMED(ctx, KID_INIT_STATE, s, k_init_state<<<fg, kFullBlock, 0, s>>>(d_args, plane_in, views_in, weak_in, weak_flag));
-  PM_LAUNCHED("k_init_state", s);
-  if (a.P.use_APD) {
-    size_t tmp_bytes = 0;
-    cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, weak_flag, a.nmap, (int)L, s);
-    void *tmp = A.get<uint8_t>("scan_tmp", tmp_bytes + 16);
-    if (!tmp) return DPE_ERR_OUT_OF_MEMORY;
-    DPE_TRY(cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, weak_flag, a.nmap, (int)L, s));
+  SequenceGrids g;
+  if (n == 1) {
+    const PMArgs &a = ps[0].a;
+    const Launch one{d_args, nullptr, 1};
+    g.full = g.half = g.prep = g.eval = one;
+    g.fg = full_grid(a.W, a.H);
+    g.hg = half_grid(a.W, a.H);
+    g.gp = list_grid(ctx, (long long)ps[0].wcap);
+    g.ge = list_grid(ctx, (long long)ps[0].wcap * 10 * (a.N - 1));
   } else {
-    DPE_TRY(cudaMemsetAsync(a.nmap, 0, L * 4, s));
-  }
-  DPE_TIMED(ctx, KID_GEN_EDGE_INFORM, s, k_gen_edge_inform<<<fg, kFullBlock, 0, s>>>(d_args));
-  PM_LAUNCHED("k_gen_edge_inform", s);
-  DPE_TIMED(ctx, KID_FIND_NEAREST, s, k_find_nearest_strong<<<fg, kFullBlock, 0, s>>>(d_args));
-  PM_LAUNCHED("k_find_nearest_strong", s);
-  DPE_TIMED(ctx, KID_GEN_NEIGHBOURS, s, k_gen_neighbours<<<fg, kFullBlock, 0, s>>>(d_args));
-  PM_LAUNCHED("k_gen_neighbours", s);
-  DPE_TIMED(ctx, KID_NEIGHBOUR_UPDATE, s, k_neighbour_update<<<fg, kFullBlock, 0, s>>>(d_args));
-  PM_LAUNCHED("k_neighbour_update", s);
-  if (a.P.use_APD) {
-    // WEAK pixels per colour, in raster order; the states are final for the iterations
-    size_t sel_bytes = 0;
-    thrust::counting_iterator<int> first(0);
-    cub::DeviceSelect::If(nullptr, sel_bytes, first, const_cast<int *>(a.wlist[0]), const_cast<int *>(a.wcount),
-                          (int)L, WeakOfColour{a.weak, W, 0}, s);
-    void *sel_tmp = A.get<uint8_t>("select_tmp", sel_bytes + 16);
-    if (!sel_tmp) return DPE_ERR_OUT_OF_MEMORY;
-    for (int parity = 0; parity < 2; ++parity)
-      DPE_TRY(cub::DeviceSelect::If(sel_tmp, sel_bytes, first, const_cast<int *>(a.wlist[parity]),
-                                    const_cast<int *>(a.wcount) + parity, (int)L, WeakOfColour{a.weak, W, parity}, s));
-  }
-  DPE_TIMED(ctx, KID_RANDOM_INIT, s, with_stage(staging, [&](auto st) { k_random_init<decltype(st)::value><<<fg, kFullBlock, 0, s>>>(d_args); }));
-  PM_LAUNCHED("k_random_init", s);
-  for (int it = 0; it < a.P.max_iterations; ++it) {
-    for (int parity = 0; parity < 2; ++parity) {
-      if (a.P.use_edge) {
-        DPE_TRY(cudaMemcpyAsync(a.plane_snap, a.plane, L * sizeof(float4), cudaMemcpyDeviceToDevice, s));
-        DPE_TRY(cudaMemcpyAsync(a.cost_snap, a.cost, L * 4, cudaMemcpyDeviceToDevice, s));
-      }
-      DPE_TIMED(ctx, KID_STRONG_UPDATE, s, launch_strong_update(staging, a.gn != 0, hg, s, d_args, it, parity));
-      PM_LAUNCHED("k_strong_update", s);
+    // the problems' grids laid end to end: prefix tables per grid kind
+    std::vector<int> start(4 * (n + 1), 0);
+    for (int b = 0; b < n; ++b) {
+      const PMArgs &a = ps[b].a;
+      const dim3 f = full_grid(a.W, a.H), h = half_grid(a.W, a.H);
+      start[0 * (n + 1) + b + 1] = start[0 * (n + 1) + b] + (int)(f.x * f.y);
+      start[1 * (n + 1) + b + 1] = start[1 * (n + 1) + b] + (int)(h.x * h.y);
+      start[2 * (n + 1) + b + 1] = start[2 * (n + 1) + b] + (int)list_grid(ctx, (long long)ps[b].wcap);
+      start[3 * (n + 1) + b + 1] =
+          start[3 * (n + 1) + b] + (int)list_grid(ctx, (long long)ps[b].wcap * 10 * (a.N - 1));
     }
-    DPE_TIMED(ctx, KID_RANSAC, s, k_ransac_fit_plane<<<fg, kFullBlock, 0, s>>>(d_args));
-    PM_LAUNCHED("k_ransac_fit_plane", s);
-    if (a.P.use_APD)
-      for (int parity = 0; parity < 2; ++parity) {
-        const unsigned gp = list_grid(ctx, (long long)wcap);
-        const unsigned ge = list_grid(ctx, (long long)wcap * 10 * (N - 1));
-        DPE_TIMED(ctx, KID_WEAK_PREPARE, s, k_weak_prepare<<<gp, 128, 0, s>>>(d_args, parity));
-        PM_LAUNCHED("k_weak_prepare", s);
-        DPE_TIMED(ctx, KID_WEAK_EVAL, s, with_stage(staging, [&](auto st) { k_weak_eval<false, decltype(st)::value><<<ge, 128, 0, s>>>(d_args, parity); }));
-        PM_LAUNCHED("k_weak_eval", s);
-        DPE_TIMED(ctx, KID_WEAK_DECIDE, s, k_weak_decide<<<gp, 128, 0, s>>>(d_args, it, parity));
-        PM_LAUNCHED("k_weak_decide", s);
-        DPE_TIMED(ctx, KID_WEAK_EVAL, s, with_stage(staging, [&](auto st) { k_weak_eval<true, decltype(st)::value><<<ge, 128, 0, s>>>(d_args, parity); }));
-        PM_LAUNCHED("k_weak_eval", s);
-        DPE_TIMED(ctx, KID_WEAK_FINISH, s, with_stage(staging, [&](auto st) { k_weak_finish<decltype(st)::value><<<gp, 128, 0, s>>>(d_args, parity); }));
-        PM_LAUNCHED("k_weak_finish", s);
-      }
+    DPE_TRY(cudaMemcpyAsync(d_start, start.data(), start.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+    g.full = Launch{d_args, d_start + 0 * (n + 1), n};
+    g.half = Launch{d_args, d_start + 1 * (n + 1), n};
+    g.prep = Launch{d_args, d_start + 2 * (n + 1), n};
+    g.eval = Launch{d_args, d_start + 3 * (n + 1), n};
+    g.fg = dim3(start[0 * (n + 1) + n]);
+    g.hg = dim3(start[1 * (n + 1) + n]);
+    g.gp = (unsigned)start[2 * (n + 1) + n];
+    g.ge = (unsigned)start[3 * (n + 1) + n];
+    // blocks keep the single-problem shapes (16x8 full, 32x4 half): only the block index is 1D
   }
-  DPE_TIMED(ctx, KID_DEPTH_NORMAL, s, k_get_depth_normal<<<fg, kFullBlock, 0, s>>>(d_args));
-  PM_LAUNCHED("k_get_depth_normal", s);
-  for (int parity = 0; parity < 2; ++parity) {
-    DPE_TIMED(ctx, KID_FILTER, s, k_filter_strong<<<hg, kHalfBlock, 0, s>>>(d_args, parity));
-    PM_LAUNCHED("k_filter_strong", s);
-  }
-  DPE_TIMED(ctx, KID_DEPTH_TO_WEAK, s, with_stage(staging, [&](auto st) { k_depth_to_weak<decltype(st)::value><<<fg, kFullBlock, 0, s>>>(d_args, a.weak); }));
-  PM_LAUNCHED("k_depth_to_weak", s);
-  DPE_TIMED(ctx, KID_LOCAL_REFINE, s, with_stage(staging, [&](auto st) { k_local_refine<decltype(st)::value><<<fg, kFullBlock, 0, s>>>(d_args); }));
-  PM_LAUNCHED("k_local_refine", s);
+  DPE_TRY(cudaEventRecord(ctx->ev0, s));
+  int st = run_sequence(ctx, ps.data(), n, d_args, g);
+  if (st) return st;
   DPE_TRY(cudaEventRecord(ctx->ev1, s));
-
-  // ---- outputs (DPE.cu:3258-3260)
-  const cudaMemcpyKind d2o = host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
-  DPE_TRY(cudaMemcpyAsync(out->plane, a.plane, L * sizeof(float4), d2o, s));
-  DPE_TRY(cudaMemcpyAsync(out->weak, a.weak, L, d2o, s));
-  DPE_TRY(cudaMemcpyAsync(out->selected_views, a.views, L * 4, d2o, s));
-  if (out->costs) DPE_TRY(cudaMemcpyAsync(out->costs, a.cost, L * 4, d2o, s));
+  for (int b = 0; b < n; ++b)
+    if ((st = copy_outputs(ctx, ps[b], problems[b], outs[b]))) return st;
   unsigned long long cnt[2 * KID_COUNT] = {};
   if (ctx->count_evals) DPE_TRY(cudaMemcpyAsync(cnt, counters, sizeof(cnt), cudaMemcpyDeviceToHost, s));
   DPE_TRY(cudaStreamSynchronize(s));
@@ -505,10 +608,40 @@ extern "C" int dpe_pm_run(dpe_ctx *ctx, const dpe_problem *p, dpe_pm_out *out) {
   }
   float ms = 0.f;
   DPE_TRY(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
-  out->gpu_ms = ms;
-  out->strong_ncc_evals = strong_total;
-  out->weak_ncc_evals = weak_total;
+  for (int b = 0; b < n; ++b) {  // the batch's totals, reported on every output
+    outs[b]->gpu_ms = ms;
+    outs[b]->strong_ncc_evals = strong_total;
+    outs[b]->weak_ncc_evals = weak_total;
+  }
   return DPE_OK;
+}
+
+}  // namespace
+
+extern "C" int dpe_pm_run(dpe_ctx *ctx, const dpe_problem *p, dpe_pm_out *out) {
+  if (!ctx || !out) return DPE_ERR_INVALID_ARGUMENT;
+  int st = check_problem(p);
+  if (st) return st;
+  if (!out->plane || !out->weak || !out->selected_views) return DPE_ERR_INVALID_ARGUMENT;
+  return pm_run_problems(ctx, &p, 1, &out);
+}
+
+extern "C" int dpe_pm_run_batch(dpe_ctx *ctx, const dpe_problem *problems, int count, dpe_pm_out *outs) {
+  if (!ctx || !problems || !outs || count < 1 || count > DPE_MAX_BATCH) return DPE_ERR_INVALID_ARGUMENT;
+  std::vector<const dpe_problem *> pp(count);
+  std::vector<dpe_pm_out *> po(count);
+  for (int b = 0; b < count; ++b) {
+    int st = check_problem(&problems[b]);
+    if (st) return st;
+    if (!outs[b].plane || !outs[b].weak || !outs[b].selected_views) return DPE_ERR_INVALID_ARGUMENT;
+    const dpe_params &P = problems[b].params, &P0 = problems[0].params;
+    if (P.state != P0.state || P.use_APD != P0.use_APD || P.use_edge != P0.use_edge ||
+        P.geom_consistency != P0.geom_consistency || P.max_iterations != P0.max_iterations)
+      return DPE_ERR_INVALID_ARGUMENT;  // one kernel sequence: the schedule flags must agree
+    pp[b] = &problems[b];
+    po[b] = &outs[b];
+  }
+  return pm_run_problems(ctx, pp.data(), count, po.data());
 }
 
 // ------------------------------------------------------------------ dpe_ncc_eval
@@ -525,7 +658,7 @@ __global__ void k_ncc_queries(const PMArgs *__restrict__ pa, int64_t n, const in
     out[k] = __int_as_float(0x7fffffff);
     return;
   }
-  RefWindow rw;
+  DPE_REF_WINDOW(rw);
   build_ref_window(a, px[k], py[k], rw, KID_NCC_QUERY);
   out[k] = ncc_strong(a, px[k], py[k], src[k], pl[k], rw);
 }
@@ -594,7 +727,7 @@ __global__ void k_ncc_grad(const PMArgs *__restrict__ pa, int64_t n, const int32
   const PMArgs &a = *pa;
   const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
-  RefWindow rw;
+  DPE_REF_WINDOW(rw);
   build_ref_window(a, px[k], py[k], rw, KID_NCC_QUERY);
   float g[4];
   const int s = src[k];

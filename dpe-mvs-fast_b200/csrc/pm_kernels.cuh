@@ -1,8 +1,8 @@
 // pm_kernels.cuh -- the per-view PatchMatch kernels (one thread per pixel of a pass).
 //
 // Kernel order and per-pixel semantics follow DPE::RunPatchMatch (DPE.cu:3130-3262).  B200
-// design points: all per-call constants (cameras, relative poses, params, pointers) travel in one
-// __grid_constant__ parameter block; state is structure-of-arrays; view weights are packed as
+// design points: all per-call constants (cameras, relative poses, params, pointers) live in one
+// argument block in device memory (one per problem of a batch); state is structure-of-arrays; view weights are packed as
 // 4-bit counts (16 B per pixel instead of 32); the strong NCC's reference window is built once
 // per thread and reused by every hypothesis and source view; the same-colour race of the
 // edge-aware update is removed by reading candidates from a pre-pass snapshot.
@@ -14,17 +14,50 @@ namespace dpe {
 
 __device__ __constant__ const int kDir[8][2] = {{0, -1}, {0, 1}, {-1, 0}, {1, 0}, {-1, -1}, {1, 1}, {-1, 1}, {1, -1}};
 
+// ------------------------------------------------------------------ launch geometry
+// A kernel runs either for one problem (a 2D grid over its pixels, or a 1D grid over a work list)
+// or for a batch of problems in one launch (dpe_pm_run_batch): the batch's grid is the problems'
+// grids laid end to end in one dimension, and each block finds its problem in a prefix table of
+// block counts.
+enum GridKind { kGridFull = 0, kGridHalf = 1, kGridList = 2 };
+struct Launch {
+  const PMArgs *args;  // [nprob] per-problem argument blocks
+  const int *start;    // batched: [nprob + 1] first block of each problem; null for one problem
+  int nprob;
+};
+// This block's problem, its coordinates in the problem's own grid, and that grid's width.
+struct Blk {
+  const PMArgs *a;
+  int x, y, gx;
+};
+template <int kKind>
+__device__ __forceinline__ Blk resolve(const Launch &L) {
+  if (!L.start) return Blk{L.args, (int)blockIdx.x, (int)blockIdx.y, (int)gridDim.x};
+  const int f = (int)blockIdx.x;
+  int lo = 0, hi = L.nprob;  // the last problem whose first block is <= f
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (L.start[mid] <= f) lo = mid;
+    else hi = mid;
+  }
+  const PMArgs *a = L.args + lo;
+  const int local = f - L.start[lo];
+  const int gx = kKind == kGridFull ? (a->W + 15) / 16 : kKind == kGridHalf ? (a->W + 31) / 32
+                                                                            : L.start[lo + 1] - L.start[lo];
+  return Blk{a, local % gx, local / gx, gx};
+}
+
 // pixel of colour `parity` ((x + y) % 2) handled by this thread of a half-height grid
-__device__ __forceinline__ bool colour_pixel(const PMArgs &a, int parity, int *px, int *py) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  const int yy = blockIdx.y * blockDim.y + threadIdx.y;
+__device__ __forceinline__ bool colour_pixel(const PMArgs &a, const Blk &B, int parity, int *px, int *py) {
+  const int x = B.x * blockDim.x + threadIdx.x;
+  const int yy = B.y * blockDim.y + threadIdx.y;
   const int y = 2 * yy + ((x + parity) & 1);
   *px = x; *py = y;
   return x < a.W && y < a.H;
 }
-__device__ __forceinline__ bool full_pixel(const PMArgs &a, int *px, int *py) {
-  *px = blockIdx.x * blockDim.x + threadIdx.x;
-  *py = blockIdx.y * blockDim.y + threadIdx.y;
+__device__ __forceinline__ bool full_pixel(const PMArgs &a, const Blk &B, int *px, int *py) {
+  *px = B.x * blockDim.x + threadIdx.x;
+  *py = B.y * blockDim.y + threadIdx.y;
   return *px < a.W && *py < a.H;
 }
 
@@ -62,11 +95,12 @@ __global__ void k_stage_pairs(const float *__restrict__ pad, uint32_t *__restric
   out[o] = a | (b << 16);
 }
 
-__global__ void k_init_state(const PMArgs *__restrict__ pa, const float4 *plane_in, const uint32_t *views_in,
+__global__ void k_init_state(const Launch lc, const float4 *plane_in, const uint32_t *views_in,
                              const uint8_t *weak_in, int *weak_flag) {
-  const PMArgs &a = *pa;
+  const Blk B = resolve<kGridFull>(lc);
+  const PMArgs &a = *B.a;
   int px, py;
-  if (!full_pixel(a, &px, &py)) return;
+  if (!full_pixel(a, B, &px, &py)) return;
   const int c = px + py * a.W;
   a.plane[c] = (a.P.state != DPE_FIRST_INIT && plane_in) ? plane_in[c] : make_float4(0, 0, 0, 0);
   a.views[c] = (a.P.state != DPE_FIRST_INIT && views_in) ? views_in[c] : 0u;
@@ -83,10 +117,11 @@ __global__ void k_init_state(const PMArgs *__restrict__ pa, const float4 *plane_
 }
 
 // ------------------------------------------------------------------ GenEdgeInform (DPE.cu:2487-2595)
-__global__ void k_gen_edge_inform(const PMArgs *__restrict__ pa) {
-  const PMArgs &a = *pa;
+__global__ void k_gen_edge_inform(const Launch lc) {
+  const Blk B = resolve<kGridFull>(lc);
+  const PMArgs &a = *B.a;
   int px, py;
-  if (!full_pixel(a, &px, &py)) return;
+  if (!full_pixel(a, B, &px, &py)) return;
   const int W = a.W, H = a.H, center = px + py * W;
   if (a.P.use_edge) {
     short2 *en = &a.edge_neigh[(size_t)center * 8];
@@ -134,10 +169,11 @@ __global__ void k_gen_edge_inform(const PMArgs *__restrict__ pa) {
 }
 
 // ------------------------------------------------------------------ FindNearestStrongPoint (DPE.cu:2859-2893)
-__global__ void k_find_nearest_strong(const PMArgs *__restrict__ pa) {
-  const PMArgs &a = *pa;
+__global__ void k_find_nearest_strong(const Launch lc) {
+  const Blk B = resolve<kGridFull>(lc);
+  const PMArgs &a = *B.a;
   int px, py;
-  if (!full_pixel(a, &px, &py)) return;
+  if (!full_pixel(a, B, &px, &py)) return;
   const int W = a.W, H = a.H, center = px + py * W;
   short2 res = make_short2(-1, -1);
   if (a.weak[center] == DPE_WEAK) {
@@ -221,10 +257,11 @@ __device__ __forceinline__ void sort_small(float *d, int n) {
 }
 
 // ------------------------------------------------------------------ GenNeighbours (DPE.cu:2107-2467)
-__global__ void __launch_bounds__(128) k_gen_neighbours(const PMArgs *__restrict__ pa) {
-  const PMArgs &a = *pa;
+__global__ void __launch_bounds__(128) k_gen_neighbours(const Launch lc) {
+  const Blk B = resolve<kGridFull>(lc);
+  const PMArgs &a = *B.a;
   int px, py;
-  if (!full_pixel(a, &px, &py)) return;
+  if (!full_pixel(a, B, &px, &py)) return;
   const int W = a.W, H = a.H, center = px + py * W;
   if (a.weak[center] != DPE_WEAK) return;
   constexpr int kMaxPts = 64;
@@ -458,23 +495,25 @@ __global__ void __launch_bounds__(128) k_gen_neighbours(const PMArgs *__restrict
   a.reliable[center] = 1;
 }
 
-__global__ void k_neighbour_update(const PMArgs *__restrict__ pa) {
-  const PMArgs &a = *pa;
+__global__ void k_neighbour_update(const Launch lc) {
+  const Blk B = resolve<kGridFull>(lc);
+  const PMArgs &a = *B.a;
   int px, py;
-  if (!full_pixel(a, &px, &py)) return;
+  if (!full_pixel(a, B, &px, &py)) return;
   const int c = px + py * a.W;
   if (a.weak[c] == DPE_WEAK && a.reliable[c] != 1) a.weak[c] = DPE_UNKNOWN;
 }
 
 // ------------------------------------------------------------------ RandomInitialization (DPE.cu:1039-1067, 784-861)
 template <int kStage>
-__global__ void __launch_bounds__(128) k_random_init(const PMArgs *__restrict__ pa) {
-  const PMArgs &a = *pa;
+__global__ void __launch_bounds__(128, DPE_COST_MIN_BLOCKS) k_random_init(const Launch lc) {
+  const Blk B = resolve<kGridFull>(lc);
+  const PMArgs &a = *B.a;
   int px, py;
-  if (!full_pixel(a, &px, &py)) return;
+  if (!full_pixel(a, B, &px, &py)) return;
   const int center = px + py * a.W;
   const dpe_camera &rc = a.cam[0];
-  RefWindow rw;
+  DPE_REF_WINDOW(rw);
   build_ref_window(a, px, py, rw, KID_RANDOM_INIT);
   const int n = a.N - 1;
   if (a.P.state == DPE_FIRST_INIT) {
@@ -640,16 +679,17 @@ __device__ __forceinline__ void gn_hypothesis(const PMArgs &a, int px, int py, c
 
 // ------------------------------------------------------------------ strong update (DPE.cu:1218-1670, 1069-1122)
 template <int kStage, bool kGN>
-__global__ void __launch_bounds__(128) k_strong_update(const PMArgs *__restrict__ pa, int iter, int parity) {
-  const PMArgs &a = *pa;
+__global__ void __launch_bounds__(128, DPE_COST_MIN_BLOCKS) k_strong_update(const Launch lc, int iter, int parity) {
+  const Blk B = resolve<kGridHalf>(lc);
+  const PMArgs &a = *B.a;
   int px, py;
-  if (!colour_pixel(a, parity, &px, &py)) return;
+  if (!colour_pixel(a, B, parity, &px, &py)) return;
   const int W = a.W, H = a.H, n = a.N - 1;
   const int center = py * W + px;
   const long long L = (long long)W * H;
   if (G(a.weak, center, L, 201) == DPE_WEAK) return;
   const dpe_camera &rc = a.cam[0];
-  RefWindow rw;
+  DPE_REF_WINDOW(rw);
   build_ref_window(a, px, py, rw, KID_STRONG_UPDATE);
   float cost_array[8][kMaxSrc];
   for (int d = 0; d < 8; ++d)
@@ -890,10 +930,11 @@ __global__ void __launch_bounds__(128) k_strong_update(const PMArgs *__restrict_
 }
 
 // ------------------------------------------------------------------ RANSACToGetFitPlane (DPE.cu:2895-3128)
-__global__ void __launch_bounds__(128) k_ransac_fit_plane(const PMArgs *__restrict__ pa) {
-  const PMArgs &a = *pa;
+__global__ void __launch_bounds__(128) k_ransac_fit_plane(const Launch lc) {
+  const Blk B = resolve<kGridFull>(lc);
+  const PMArgs &a = *B.a;
   int px, py;
-  if (!full_pixel(a, &px, &py)) return;
+  if (!full_pixel(a, B, &px, &py)) return;
   const int W = a.W, center = px + py * W;
   if (a.weak[center] != DPE_WEAK) { a.fit_plane[center] = a.plane[center]; return; }
   Rng rng = make_rng(a, center);
@@ -1045,11 +1086,12 @@ __global__ void __launch_bounds__(128) k_ransac_fit_plane(const PMArgs *__restri
 // list does not matter.  Work items are strided over a grid sized for the GPU; the list lengths
 // stay on the device.
 
-__global__ void __launch_bounds__(128) k_weak_prepare(const PMArgs *__restrict__ pa, int parity) {
-  const PMArgs &a = *pa;
+__global__ void __launch_bounds__(128) k_weak_prepare(const Launch lc, int parity) {
+  const Blk B = resolve<kGridList>(lc);
+  const PMArgs &a = *B.a;
   const int count = a.wcount[parity];
   const int *list = a.wlist[parity];
-  for (int slot = blockIdx.x * blockDim.x + threadIdx.x; slot < count; slot += gridDim.x * blockDim.x) {
+  for (int slot = B.x * blockDim.x + threadIdx.x; slot < count; slot += B.gx * blockDim.x) {
     const int center = list[slot];
     const int px = center % a.W, py = center / a.W;
     const float ref_center = texel(a, 0, px, py);
@@ -1085,8 +1127,9 @@ __global__ void __launch_bounds__(128) k_weak_prepare(const PMArgs *__restrict__
 // sources the pixel sampled.  Unevaluated candidates keep the fused form's initial costs (0, and 2
 // for the first candidate's first source: quirk Q2).
 template <bool kRandom, int kStage>
-__global__ void __launch_bounds__(128) k_weak_eval(const PMArgs *__restrict__ pa, int parity) {
-  const PMArgs &a = *pa;
+__global__ void __launch_bounds__(128) k_weak_eval(const Launch lc, int parity) {
+  const Blk B = resolve<kGridList>(lc);
+  const PMArgs &a = *B.a;
   const int n = a.N - 1;
   const int hyps = kRandom ? 5 : 10;
   const long long per = (long long)hyps * n;
@@ -1095,8 +1138,7 @@ __global__ void __launch_bounds__(128) k_weak_eval(const PMArgs *__restrict__ pa
   const bool geom = a.P.geom_consistency != 0;
   float *costs = kRandom ? a.wcost_r : a.wcost;
   float *geoms = kRandom ? a.wgeom_r : a.wgeom;
-  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
-       t += (long long)gridDim.x * blockDim.x) {
+  for (long long t = (long long)B.x * blockDim.x + threadIdx.x; t < total; t += (long long)B.gx * blockDim.x) {
     const int slot = (int)(t / per);
     const int r = (int)(t - (long long)slot * per);
     const int h = r / n, j = r - h * n;
@@ -1127,8 +1169,9 @@ __global__ void __launch_bounds__(128) k_weak_eval(const PMArgs *__restrict__ pa
   }
 }
 
-__global__ void __launch_bounds__(128) k_weak_decide(const PMArgs *__restrict__ pa, int iter, int parity) {
-  const PMArgs &a = *pa;
+__global__ void __launch_bounds__(128) k_weak_decide(const Launch lc, int iter, int parity) {
+  const Blk B = resolve<kGridList>(lc);
+  const PMArgs &a = *B.a;
   const int n = a.N - 1, W = a.W;
   const int count = a.wcount[parity];
   const int *list = a.wlist[parity];
@@ -1141,7 +1184,7 @@ __global__ void __launch_bounds__(128) k_weak_decide(const PMArgs *__restrict__ 
   float final_costs[8];
   bool flag[8];
   float4 cand[8];
-  for (int slot = blockIdx.x * blockDim.x + threadIdx.x; slot < count; slot += gridDim.x * blockDim.x) {
+  for (int slot = B.x * blockDim.x + threadIdx.x; slot < count; slot += B.gx * blockDim.x) {
     const int center = list[slot];
     const int px = center % W, py = center / W;
     const float *ca = a.wcost + (size_t)slot * 10 * n;
@@ -1227,8 +1270,9 @@ __global__ void __launch_bounds__(128) k_weak_decide(const PMArgs *__restrict__ 
 }
 
 template <int kStage>
-__global__ void __launch_bounds__(128) k_weak_finish(const PMArgs *__restrict__ pa, int parity) {
-  const PMArgs &a = *pa;
+__global__ void __launch_bounds__(128) k_weak_finish(const Launch lc, int parity) {
+  const Blk B = resolve<kGridList>(lc);
+  const PMArgs &a = *B.a;
   const int n = a.N - 1, W = a.W;
   const int count = a.wcount[parity];
   const int *list = a.wlist[parity];
@@ -1236,7 +1280,7 @@ __global__ void __launch_bounds__(128) k_weak_finish(const PMArgs *__restrict__ 
   const bool geom = a.P.geom_consistency != 0;
   const float gf = a.P.geom_factor;
   const float dmin = a.P.depth_min, dmax = a.P.depth_max;
-  for (int slot = blockIdx.x * blockDim.x + threadIdx.x; slot < count; slot += gridDim.x * blockDim.x) {
+  for (int slot = B.x * blockDim.x + threadIdx.x; slot < count; slot += B.gx * blockDim.x) {
     const int center = list[slot];
     const int px = center % W, py = center / W;
     float4 pl_now = a.wstate[(size_t)slot * 2];
@@ -1272,7 +1316,7 @@ __global__ void __launch_bounds__(128) k_weak_finish(const PMArgs *__restrict__ 
     }
     a.plane[center] = pl_final;
     // final re-cost with the strong window (DPE.cu:1849-1865); the radius swap there has no effect
-    RefWindow rw;
+    DPE_REF_WINDOW(rw);
     build_ref_window(a, px, py, rw, KID_WEAK_FINISH);
     uint8_t vw[32];
     int act[kMaxSrc];
@@ -1286,10 +1330,11 @@ __global__ void __launch_bounds__(128) k_weak_finish(const PMArgs *__restrict__ 
 }
 
 // ------------------------------------------------------------------ post passes
-__global__ void k_get_depth_normal(const PMArgs *__restrict__ pa) {
-  const PMArgs &a = *pa;
+__global__ void k_get_depth_normal(const Launch lc) {
+  const Blk B = resolve<kGridFull>(lc);
+  const PMArgs &a = *B.a;
   int px, py;
-  if (!full_pixel(a, &px, &py)) return;
+  if (!full_pixel(a, B, &px, &py)) return;
   const int c = py * a.W + px;
   float4 pl = a.plane[c];
   pl.w = depth_from_plane(a.cam[0], pl, px, py);
@@ -1297,10 +1342,11 @@ __global__ void k_get_depth_normal(const PMArgs *__restrict__ pa) {
 }
 
 // CheckerboardFilterStrong (DPE.cu:1961-2071)
-__global__ void k_filter_strong(const PMArgs *__restrict__ pa, int parity) {
-  const PMArgs &a = *pa;
+__global__ void k_filter_strong(const Launch lc, int parity) {
+  const Blk B = resolve<kGridHalf>(lc);
+  const PMArgs &a = *B.a;
   int px, py;
-  if (!colour_pixel(a, parity, &px, &py)) return;
+  if (!colour_pixel(a, B, parity, &px, &py)) return;
   const int W = a.W, H = a.H, center = py * W + px;
   if (a.weak[center] == DPE_WEAK) return;
   if (a.cost[center] < 0.001f) return;
@@ -1358,18 +1404,19 @@ __device__ __forceinline__ void sweep_setup(const PMArgs &a, int px, int py, con
 
 // DepthToWeak (DPE.cu:2597-2751)
 template <int kStage>
-__global__ void __launch_bounds__(128) k_depth_to_weak(const PMArgs *__restrict__ pa, uint8_t *weak_out) {
-  const PMArgs &a = *pa;
+__global__ void __launch_bounds__(128, DPE_COST_MIN_BLOCKS) k_depth_to_weak(const Launch lc) {
+  const Blk B = resolve<kGridFull>(lc);
+  const PMArgs &a = *B.a;
   int px, py;
-  if (!full_pixel(a, &px, &py)) return;
+  if (!full_pixel(a, B, &px, &py)) return;
   const int W = a.W, H = a.H, center = px + py * W, margin = 6;
-  if (px < margin || py < margin || px >= W - margin || py >= H - margin) { weak_out[center] = DPE_UNKNOWN; return; }
+  if (px < margin || py < margin || px >= W - margin || py >= H - margin) { a.weak[center] = DPE_UNKNOWN; return; }
   const dpe_camera &rc = a.cam[0];
-  RefWindow rw;
+  DPE_REF_WINDOW(rw);
   build_ref_window(a, px, py, rw, KID_DEPTH_TO_WEAK);
   Sweep s;
   sweep_setup<kStage>(a, px, py, rw, s);
-  if (s.depth == 0 || s.valid == 0) { weak_out[center] = DPE_UNKNOWN; return; }
+  if (s.depth == 0 || s.valid == 0) { a.weak[center] = DPE_UNKNOWN; return; }
   s.cost_now /= s.weight_normal;
   s.base_line /= s.valid;
   const float disp = rc.K[0] * s.base_line / s.depth;
@@ -1412,18 +1459,19 @@ __global__ void __launch_bounds__(128) k_depth_to_weak(const PMArgs *__restrict_
     var /= (peaks - 1);
     res = var > 0.2f ? DPE_STRONG : DPE_WEAK;
   }
-  weak_out[center] = res;
+  a.weak[center] = res;
 }
 
 // LocalRefine (DPE.cu:2753-2839)
 template <int kStage>
-__global__ void __launch_bounds__(128) k_local_refine(const PMArgs *__restrict__ pa) {
-  const PMArgs &a = *pa;
+__global__ void __launch_bounds__(128, DPE_COST_MIN_BLOCKS) k_local_refine(const Launch lc) {
+  const Blk B = resolve<kGridFull>(lc);
+  const PMArgs &a = *B.a;
   int px, py;
-  if (!full_pixel(a, &px, &py)) return;
+  if (!full_pixel(a, B, &px, &py)) return;
   const int center = px + py * a.W;
   const dpe_camera &rc = a.cam[0];
-  RefWindow rw;
+  DPE_REF_WINDOW(rw);
   build_ref_window(a, px, py, rw, KID_LOCAL_REFINE);
   Sweep s;
   sweep_setup<kStage>(a, px, py, rw, s);

@@ -114,7 +114,7 @@ class Limits(C.Structure):
 EXPORTED = ["dpe_status_string", "dpe_last_error", "dpe_params_default", "dpe_ctx_create", "dpe_ctx_destroy", "dpe_pm_run",
             "dpe_fuse", "dpe_ncc_eval", "dpe_ctx_set_eval_counting", "dpe_scene_run", "dpe_ctx_set_profiling",
             "dpe_ctx_reset_kernel_stats", "dpe_ctx_get_kernel_stats", "dpe_launch_count", "dpe_fp32_peak",
-            "dpe_ncc_eval_noalloc", "dpe_ncc_grad", "dpe_ctx_set_options"]
+            "dpe_ncc_eval_noalloc", "dpe_ncc_grad", "dpe_ctx_set_options", "dpe_pm_run_batch"]
 
 _lib = None
 
@@ -148,6 +148,7 @@ def load_library(path: Optional[str] = None) -> C.CDLL:
     lib.dpe_fp32_peak.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
     lib.dpe_ncc_eval_noalloc.argtypes = [C.POINTER(NCCQuery), C.c_void_p, C.c_void_p]
     lib.dpe_ctx_set_options.argtypes = [C.c_void_p, C.POINTER(Options)]
+    lib.dpe_pm_run_batch.argtypes = [C.c_void_p, C.POINTER(Problem), C.c_int, C.POINTER(PMOut)]
     lib.dpe_ncc_grad.argtypes = [C.c_void_p, C.POINTER(NCCQuery), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     if path is None:
         _lib = lib
@@ -288,6 +289,28 @@ class Context:
         out["strong_ncc_evals"] = int(po.strong_ncc_evals)
         out["weak_ncc_evals"] = int(po.weak_ncc_evals)
         return out
+
+    def pm_run_batch(self, calls: List[Dict]) -> List[Dict]:
+        """dpe_pm_run_batch on host arrays: each call a dict(images=, cameras=, params=, **pm_run keywords)."""
+        n = len(calls)
+        probs = (Problem * n)()
+        outs = (PMOut * n)()
+        results = []
+        for b, c in enumerate(calls):
+            kw = {k: v for k, v in c.items() if k not in ("images", "cameras", "params")}
+            probs[b] = build_problem(c["images"], c["cameras"], c["params"], **kw)
+            H, W = probs[b].height, probs[b].width
+            o = dict(plane=np.zeros((H, W, 4), np.float32), weak=np.zeros((H, W), np.uint8),
+                     views=np.zeros((H, W), np.uint32), costs=np.zeros((H, W), np.float32))
+            outs[b].plane, outs[b].weak = _ptr(o["plane"]), _ptr(o["weak"])
+            outs[b].selected_views, outs[b].costs = _ptr(o["views"]), _ptr(o["costs"])
+            results.append(o)
+        st = self.lib.dpe_pm_run_batch(self.handle, probs, n, outs)
+        if st != OK:
+            raise DPEError(st, "dpe_pm_run_batch")
+        for b in range(n):
+            results[b]["gpu_ms"] = outs[b].gpu_ms
+        return results
 
     # ------------------------------------------------------------------ fusion
     def fuse(self, views: List[Dict], mode: int = FUSE_FP64, capacity: Optional[int] = None,

@@ -251,6 +251,17 @@ int dpe_ctx_destroy(dpe_ctx *ctx);
  * (DPE.cpp:1071-1288, DPE.cu:3130-3262) for one reference view. */
 int dpe_pm_run(dpe_ctx *ctx, const dpe_problem *problem, dpe_pm_out *out);
 
+/* Batched form of dpe_pm_run (no reference counterpart; the reference runs one view per call):
+ * `count` independent per-view problems, each with its own size, images, cameras, inputs and
+ * seed, run through ONE kernel sequence -- every kernel is launched once for the whole batch, its
+ * grid the problems' grids laid end to end, so small views fill the GPU together.  The problems
+ * must agree on the schedule flags (params.state, use_APD, use_edge, geom_consistency,
+ * max_iterations); other parameters may differ.  Each problem's result equals its dpe_pm_run
+ * result.  outs[b].gpu_ms and the evaluation counts are the batch's totals.  count <=
+ * DPE_MAX_BATCH. */
+#define DPE_MAX_BATCH 256
+int dpe_pm_run_batch(dpe_ctx *ctx, const dpe_problem *problems, int count, dpe_pm_out *outs);
+
 /* Replaces the compute of RunFusion (DPE.cpp:1387-1548): returns the fused points in the
  * reference order (view order, then raster order).  Writing the PLY stays with the caller
  * (ExportPointCloud, DPE.cpp:532-572). */

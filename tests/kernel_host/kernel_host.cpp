@@ -27,7 +27,7 @@ static dim3 blockIdx, threadIdx, blockDim, gridDim;
 #define __device__
 #define __host__
 #define __forceinline__ inline
-#define __launch_bounds__(x)
+#define __launch_bounds__(...)
 #define __grid_constant__
 #define __constant__
 #define __restrict__
@@ -102,16 +102,17 @@ extern "C" int host_pm_run(const dpe_problem *p, dpe_pm_out *out) {
   int *weak_flag = alloc<int>(L);
   a.neigh = alloc<short2>(L * kNeighbours); a.lab_bound = alloc<short2>(L * 8);
   a.edge_neigh = alloc<short2>(L * 8); a.nearest = alloc<short2>(L);
+  const Launch one{&a, nullptr, 1};
   a.lowW = p->low_width; a.lowH = p->low_height;
   a.edge = p->edge; a.edge_low = p->edge_low_res; a.label = p->label;
   const dim3 fg((W + 15) / 16, (H + 7) / 8), fb(16, 8), hg((W + 31) / 32, ((H + 1) / 2 + 3) / 4), hb(32, 4);
-  launch(fg, fb, k_init_state, &a, (const float4 *)p->plane_in, p->selected_views_in, p->weak_in, weak_flag);
+  launch(fg, fb, k_init_state, one, (const float4 *)p->plane_in, p->selected_views_in, p->weak_in, weak_flag);
   int acc = 0;
   for (size_t i = 0; i < L; ++i) { a.nmap[i] = acc; acc += weak_flag[i]; }
-  launch(fg, fb, k_gen_edge_inform, &a);
-  launch(fg, fb, k_find_nearest_strong, &a);
-  launch(fg, fb, k_gen_neighbours, &a);
-  launch(fg, fb, k_neighbour_update, &a);
+  launch(fg, fb, k_gen_edge_inform, one);
+  launch(fg, fb, k_find_nearest_strong, one);
+  launch(fg, fb, k_gen_neighbours, one);
+  launch(fg, fb, k_neighbour_update, one);
   // WEAK pixels per colour in raster order (the cub select of dpe_pm_run)
   const size_t wcap = (L + 1) / 2;
   std::vector<int> wlist(2 * wcap), wcount(2, 0);
@@ -133,27 +134,27 @@ extern "C" int host_pm_run(const dpe_problem *p, dpe_pm_out *out) {
     a.wtab = wtab.data(); a.wwin = wwin.data(); a.whyp = whyp.data(); a.wstate = wstate.data();
     a.wcost = wcost.data(); a.wgeom = wgeom.data(); a.wcost_r = wcost_r.data(); a.wgeom_r = wgeom_r.data();
   }
-  launch(fg, fb, k_random_init<DPE_STAGE_FP32>, &a);
+  launch(fg, fb, k_random_init<DPE_STAGE_FP32>, one);
   for (int it = 0; it < a.P.max_iterations; ++it) {
     for (int parity = 0; parity < 2; ++parity) {
       if (a.P.use_edge) { memcpy(a.plane_snap, a.plane, L * 16); memcpy(a.cost_snap, a.cost, L * 4); }
-      launch(hg, hb, k_strong_update<DPE_STAGE_FP32, false>, &a, it, parity);
+      launch(hg, hb, k_strong_update<DPE_STAGE_FP32, false>, one, it, parity);
     }
-    launch(fg, fb, k_ransac_fit_plane, &a);
+    launch(fg, fb, k_ransac_fit_plane, one);
     if (a.P.use_APD)
       for (int parity = 0; parity < 2; ++parity) {
         const dim3 lg(7), lb(32);  // strided work lists: any grid covers them
-        launch(lg, lb, k_weak_prepare, &a, parity);
-        launch(lg, lb, k_weak_eval<false, DPE_STAGE_FP32>, &a, parity);
-        launch(lg, lb, k_weak_decide, &a, it, parity);
-        launch(lg, lb, k_weak_eval<true, DPE_STAGE_FP32>, &a, parity);
-        launch(lg, lb, k_weak_finish<DPE_STAGE_FP32>, &a, parity);
+        launch(lg, lb, k_weak_prepare, one, parity);
+        launch(lg, lb, k_weak_eval<false, DPE_STAGE_FP32>, one, parity);
+        launch(lg, lb, k_weak_decide, one, it, parity);
+        launch(lg, lb, k_weak_eval<true, DPE_STAGE_FP32>, one, parity);
+        launch(lg, lb, k_weak_finish<DPE_STAGE_FP32>, one, parity);
       }
   }
-  launch(fg, fb, k_get_depth_normal, &a);
-  for (int parity = 0; parity < 2; ++parity) launch(hg, hb, k_filter_strong, &a, parity);
-  launch(fg, fb, k_depth_to_weak<DPE_STAGE_FP32>, &a, a.weak);
-  launch(fg, fb, k_local_refine<DPE_STAGE_FP32>, &a);
+  launch(fg, fb, k_get_depth_normal, one);
+  for (int parity = 0; parity < 2; ++parity) launch(hg, hb, k_filter_strong, one, parity);
+  launch(fg, fb, k_depth_to_weak<DPE_STAGE_FP32>, one);
+  launch(fg, fb, k_local_refine<DPE_STAGE_FP32>, one);
   memcpy(out->plane, a.plane, L * 16);
   memcpy(out->weak, a.weak, L);
   memcpy(out->selected_views, a.views, L * 4);
