@@ -326,6 +326,33 @@ def run_ours(args):
     rel = np.concatenate([np.abs(res["depth"][v] - sc.depth[v]).ravel() / sc.depth[v].ravel() for v in range(V)])
     valid = np.concatenate([(res["depth"][v] > 0).ravel() for v in range(V)])
 
+    # the batched forms on the same scene (device-resident, 1 warm-up + 1 timed schedule each):
+    # all views of a call in one batch (reading the previous call's depths), then additionally
+    # FP16-staged sources and the Gauss-Newton plane hypothesis from the NCC adjoint
+    def accuracy(r):
+        rl = np.concatenate([np.abs(r["depth"][v] - sc.depth[v]).ravel() / sc.depth[v].ravel() for v in range(V)])
+        ok = np.concatenate([(r["depth"][v] > 0).ravel() for v in range(V)])
+        return float((rl[ok] < 0.01).mean()), float((rl[ok] < 0.001).mean())
+
+    plain_acc = accuracy(res)
+    forms = {}
+    if not args.no_forms:
+        for name, staging, gn in (("batched", D.STAGE_FP32, 0), ("batched_fp16_gn", D.STAGE_FP16, 1)):
+            ctx.set_options(staging=staging, gn_refine=gn)
+            ctx.scene_run(gray_d, bgr_d, cams, srcs, edges_d, labels_d, seed=7, memory=D.MEM_DEVICE, want_maps=False,
+                          batch_views=True, **kw)
+            torch.cuda.synchronize()
+            r = ctx.scene_run(gray_d, bgr_d, cams, srcs, edges_d, labels_d, seed=7, memory=D.MEM_DEVICE,
+                              want_maps=True, batch_views=True, **kw)
+            ctx.set_options()
+            fms = r["gpu_ms"]
+            fv = pix_step * world / (fms / 1e3)
+            a1, a01 = accuracy(r)
+            forms[name] = dict(value=round(fv, 4), unit=UNIT, ms_per_step=round(fms, 3), vs_plain=round(fv / value, 3),
+                               depth_within_1pct=round(a1, 4), depth_within_0_1pct=round(a01, 4),
+                               staging={D.STAGE_FP32: "fp32", D.STAGE_FP16: "fp16"}[staging],
+                               gauss_newton=bool(gn), points=int(r["points"]))
+
     # roofline of the dominant kernel (device time share in the timed region)
     dom = max(stats.items(), key=lambda kv: kv[1]["ms"])
     dname, dstat = dom
@@ -369,7 +396,8 @@ def run_ours(args):
                 roofline=roofline, cpu_baseline=cpu, clocks=clocks.summary(), gpu_launches=int(launches),
                 e2e=dict(value=round(e2e_value, 4), unit=UNIT, h2d_bytes_per_step=int(h2d), d2h_bytes_per_step=int(d2h)),
                 kernel_ms_per_step={k: round(v["ms"] / max(1, args.steps), 3) for k, v in
-                                    sorted(stats.items(), key=lambda kv: -kv[1]["ms"])})
+                                    sorted(stats.items(), key=lambda kv: -kv[1]["ms"])},
+                forms=forms or None)
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
@@ -383,6 +411,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-forms", action="store_true", help="skip the batched / FP16 / Gauss-Newton forms")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

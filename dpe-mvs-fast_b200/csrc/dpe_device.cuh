@@ -21,10 +21,21 @@ constexpr int kMaxSrc = DPE_MAX_IMAGES - 1;
 constexpr int kNeighbours = DPE_NEIGHBOUR_NUM;
 constexpr int kMaxWin = 6;  // taps per window side for radius 5 / step 2 (DPE.cu:728-737)
 // Minimum resident blocks per multiprocessor requested for the strong-window cost kernels
-// (__launch_bounds__): bounds their registers, trading spills against occupancy.
+// (__launch_bounds__): bounds their registers, trading spills against occupancy.  Measured on
+// the 10-view 1600x1200 schedule: the strong update runs fastest at 6 blocks (80 registers,
+// 24 warps), the sweep kernels unconstrained.
 #ifndef DPE_COST_MIN_BLOCKS
 #define DPE_COST_MIN_BLOCKS 1
 #endif
+#ifndef DPE_STRONG_MIN_BLOCKS
+#define DPE_STRONG_MIN_BLOCKS 6
+#endif
+// Taps of a window column issued as one unrolled group when the window is the reference's
+// (radius 5, step 2: 6 taps per column); 0 keeps the general loop.
+#ifndef DPE_TAP_UNROLL
+#define DPE_TAP_UNROLL 0
+#endif
+constexpr int kTapUnroll = DPE_TAP_UNROLL > 0 ? DPE_TAP_UNROLL : 1;
 
 // All per-call read-only data (cameras, relative poses, params, buffer pointers).  It lives in a
 // small device buffer written once per call; kernels receive its address.
@@ -394,12 +405,12 @@ __device__ __forceinline__ float bilateral_weight(float dx, float dy, float pix,
 // shared memory per block cuts the resident blocks and the L1 left for the image gathers.)
 constexpr int kWinTaps = kMaxWin * kMaxWin;
 struct RefWindow {
-  float w_[kWinTaps];
-  float wr_[kWinTaps];
+  float2 t_[kWinTaps];  // per tap (w, w * (r - c)): one 8-byte load per tap
   float center, inv_wsum, mean_r, var_r;
   unsigned long long *cnt;  // this kernel's strong-evaluation counter (counting runs only)
-  __device__ __forceinline__ float w(int k) const { return G(w_, k, kWinTaps, 322); }
-  __device__ __forceinline__ float wr(int k) const { return G(wr_, k, kWinTaps, 323); }
+  __device__ __forceinline__ float2 tap(int k) const { return G(t_, k, kWinTaps, 322); }
+  __device__ __forceinline__ float w(int k) const { return tap(k).x; }
+  __device__ __forceinline__ float wr(int k) const { return tap(k).y; }
 };
 #define DPE_REF_WINDOW(rw) ::dpe::RefWindow rw
 
@@ -414,8 +425,7 @@ __device__ __forceinline__ void build_ref_window(const PMArgs &a, int px, int py
       const float rp = texel(a, 0, px + i, py + j);
       const float w = bilateral_weight((float)i, (float)j, rp, center, a.P.sigma_spatial, a.P.sigma_color);
       const float rc = rp - center;
-      G(rw.w_, k, kWinTaps, 320) = w;
-      G(rw.wr_, k, kWinTaps, 321) = w * rc;
+      G(rw.t_, k, kWinTaps, 320) = make_float2(w, w * rc);
       sw += w; swr += w * rc; swrr += w * rc * rc;
       ++k;
     }
@@ -426,8 +436,19 @@ __device__ __forceinline__ void build_ref_window(const PMArgs &a, int px, int py
   rw.var_r = swrr * rw.inv_wsum - rw.mean_r * rw.mean_r;
 }
 
-// ComputeBilateralNCCOld (DPE.cu:696-782) with the reference window precomputed; the window loop
-// for one source sampler.
+// Reciprocal of a tap's projective depth.  The device uses the hardware reciprocal
+// (rcp.approx.ftz, within 1 ulp of 1/z; the perspective divide only places the bilinear sample,
+// so the difference is far inside the NCC's 1e-4 bar).  Host builds of this source (the
+// bit-exact logic check against the oracle) keep the exact quotient.
+__device__ __forceinline__ float tap_rcp(float z) {
+#if defined(__CUDA_ARCH__)
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(z));
+  return r;
+#else
+  return 1.0f / z;
+#endif
+}
 // One tap of the strong window: sample the source at the projected tap and accumulate the
 // hypothesis-dependent moments (sums of w*s, w*s^2, w*(r-c)*s over s = sample - c).
 template <class Src>
@@ -435,12 +456,13 @@ __device__ __forceinline__ void strong_tap(const PMArgs &a, const float H[9], co
                                            float bx, float by, float bz, float y, int k, float &s_s, float &s_ss,
                                            float &s_rs) {
   const float X = H[1] * y + bx, Y = H[4] * y + by, Z = H[7] * y + bz;
-  const float iz = 1.0f / Z;
+  const float iz = tap_rcp(Z);
   const float sv = bilinear_s(src, a.W, a.H, X * iz, Y * iz) - rw.center;
-  const float ws = rw.w(k) * sv;
+  const float2 t = rw.tap(k);
+  const float ws = t.x * sv;
   s_s += ws;
   s_ss += ws * sv;
-  s_rs += rw.wr(k) * sv;
+  s_rs += t.y * sv;
 }
 // ComputeBilateralNCCOld (DPE.cu:696-782) with the reference window precomputed; the window loop
 // for one source sampler.
@@ -449,12 +471,22 @@ __device__ __forceinline__ float ncc_strong_src(const PMArgs &a, int px, int py,
                                                 const RefWindow &rw) {
   const int r = a.P.strong_radius, inc = a.P.strong_increment;
   float s_s = 0.f, s_ss = 0.f, s_rs = 0.f;
-  int k = 0;
-  for (int i = -r; i <= r; i += inc) {
-    const float x = (float)(px + i);
-    // column x is fixed while y walks the window: the projective numerators are affine in y
-    const float bx = H[0] * x + H[2], by = H[3] * x + H[5], bz = H[6] * x + H[8];
-    for (int j = -r; j <= r; j += inc) strong_tap(a, H, src, rw, bx, by, bz, (float)(py + j), k++, s_s, s_ss, s_rs);
+  if (DPE_TAP_UNROLL > 0 && r == 5 && inc == 2) {
+    for (int ii = 0; ii < 6; ++ii) {
+      const float x = (float)(px - 5 + 2 * ii);
+      const float bx = H[0] * x + H[2], by = H[3] * x + H[5], bz = H[6] * x + H[8];
+#pragma unroll kTapUnroll
+      for (int jj = 0; jj < 6; ++jj)
+        strong_tap(a, H, src, rw, bx, by, bz, (float)(py - 5 + 2 * jj), 6 * ii + jj, s_s, s_ss, s_rs);
+    }
+  } else {
+    int k = 0;
+    for (int i = -r; i <= r; i += inc) {
+      const float x = (float)(px + i);
+      // column x is fixed while y walks the window: the projective numerators are affine in y
+      const float bx = H[0] * x + H[2], by = H[3] * x + H[5], bz = H[6] * x + H[8];
+      for (int j = -r; j <= r; j += inc) strong_tap(a, H, src, rw, bx, by, bz, (float)(py + j), k++, s_s, s_ss, s_rs);
+    }
   }
   const float m_s = s_s * rw.inv_wsum;
   const float var_s = s_ss * rw.inv_wsum - m_s * m_s;

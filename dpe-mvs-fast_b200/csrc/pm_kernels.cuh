@@ -679,7 +679,7 @@ __device__ __forceinline__ void gn_hypothesis(const PMArgs &a, int px, int py, c
 
 // ------------------------------------------------------------------ strong update (DPE.cu:1218-1670, 1069-1122)
 template <int kStage, bool kGN>
-__global__ void __launch_bounds__(128, DPE_COST_MIN_BLOCKS) k_strong_update(const Launch lc, int iter, int parity) {
+__global__ void __launch_bounds__(128, DPE_STRONG_MIN_BLOCKS) k_strong_update(const Launch lc, int iter, int parity) {
   const Blk B = resolve<kGridHalf>(lc);
   const PMArgs &a = *B.a;
   int px, py;

@@ -133,6 +133,8 @@ extern "C" int dpe_scene_run(dpe_ctx *ctx, const dpe_scene *sc, const dpe_schedu
   const int L = sch->num_levels > 0 ? sch->num_levels : round_num(W, H);
   if (L > 8 || (W >> (L - 1)) < 16 || (H >> (L - 1)) < 16) return DPE_ERR_INVALID_ARGUMENT;
   if (sch->refine_calls < 0 || sch->max_iterations < 0) return DPE_ERR_INVALID_ARGUMENT;
+  if (sch->batch_views != 0 && sch->batch_views != 1) return DPE_ERR_INVALID_ARGUMENT;
+  if (sch->batch_views && sc->num_views > DPE_MAX_BATCH) return DPE_ERR_INVALID_ARGUMENT;
   const bool have_edges = sc->views[0].edges != nullptr, have_labels = sc->views[0].labels != nullptr;
   for (int v = 0; v < V; ++v) {
     const dpe_scene_view &sv = sc->views[v];
@@ -172,6 +174,10 @@ extern "C" int dpe_scene_run(dpe_ctx *ctx, const dpe_scene *sc, const dpe_schedu
   float4 *out_plane = A.get<float4>("sc_out_plane", LF);
   uint8_t *out_weak = A.get<uint8_t>("sc_out_weak", LF);
   uint32_t *out_views = A.get<uint32_t>("sc_out_views", LF);
+  // per-view outputs of a batched call
+  float4 *bout_plane = sch->batch_views ? A.get<float4>("sc_bout_plane", LF * V) : nullptr;
+  uint8_t *bout_weak = sch->batch_views ? A.get<uint8_t>("sc_bout_weak", LF * V) : nullptr;
+  uint32_t *bout_views = sch->batch_views ? A.get<uint32_t>("sc_bout_views", LF * V) : nullptr;
   if (!A.ok()) return DPE_ERR_OUT_OF_MEMORY;
   for (int v = 0; v < V; ++v)
     st[v] = ViewState{img_lvl + LF * v, planes + LF * v, depths + LF * v, weaks + LF * v, views + LF * v};
@@ -259,14 +265,13 @@ extern "C" int dpe_scene_run(dpe_ctx *ctx, const dpe_scene *sc, const dpe_schedu
       }
     }
     for (int call = 0; call <= sch->refine_calls; ++call) {
-      for (int v = 0; v < V; ++v) {
+      // The problem of view v in this call (main.cpp:390-457 parameters).
+      auto make_problem = [&](int v, dpe_problem &p) {
         const dpe_scene_view &sv = sc->views[v];
-        dpe_problem p;
         std::memset(&p, 0, sizeof(p));
         p.width = w; p.height = h; p.num_images = 1 + sv.num_src;
         p.memory = DPE_MEM_DEVICE;
-        const int ids0 = v;
-        p.images[0] = st[ids0].img;
+        p.images[0] = st[v].img;
         p.cameras[0] = camera_at(sv.camera, W, H, w, h);
         for (int j = 0; j < sv.num_src; ++j) {
           const int id = sv.src_views[j];
@@ -320,18 +325,44 @@ extern "C" int dpe_scene_run(dpe_ctx *ctx, const dpe_scene *sc, const dpe_schedu
           for (int j = 0; j < sv.num_src; ++j) p.depths[1 + j] = st[sv.src_views[j]].depth;
         }
         p.seed = mix64(sch->seed ^ ((uint64_t)l << 48) ^ ((uint64_t)call << 40) ^ (uint64_t)v);
-        dpe_pm_out o;
-        std::memset(&o, 0, sizeof(o));
-        o.plane = reinterpret_cast<float *>(out_plane);
-        o.weak = out_weak;
-        o.selected_views = out_views;
-        const int rc = dpe_pm_run(ctx, &p, &o);
-        if (rc != DPE_OK) return rc;
-        k_store_result<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(out_plane, out_weak, out_views, (int)n, P.depth_min,
-                                                                   P.depth_max, st[v].plane, st[v].depth, st[v].weak,
-                                                                   st[v].views);
+      };
+      auto store = [&](int v, const dpe_problem &p, float4 *op, uint8_t *ow, uint32_t *ov) -> int {
+        k_store_result<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(op, ow, ov, (int)n, p.params.depth_min,
+                                                                   p.params.depth_max, st[v].plane, st[v].depth,
+                                                                   st[v].weak, st[v].views);
         DPE_LAUNCHED("k_store_result", s);
-        ++calls;
+        return DPE_OK;
+      };
+      if (!sch->batch_views) {
+        // the reference's order: view by view, each reading the depths its predecessors just wrote
+        for (int v = 0; v < V; ++v) {
+          dpe_problem p;
+          make_problem(v, p);
+          dpe_pm_out o;
+          std::memset(&o, 0, sizeof(o));
+          o.plane = reinterpret_cast<float *>(out_plane);
+          o.weak = out_weak;
+          o.selected_views = out_views;
+          const int rc = dpe_pm_run(ctx, &p, &o);
+          if (rc != DPE_OK) return rc;
+          store(v, p, out_plane, out_weak, out_views);
+          ++calls;
+        }
+      } else {
+        // all views of the call in one batch, each reading the previous call's depths
+        std::vector<dpe_problem> probs(V);
+        std::vector<dpe_pm_out> outs(V);
+        for (int v = 0; v < V; ++v) {
+          make_problem(v, probs[v]);
+          std::memset(&outs[v], 0, sizeof(dpe_pm_out));
+          outs[v].plane = reinterpret_cast<float *>(bout_plane + LF * v);
+          outs[v].weak = bout_weak + LF * v;
+          outs[v].selected_views = bout_views + LF * v;
+        }
+        const int rc = dpe_pm_run_batch(ctx, probs.data(), V, outs.data());
+        if (rc != DPE_OK) return rc;
+        for (int v = 0; v < V; ++v) store(v, probs[v], bout_plane + LF * v, bout_weak + LF * v, bout_views + LF * v);
+        calls += V;
       }
     }
   }

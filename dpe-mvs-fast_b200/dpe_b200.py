@@ -84,7 +84,7 @@ class SceneView(C.Structure):
 
 class Schedule(C.Structure):
     _fields_ = [("num_levels", C.c_int), ("refine_calls", C.c_int), ("max_iterations", C.c_int),
-                ("fuse_mode", C.c_int), ("min_consistent", C.c_int), ("seed", C.c_uint64)]
+                ("fuse_mode", C.c_int), ("min_consistent", C.c_int), ("seed", C.c_uint64), ("batch_views", C.c_int)]
 
 
 class KernelStat(C.Structure):
@@ -351,7 +351,7 @@ class Context:
     # ------------------------------------------------------------------ whole scene
     def scene_run(self, gray, bgr, cameras, srcs, edges=None, labels=None, *, num_levels=0, refine_calls=3,
                   max_iterations=3, fuse_mode=FUSE_FP64, min_consistent=1, seed=1, memory=MEM_HOST,
-                  want_maps=True, point_capacity=None) -> Dict:
+                  want_maps=True, point_capacity=None, batch_views=False) -> Dict:
         """The reference's full schedule over all views (dpe_scene_run).  gray[v]: (H, W) uint8,
         bgr[v]: (H, W, 3) uint8, cameras[v]: full-resolution camera dicts, srcs[v]: source view
         indices, edges[v][level] / labels[v][level]: per-level maps (level 0 = coarsest)."""
@@ -378,7 +378,7 @@ class Context:
                 sv.labels = C.cast(la, C.POINTER(C.c_void_p))
         sc = SceneIn(V, W, H, arr, memory)
         sch = Schedule(num_levels, refine_calls, max_iterations, fuse_mode if fuse_mode is not None else -1,
-                       min_consistent, seed)
+                       min_consistent, seed, 1 if batch_views else 0)
         so = SceneOut()
         so.out_memory = MEM_HOST
         res = {}

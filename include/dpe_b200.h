@@ -187,6 +187,9 @@ typedef struct dpe_schedule {
   int fuse_mode;        /* DPE_FUSE_FP64 / DPE_FUSE_FLOAT, or -1 for no fusion                   */
   int min_consistent;   /* fusion: consistent sources per point (<= 1: the reference rule)        */
   uint64_t seed;        /* base of the per-call random streams                                    */
+  int batch_views;      /* 0: views one after another within a call, each reading the depths its
+                           predecessors wrote (the reference's order); 1: all views of a call in one
+                           dpe_pm_run_batch, each reading the previous call's depths            */
 } dpe_schedule;
 
 typedef struct dpe_scene {
