@@ -16,6 +16,10 @@ CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libdpe_sm100.so")
 LIB_CHECKED = os.path.join(HERE, "libdpe_sm100_checked.so")
+# The exact build: no multiply-add contraction and IEEE division in every kernel, so the device
+# computes the CPU oracle's arithmetic bit for bit (the default build contracts, and differs from
+# the oracle by rounding only).
+EXACT_FLAGS = ("-fmad=false", "-DDPE_EXACT")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2"]
 # per-source extra flags: fusion rounds like its CPU restatement (no FMA contraction)
@@ -72,8 +76,18 @@ def build(force: bool = False, verbose: bool = False, checked: bool = False, var
     return lib
 
 
+def build_all(force: bool = False, verbose: bool = False) -> list:
+    """The default library and the exact build (libdpe_sm100_exact.so)."""
+    return [build(force=force, verbose=verbose), build(force=force, verbose=verbose, variant="exact", defines=EXACT_FLAGS)]
+
+
 if __name__ == "__main__":
     args = sys.argv[1:]
-    name = args[args.index("--variant") + 1] if "--variant" in args else ""
-    defs = tuple(a for a in args if a.startswith("-D"))
-    print(build(force="--force" in args, verbose=True, checked="--checked" in args, variant=name, defines=defs))
+    if "--variant" in args:
+        name = args[args.index("--variant") + 1]
+        flags = tuple(a for a in args if a.startswith("-D") or a.startswith("-f"))
+        print(build(force="--force" in args, verbose=True, variant=name, defines=flags))
+    elif "--checked" in args:
+        print(build(force="--force" in args, verbose=True, checked=True))
+    else:
+        print("\n".join(build_all(force="--force" in args, verbose=True)))

@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/dpe_b200.h"
+#include "dpe_math.h"
 #include "kernel_ids.h"
 
 namespace dpe {
@@ -30,12 +31,14 @@ constexpr int kMaxWin = 6;  // taps per window side for radius 5 / step 2 (DPE.c
 #ifndef DPE_STRONG_MIN_BLOCKS
 #define DPE_STRONG_MIN_BLOCKS 6
 #endif
-// Taps of a window column issued as one unrolled group when the window is the reference's
-// (radius 5, step 2: 6 taps per column); 0 keeps the general loop.
-#ifndef DPE_TAP_UNROLL
-#define DPE_TAP_UNROLL 0
+// Unrolling of a window column's taps (the reference window, radius 5 / step 2, has 6 per column)
+// in the kernels that sweep one plane family over all sources: measured, unrolling by 3 speeds
+// DepthToWeak, LocalRefine and the random initialisation by 8-15 %, and slows the strong update,
+// whose registers are bounded for occupancy, by 25 %.
+#ifndef DPE_SWEEP_UNROLL
+#define DPE_SWEEP_UNROLL 3
 #endif
-constexpr int kTapUnroll = DPE_TAP_UNROLL > 0 ? DPE_TAP_UNROLL : 1;
+constexpr int kSweepUnroll = DPE_SWEEP_UNROLL;
 
 // All per-call read-only data (cameras, relative poses, params, buffer pointers).  It lives in a
 // small device buffer written once per call; kernels receive its address.
@@ -74,6 +77,8 @@ struct PMArgs {
   short2 *lab_bound;
   short2 *edge_neigh;
   short2 *nearest;
+  int *wall;        // the pixels WEAK at the start of the call (k_list_weak), raster order
+  int *wall_count;  // [1] their number
   unsigned long long *counters;  // per kernel class: [2k] strong NCC evals, [2k+1] weak (counting runs)
   // Weak-texture pass.  The WEAK pixels of each colour are listed once per call (wlist, wcount,
   // raster order); a listed pixel's position in its list is its slot in the scratch below, which
@@ -244,10 +249,12 @@ struct SrcBF16 {
                        __uint_as_float(b & 0xFFFF0000u));
   }
 };
-template <class Src>
+// kClamp = false: the caller knows -1 <= x <= W-1 and -1 <= y <= H-1, where the clamp is the
+// identity.
+template <class Src, bool kClamp = true>
 __device__ __forceinline__ float bilinear_s(const Src &src, int W, int H, float x, float y) {
-  const float xc = fminf(fmaxf(x, -1.0f), (float)(W - 1));
-  const float yc = fminf(fmaxf(y, -1.0f), (float)(H - 1));
+  const float xc = kClamp ? fminf(fmaxf(x, -1.0f), (float)(W - 1)) : x;
+  const float yc = kClamp ? fminf(fmaxf(y, -1.0f), (float)(H - 1)) : y;
   const float fx = floorf(xc), fy = floorf(yc);
   const float ax = xc - fx, ay = yc - fy;
   const float4 v = src.fetch(((int)fy + 1) * src.pw + ((int)fx + 1));
@@ -342,9 +349,9 @@ __device__ __forceinline__ float4 perturbed_normal(const dpe_camera &c, int x, i
   const float a2 = (rng.uniform() - 0.5f) * pert;
   const float a3 = (rng.uniform() - 0.5f) * pert;
   float s1, s2, s3, c1, c2, c3;
-  sincosf(a1, &s1, &c1);
-  sincosf(a2, &s2, &c2);
-  sincosf(a3, &s3, &c3);
+  dpe_sincos_small(a1, &s1, &c1);  // |a| <= 0.01 pi
+  dpe_sincos_small(a2, &s2, &c2);
+  dpe_sincos_small(a3, &s3, &c3);
   const float R0 = c2 * c3, R1 = c3 * s1 * s2 - c1 * s3, R2 = s1 * s3 + c1 * c3 * s2;
   const float R3 = c2 * s3, R4 = c1 * c3 + s1 * s2 * s3, R5 = c1 * s2 * s3 - c3 * s1;
   const float R6 = -s2, R7 = c2 * s1, R8 = c1 * c2;
@@ -390,7 +397,7 @@ __device__ __forceinline__ float2 project(const float H[9], int x, int y) {
 __device__ __forceinline__ float bilateral_weight(float dx, float dy, float pix, float center, float ss, float sc) {
   const float spatial = sqrtf(dx * dx + dy * dy);
   const float color = fabsf(pix - center);
-  return expf(-spatial / (2.0f * ss * ss) - color / (2.0f * sc * sc));
+  return dpe_expf(-spatial / (2.0f * ss * ss) - color / (2.0f * sc * sc));
 }
 
 // ------------------------------------------------------------------ strong NCC
@@ -436,12 +443,12 @@ __device__ __forceinline__ void build_ref_window(const PMArgs &a, int px, int py
   rw.var_r = swrr * rw.inv_wsum - rw.mean_r * rw.mean_r;
 }
 
-// Reciprocal of a tap's projective depth.  The device uses the hardware reciprocal
+// Reciprocal of a tap's projective depth.  The fast device build uses the hardware reciprocal
 // (rcp.approx.ftz, within 1 ulp of 1/z; the perspective divide only places the bilinear sample,
-// so the difference is far inside the NCC's 1e-4 bar).  Host builds of this source (the
-// bit-exact logic check against the oracle) keep the exact quotient.
+// so the difference is far inside the NCC's 1e-4 bar).  The exact build (DPE_EXACT) and host
+// builds of this source keep the IEEE quotient.
 __device__ __forceinline__ float tap_rcp(float z) {
-#if defined(__CUDA_ARCH__)
+#if defined(__CUDA_ARCH__) && !defined(DPE_EXACT)
   float r;
   asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(z));
   return r;
@@ -451,13 +458,13 @@ __device__ __forceinline__ float tap_rcp(float z) {
 }
 // One tap of the strong window: sample the source at the projected tap and accumulate the
 // hypothesis-dependent moments (sums of w*s, w*s^2, w*(r-c)*s over s = sample - c).
-template <class Src>
+template <bool kClamp, class Src>
 __device__ __forceinline__ void strong_tap(const PMArgs &a, const float H[9], const Src &src, const RefWindow &rw,
                                            float bx, float by, float bz, float y, int k, float &s_s, float &s_ss,
                                            float &s_rs) {
   const float X = H[1] * y + bx, Y = H[4] * y + by, Z = H[7] * y + bz;
   const float iz = tap_rcp(Z);
-  const float sv = bilinear_s(src, a.W, a.H, X * iz, Y * iz) - rw.center;
+  const float sv = bilinear_s<Src, kClamp>(src, a.W, a.H, X * iz, Y * iz) - rw.center;
   const float2 t = rw.tap(k);
   const float ws = t.x * sv;
   s_s += ws;
@@ -466,18 +473,32 @@ __device__ __forceinline__ void strong_tap(const PMArgs &a, const float H[9], co
 }
 // ComputeBilateralNCCOld (DPE.cu:696-782) with the reference window precomputed; the window loop
 // for one source sampler.
-template <class Src>
-__device__ __forceinline__ float ncc_strong_src(const PMArgs &a, int px, int py, const float H[9], const Src &src,
-                                                const RefWindow &rw) {
+// The window's taps lie in the rectangle [px - r, px + r] x [py - r, py + r]; when its four
+// corners project with a positive depth to at least 0.01 pixel inside the clamp range, every tap
+// does (the projective map is affine in the depth and sends the rectangle to the convex hull of
+// the corner images), and the taps skip the clamp, which would be the identity.
+__device__ __forceinline__ bool window_inside(const PMArgs &a, const float H[9], int px, int py, int r) {
+  const float lo = -1.0f + 0.01f, hx = (float)(a.W - 1) - 0.01f, hy = (float)(a.H - 1) - 0.01f;
+  bool in = true;
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    const float x = (float)(px + ((c & 1) ? r : -r)), y = (float)(py + ((c & 2) ? r : -r));
+    const float X = H[0] * x + H[1] * y + H[2], Y = H[3] * x + H[4] * y + H[5], Z = H[6] * x + H[7] * y + H[8];
+    in = in && Z > 0.0f && X >= lo * Z && X <= hx * Z && Y >= lo * Z && Y <= hy * Z;
+  }
+  return in;
+}
+template <bool kClamp, class Src, int kUnroll>
+__device__ __forceinline__ void strong_window(const PMArgs &a, int px, int py, const float H[9], const Src &src,
+                                              const RefWindow &rw, float &s_s, float &s_ss, float &s_rs) {
   const int r = a.P.strong_radius, inc = a.P.strong_increment;
-  float s_s = 0.f, s_ss = 0.f, s_rs = 0.f;
-  if (DPE_TAP_UNROLL > 0 && r == 5 && inc == 2) {
+  if (kUnroll > 0 && r == 5 && inc == 2) {
     for (int ii = 0; ii < 6; ++ii) {
       const float x = (float)(px - 5 + 2 * ii);
       const float bx = H[0] * x + H[2], by = H[3] * x + H[5], bz = H[6] * x + H[8];
-#pragma unroll kTapUnroll
+#pragma unroll(kUnroll > 0 ? kUnroll : 1)
       for (int jj = 0; jj < 6; ++jj)
-        strong_tap(a, H, src, rw, bx, by, bz, (float)(py - 5 + 2 * jj), 6 * ii + jj, s_s, s_ss, s_rs);
+        strong_tap<kClamp>(a, H, src, rw, bx, by, bz, (float)(py - 5 + 2 * jj), 6 * ii + jj, s_s, s_ss, s_rs);
     }
   } else {
     int k = 0;
@@ -485,16 +506,26 @@ __device__ __forceinline__ float ncc_strong_src(const PMArgs &a, int px, int py,
       const float x = (float)(px + i);
       // column x is fixed while y walks the window: the projective numerators are affine in y
       const float bx = H[0] * x + H[2], by = H[3] * x + H[5], bz = H[6] * x + H[8];
-      for (int j = -r; j <= r; j += inc) strong_tap(a, H, src, rw, bx, by, bz, (float)(py + j), k++, s_s, s_ss, s_rs);
+      for (int j = -r; j <= r; j += inc)
+        strong_tap<kClamp>(a, H, src, rw, bx, by, bz, (float)(py + j), k++, s_s, s_ss, s_rs);
     }
   }
+}
+template <class Src, int kUnroll>
+__device__ __forceinline__ float ncc_strong_src(const PMArgs &a, int px, int py, const float H[9], const Src &src,
+                                                const RefWindow &rw) {
+  float s_s = 0.f, s_ss = 0.f, s_rs = 0.f;
+  if (window_inside(a, H, px, py, a.P.strong_radius))
+    strong_window<false, Src, kUnroll>(a, px, py, H, src, rw, s_s, s_ss, s_rs);
+  else
+    strong_window<true, Src, kUnroll>(a, px, py, H, src, rw, s_s, s_ss, s_rs);
   const float m_s = s_s * rw.inv_wsum;
   const float var_s = s_ss * rw.inv_wsum - m_s * m_s;
   if (rw.var_r < 1e-5f || var_s < 1e-5f) return 2.0f;
   const float cov = s_rs * rw.inv_wsum - rw.mean_r * m_s;
   return fmaxf(0.0f, fminf(2.0f, 1.0f - cov / sqrtf(rw.var_r * var_s)));
 }
-template <int kStage = DPE_STAGE_FP32>
+template <int kStage = DPE_STAGE_FP32, int kUnroll = 0>
 __device__ __forceinline__ float ncc_strong(const PMArgs &a, int px, int py, int s, float4 pl, const RefWindow &rw) {
   float H[9];
   homography(a, s, pl, H);
@@ -502,7 +533,7 @@ __device__ __forceinline__ float ncc_strong(const PMArgs &a, int px, int py, int
   const dpe_camera &sc = a.cam[s];
   if (pt.x >= sc.width || pt.x < 0.0f || pt.y >= sc.height || pt.y < 0.0f) return 2.0f;
   if (rw.cnt) atomicAdd(rw.cnt, 1ull);
-  return ncc_strong_src(a, px, py, H, SrcOf<kStage>::make(a, s), rw);
+  return ncc_strong_src<decltype(SrcOf<kStage>::make(a, s)), kUnroll>(a, px, py, H, SrcOf<kStage>::make(a, s), rw);
 }
 
 // ------------------------------------------------------------------ strong NCC adjoint
@@ -622,10 +653,10 @@ __device__ __forceinline__ float ncc_strong_adjoint(const PMArgs &a, int px, int
 }
 
 // Strong costs of plane pl against every source: out[j] = cost against source j + 1.
-template <int kStage>
+template <int kStage, int kUnroll = 0>
 __device__ __forceinline__ void ncc_all_sources(const PMArgs &a, int px, int py, float4 pl, const RefWindow &rw,
                                                 float *out) {
-  for (int j = 0; j < a.N - 1; ++j) out[j] = ncc_strong<kStage>(a, px, py, j + 1, pl, rw);
+  for (int j = 0; j < a.N - 1; ++j) out[j] = ncc_strong<kStage, kUnroll>(a, px, py, j + 1, pl, rw);
 }
 // Sum over the listed sources act[0..na) (ascending) of vw[j] * cost(j), in list order.
 template <int kStage>

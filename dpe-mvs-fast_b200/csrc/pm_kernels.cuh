@@ -169,11 +169,7 @@ __global__ void k_gen_edge_inform(const Launch lc) {
 }
 
 // ------------------------------------------------------------------ FindNearestStrongPoint (DPE.cu:2859-2893)
-__global__ void k_find_nearest_strong(const Launch lc) {
-  const Blk B = resolve<kGridFull>(lc);
-  const PMArgs &a = *B.a;
-  int px, py;
-  if (!full_pixel(a, B, &px, &py)) return;
+__device__ __forceinline__ void find_nearest_strong_pixel(const PMArgs &a, int px, int py) {
   const int W = a.W, H = a.H, center = px + py * W;
   short2 res = make_short2(-1, -1);
   if (a.weak[center] == DPE_WEAK) {
@@ -193,6 +189,31 @@ __global__ void k_find_nearest_strong(const Launch lc) {
     }
   }
   a.nearest[center] = res;
+}
+// The pixels WEAK at the start of the call, in raster order, from the prefix map nmap: the work
+// list of the kernels that serve WEAK pixels only (nearest strong point, neighbour search, plane
+// fit).  The state map does not gain WEAK pixels later in the call.
+__global__ void k_list_weak(const Launch lc) {
+  const Blk B = resolve<kGridFull>(lc);
+  const PMArgs &a = *B.a;
+  int px, py;
+  if (!full_pixel(a, B, &px, &py)) return;
+  const int c = px + py * a.W;
+  const bool w = a.weak[c] == DPE_WEAK;
+  if (w) a.wall[a.nmap[c]] = c;
+  if (c == a.W * a.H - 1) *a.wall_count = a.nmap[c] + (w ? 1 : 0);
+}
+
+// Over the pixels WEAK at the start of the call; every other entry of `nearest` is (-1, -1) from
+// the fill before the launch.
+__global__ void __launch_bounds__(128) k_find_nearest_strong(const Launch lc) {
+  const Blk B = resolve<kGridList>(lc);
+  const PMArgs &a = *B.a;
+  const int count = *a.wall_count;
+  for (int slot = B.x * blockDim.x + threadIdx.x; slot < count; slot += B.gx * blockDim.x) {
+    const int c = a.wall[slot];
+    find_nearest_strong_pixel(a, c % a.W, c / a.W);
+  }
 }
 
 // ------------------------------------------------------------------ geometry helpers for GenNeighbours
@@ -257,11 +278,7 @@ __device__ __forceinline__ void sort_small(float *d, int n) {
 }
 
 // ------------------------------------------------------------------ GenNeighbours (DPE.cu:2107-2467)
-__global__ void __launch_bounds__(128) k_gen_neighbours(const Launch lc) {
-  const Blk B = resolve<kGridFull>(lc);
-  const PMArgs &a = *B.a;
-  int px, py;
-  if (!full_pixel(a, B, &px, &py)) return;
+__device__ __forceinline__ void gen_neighbours_pixel(const PMArgs &a, int px, int py) {
   const int W = a.W, H = a.H, center = px + py * W;
   if (a.weak[center] != DPE_WEAK) return;
   constexpr int kMaxPts = 64;
@@ -494,6 +511,16 @@ __global__ void __launch_bounds__(128) k_gen_neighbours(const Launch lc) {
   for (int i = 1; i < kNeighbours; ++i) nbs[i] = (i - 1 < vc) ? sv[i - 1] : make_short2(-1, -1);
   a.reliable[center] = 1;
 }
+// Over the pixels WEAK at the start of the call.
+__global__ void __launch_bounds__(128) k_gen_neighbours(const Launch lc) {
+  const Blk B = resolve<kGridList>(lc);
+  const PMArgs &a = *B.a;
+  const int count = *a.wall_count;
+  for (int slot = B.x * blockDim.x + threadIdx.x; slot < count; slot += B.gx * blockDim.x) {
+    const int c = a.wall[slot];
+    gen_neighbours_pixel(a, c % a.W, c / a.W);
+  }
+}
 
 __global__ void k_neighbour_update(const Launch lc) {
   const Blk B = resolve<kGridFull>(lc);
@@ -525,7 +552,7 @@ __global__ void __launch_bounds__(128, DPE_COST_MIN_BLOCKS) k_random_init(const 
     a.plane[center] = pl;
     float cv[kMaxSrc], srt[kMaxSrc];
     int valid = 0;
-    ncc_all_sources<kStage>(a, px, py, pl, rw, cv);
+    ncc_all_sources<kStage, kSweepUnroll>(a, px, py, pl, rw, cv);
     for (int i = 0; i < n; ++i) {
       const float v = cv[i];
       srt[i] = v;
@@ -555,7 +582,7 @@ __global__ void __launch_bounds__(128, DPE_COST_MIN_BLOCKS) k_random_init(const 
     float cost = 0.0f;
     for (int i = 1; i < a.N; ++i) {
       if (isSet(views, i - 1)) {
-        const float v = ncc_strong<kStage>(a, px, py, i, pl, rw);
+        const float v = ncc_strong<kStage, kSweepUnroll>(a, px, py, i, pl, rw);
         if (v < 2.0f) { cnt++; cost += v; }
         else unSetBit(&views, i - 1);
       }
@@ -572,15 +599,15 @@ __device__ __forceinline__ float sample_views(const PMArgs &a, Rng &rng, int ite
                                               const float *priors, uint8_t *vw, uint32_t *temp_sel, float *probs) {
   const int n = a.N - 1;
   for (int i = 0; i < 32; ++i) vw[i] = 0;
-  const float thr = (float)(0.8 * (double)expf((float)(iter * iter) / (-90.0f)));
-  const float base = expf(thr * thr / (-0.32f));
+  const float thr = (float)(0.8 * (double)dpe_expf((float)(iter * iter) / (-90.0f)));
+  const float base = dpe_expf(thr * thr / (-0.32f));
   for (int i = 0; i < n; ++i) {
     float count = 0;
     int count_false = 0;
     float tmpw = 0;
     for (int j = 0; j < 8; ++j) {
       const float v = cost_array[j * stride + i];
-      if (v < thr) { tmpw += expf(v * v / (-0.18f)); count++; }
+      if (v < thr) { tmpw += dpe_expf(v * v / (-0.18f)); count++; }
       if (v > 1.2f) count_false++;
     }
     float p = 0.0f;
@@ -739,7 +766,7 @@ __global__ void __launch_bounds__(128, DPE_STRONG_MIN_BLOCKS) k_strong_update(co
       }
     }
     if (!on_edge) {
-      const float good_thr = 0.8f * expf((float)(iter * iter) / (-90.0f));
+      const float good_thr = 0.8f * dpe_expf((float)(iter * iter) / (-90.0f));
       for (int d = 0; d < 8; ++d) {
         const int dx = kDir[d][0], dy = kDir[d][1];
         const int sx = cvmax(1, 5 - 2 * iter) * dx, sy = cvmax(1, 5 - 2 * iter) * dy;
@@ -930,11 +957,7 @@ __global__ void __launch_bounds__(128, DPE_STRONG_MIN_BLOCKS) k_strong_update(co
 }
 
 // ------------------------------------------------------------------ RANSACToGetFitPlane (DPE.cu:2895-3128)
-__global__ void __launch_bounds__(128) k_ransac_fit_plane(const Launch lc) {
-  const Blk B = resolve<kGridFull>(lc);
-  const PMArgs &a = *B.a;
-  int px, py;
-  if (!full_pixel(a, B, &px, &py)) return;
+__device__ __forceinline__ void ransac_fit_plane_pixel(const PMArgs &a, int px, int py) {
   const int W = a.W, center = px + py * W;
   if (a.weak[center] != DPE_WEAK) { a.fit_plane[center] = a.plane[center]; return; }
   Rng rng = make_rng(a, center);
@@ -1067,6 +1090,16 @@ __global__ void __launch_bounds__(128) k_ransac_fit_plane(const Launch lc) {
   } else {
     a.fit_plane[center] = make_float4(0, 0, 0, 0);
     if (a.P.use_radius) a.radius[center] = a.P.strong_radius;
+  }
+}
+// Over the pixels WEAK at the start of the call; the fitted plane is read for WEAK pixels only.
+__global__ void __launch_bounds__(128) k_ransac_fit_plane(const Launch lc) {
+  const Blk B = resolve<kGridList>(lc);
+  const PMArgs &a = *B.a;
+  const int count = *a.wall_count;
+  for (int slot = B.x * blockDim.x + threadIdx.x; slot < count; slot += B.gx * blockDim.x) {
+    const int c = a.wall[slot];
+    ransac_fit_plane_pixel(a, c % a.W, c / a.W);
   }
 }
 
@@ -1390,7 +1423,7 @@ __device__ __forceinline__ void sweep_setup(const PMArgs &a, int px, int py, con
     if (!isSet(s.views, vi)) continue;
     float4 t = s.pl;
     t.w = dist_to_origin(a.cam[0], px, py, s.depth, t);
-    float tc = ncc_strong<kStage>(a, px, py, si, t, rw);
+    float tc = ncc_strong<kStage, kSweepUnroll>(a, px, py, si, t, rw);
     if (a.P.geom_consistency) tc += a.P.geom_factor * geom_cost(a, px, py, si, t);
     const int w = vweight_at(s.vw, vi);
     s.cost_now += tc * w;
@@ -1433,7 +1466,7 @@ __global__ void __launch_bounds__(128, DPE_COST_MIN_BLOCKS) k_depth_to_weak(cons
     t.w = dist_to_origin(rc, px, py, pdep, t);
     float cost = 0.0f;
     for (int q = 0; q < na; ++q) {
-      float tc = ncc_strong<kStage>(a, px, py, act[q] + 1, t, rw);
+      float tc = ncc_strong<kStage, kSweepUnroll>(a, px, py, act[q] + 1, t, rw);
       if (a.P.geom_consistency) tc += a.P.geom_factor * geom_cost(a, px, py, act[q] + 1, t);
       cost += tc * vweight_at(s.vw, act[q]);
     }
@@ -1494,7 +1527,7 @@ __global__ void __launch_bounds__(128, DPE_COST_MIN_BLOCKS) k_local_refine(const
     for (int q = 0; q < na; ++q) {
       const int vi = act[q];
       const int w = vweight_at(s.vw, vi);
-      tc += ncc_strong<kStage>(a, px, py, vi + 1, t, rw) * w;
+      tc += ncc_strong<kStage, kSweepUnroll>(a, px, py, vi + 1, t, rw) * w;
       if (a.P.geom_consistency) tc += a.P.geom_factor * geom_cost(a, px, py, vi + 1, t) * w;
     }
     tc /= s.weight_normal;

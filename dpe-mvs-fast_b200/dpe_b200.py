@@ -15,6 +15,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 # DPE_LIBRARY selects another in-tree build (e.g. the bounds-checked libdpe_sm100_checked.so)
 LIB_PATH = os.path.join(HERE, os.environ.get("DPE_LIBRARY", "libdpe_sm100.so"))
+# the same kernels built without multiply-add contraction: the CPU oracle's arithmetic, bit for bit
+EXACT_LIBRARY = "libdpe_sm100_exact.so"
 
 MAX_IMAGES = 32
 NEIGHBOUR_NUM = 9
@@ -222,8 +224,9 @@ def build_problem(images: Sequence, cameras: Sequence[Dict], params: Params, *, 
 class Context:
     """A dpe_ctx on one device."""
 
-    def __init__(self, device: int = 0):
-        self.lib = load_library()
+    def __init__(self, device: int = 0, library: Optional[str] = None):
+        """library: another in-tree build by file name (e.g. EXACT_LIBRARY), default the main one."""
+        self.lib = load_library(os.path.join(HERE, library)) if library else load_library()
         h = C.c_void_p()
         st = self.lib.dpe_ctx_create(device, None, C.byref(h))
         if st != OK:

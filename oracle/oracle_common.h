@@ -9,6 +9,7 @@
 #ifndef DPE_ORACLE_COMMON_H_
 #define DPE_ORACLE_COMMON_H_
 
+#include "../dpe-mvs-fast_b200/csrc/dpe_math.h"  // exp / sin / cos with the kernels' bits
 #include <cmath>
 #include <cstdint>
 #include <cstring>

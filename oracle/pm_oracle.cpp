@@ -180,8 +180,10 @@ static f4 perturbed_normal(const dpe_camera &c, int x, int y, const f4 &n, Pixel
   const float a1 = (rng.uniform() - 0.5f) * pert;
   const float a2 = (rng.uniform() - 0.5f) * pert;
   const float a3 = (rng.uniform() - 0.5f) * pert;
-  const float s1 = std::sin(a1), s2 = std::sin(a2), s3 = std::sin(a3);
-  const float c1 = std::cos(a1), c2 = std::cos(a2), c3 = std::cos(a3);
+  float s1, s2, s3, c1, c2, c3;
+  dpe::dpe_sincos_small(a1, &s1, &c1);
+  dpe::dpe_sincos_small(a2, &s2, &c2);
+  dpe::dpe_sincos_small(a3, &s3, &c3);
   const float R[9] = {c2 * c3, c3 * s1 * s2 - c1 * s3, s1 * s3 + c1 * c3 * s2,
                       c2 * s3, c1 * c3 + s1 * s2 * s3, c1 * s2 * s3 - c3 * s1,
                       -s2,     c2 * s1,                c1 * c2};
@@ -257,7 +259,7 @@ struct Ctx {
 static inline float bilateral_weight(float dx, float dy, float pix, float center, float ss, float sc) {
   const float spatial = std::sqrt(dx * dx + dy * dy);
   const float color = std::fabs(pix - center);
-  return std::exp(-spatial / (2.0f * ss * ss) - color / (2.0f * sc * sc));
+  return dpe::dpe_expf(-spatial / (2.0f * ss * ss) - color / (2.0f * sc * sc));
 }
 
 // Moment form of the window NCC.  The reference accumulates raw moments (E[x^2] - E[x]^2,
@@ -497,18 +499,18 @@ static float sample_views(Ctx &c, int center, int iter, const float cost_array[8
   const int n = c.P.num_images - 1;
   for (int i = 0; i < DPE_MAX_IMAGES; ++i) vw[i] = 0;
   float probs[32] = {0.0f};
-  const float thr = (float)(0.8 * (double)std::exp((float)(iter * iter) / (-90.0f)));
+  const float thr = (float)(0.8 * (double)dpe::dpe_expf((float)(iter * iter) / (-90.0f)));
   for (int i = 0; i < n; ++i) {
     float count = 0;
     int count_false = 0;
     float tmpw = 0;
     for (int j = 0; j < 8; ++j) {
       const float v = cost_array[j][i];
-      if (v < thr) { tmpw += std::exp(v * v / (-0.18f)); count++; }
+      if (v < thr) { tmpw += dpe::dpe_expf(v * v / (-0.18f)); count++; }
       if (v > 1.2f) count_false++;
     }
     if (count > 2 && count_false < 3) probs[i] = tmpw / count;
-    else if (count_false < 3) probs[i] = std::exp(thr * thr / (-0.32f));
+    else if (count_false < 3) probs[i] = dpe::dpe_expf(thr * thr / (-0.32f));
     probs[i] = probs[i] * priors[i];
   }
   // TransformPDFToCDF, DPE.cu:297-311
@@ -615,7 +617,7 @@ static void strong_update(Ctx &c, int px, int py, int iter) {
       }
     }
     if (!c.edge[center]) {
-      const float good_thr = 0.8f * std::exp((float)(iter * iter) / (-90.0f));
+      const float good_thr = 0.8f * dpe::dpe_expf((float)(iter * iter) / (-90.0f));
       const float bad_thr = 1.2f;
       for (int d = 0; d < 8; ++d) {
         const int dx = kDir[d][0], dy = kDir[d][1];

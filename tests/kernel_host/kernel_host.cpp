@@ -110,8 +110,14 @@ extern "C" int host_pm_run(const dpe_problem *p, dpe_pm_out *out) {
   int acc = 0;
   for (size_t i = 0; i < L; ++i) { a.nmap[i] = acc; acc += weak_flag[i]; }
   launch(fg, fb, k_gen_edge_inform, one);
-  launch(fg, fb, k_find_nearest_strong, one);
-  launch(fg, fb, k_gen_neighbours, one);
+  std::vector<int> wall(L), wall_count(1);
+  a.wall = wall.data();
+  a.wall_count = wall_count.data();
+  launch(fg, fb, k_list_weak, one);
+  for (size_t i = 0; i < L; ++i) a.nearest[i] = make_short2(-1, -1);
+  const dim3 lg(7), lb(32);  // strided work lists: any grid covers them
+  launch(lg, lb, k_find_nearest_strong, one);
+  launch(lg, lb, k_gen_neighbours, one);
   launch(fg, fb, k_neighbour_update, one);
   // WEAK pixels per colour in raster order (the cub select of dpe_pm_run)
   const size_t wcap = (L + 1) / 2;
@@ -140,10 +146,9 @@ extern "C" int host_pm_run(const dpe_problem *p, dpe_pm_out *out) {
       if (a.P.use_edge) { memcpy(a.plane_snap, a.plane, L * 16); memcpy(a.cost_snap, a.cost, L * 4); }
       launch(hg, hb, k_strong_update<DPE_STAGE_FP32, false>, one, it, parity);
     }
-    launch(fg, fb, k_ransac_fit_plane, one);
+    launch(lg, lb, k_ransac_fit_plane, one);
     if (a.P.use_APD)
       for (int parity = 0; parity < 2; ++parity) {
-        const dim3 lg(7), lb(32);  // strided work lists: any grid covers them
         launch(lg, lb, k_weak_prepare, one, parity);
         launch(lg, lb, k_weak_eval<false, DPE_STAGE_FP32>, one, parity);
         launch(lg, lb, k_weak_decide, one, it, parity);
