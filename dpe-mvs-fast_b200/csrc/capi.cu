@@ -303,8 +303,6 @@ int setup_problem(dpe_ctx *ctx, const dpe_problem *p, int index, ProblemState *p
   a.lab_bound = get((short2 *)0, "lab_bound", L * 8);
   a.edge_neigh = get((short2 *)0, "edge_neigh", L * 8);
   a.nearest = get((short2 *)0, "nearest", L);
-  a.wall = get((int *)0, "weak_all", L);
-  a.wall_count = get((int *)0, "weak_all_count", 1);
   const size_t wcap = ps->wcap;
   if (a.P.use_APD) {
     const int n = N - 1;
@@ -443,14 +441,11 @@ int run_sequence(dpe_ctx *ctx, ProblemState *ps, int n, const PMArgs *d_args, co
       DPE_TRY(cudaMemsetAsync(a.nmap, 0, (size_t)L * 4, s));
     }
   }
-  DPE_TIMED(ctx, KID_LIST_WEAK, s, k_list_weak<<<g.fg, g.fb, 0, s>>>(g.full));
-  PM_LAUNCHED("k_list_weak", s);
   DPE_TIMED(ctx, KID_GEN_EDGE_INFORM, s, k_gen_edge_inform<<<g.fg, g.fb, 0, s>>>(g.full));
   PM_LAUNCHED("k_gen_edge_inform", s);
-  for (int b = 0; b < n; ++b) DPE_TRY(cudaMemsetAsync(ps[b].a.nearest, 0xFF, ps[b].L * sizeof(short2), s));
-  DPE_TIMED(ctx, KID_FIND_NEAREST, s, k_find_nearest_strong<<<g.gp, 128, 0, s>>>(g.prep));
+  DPE_TIMED(ctx, KID_FIND_NEAREST, s, k_find_nearest_strong<<<g.fg, g.fb, 0, s>>>(g.full));
   PM_LAUNCHED("k_find_nearest_strong", s);
-  DPE_TIMED(ctx, KID_GEN_NEIGHBOURS, s, k_gen_neighbours<<<g.gp, 128, 0, s>>>(g.prep));
+  DPE_TIMED(ctx, KID_GEN_NEIGHBOURS, s, k_gen_neighbours<<<g.fg, g.fb, 0, s>>>(g.full));
   PM_LAUNCHED("k_gen_neighbours", s);
   DPE_TIMED(ctx, KID_NEIGHBOUR_UPDATE, s, k_neighbour_update<<<g.fg, g.fb, 0, s>>>(g.full));
   PM_LAUNCHED("k_neighbour_update", s);
@@ -483,7 +478,7 @@ int run_sequence(dpe_ctx *ctx, ProblemState *ps, int n, const PMArgs *d_args, co
       DPE_TIMED(ctx, KID_STRONG_UPDATE, s, launch_strong_update(staging, gn, g.hg, s, g.half, it, parity));
       PM_LAUNCHED("k_strong_update", s);
     }
-    DPE_TIMED(ctx, KID_RANSAC, s, k_ransac_fit_plane<<<g.gp, 128, 0, s>>>(g.prep));
+    DPE_TIMED(ctx, KID_RANSAC, s, k_ransac_fit_plane<<<g.fg, g.fb, 0, s>>>(g.full));
     PM_LAUNCHED("k_ransac_fit_plane", s);
     if (P.use_APD)
       for (int parity = 0; parity < 2; ++parity) {

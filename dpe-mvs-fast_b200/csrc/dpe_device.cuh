@@ -77,8 +77,6 @@ struct PMArgs {
   short2 *lab_bound;
   short2 *edge_neigh;
   short2 *nearest;
-  int *wall;        // the pixels WEAK at the start of the call (k_list_weak), raster order
-  int *wall_count;  // [1] their number
   unsigned long long *counters;  // per kernel class: [2k] strong NCC evals, [2k+1] weak (counting runs)
   // Weak-texture pass.  The WEAK pixels of each colour are listed once per call (wlist, wcount,
   // raster order); a listed pixel's position in its list is its slot in the scratch below, which
@@ -473,21 +471,6 @@ __device__ __forceinline__ void strong_tap(const PMArgs &a, const float H[9], co
 }
 // ComputeBilateralNCCOld (DPE.cu:696-782) with the reference window precomputed; the window loop
 // for one source sampler.
-// The window's taps lie in the rectangle [px - r, px + r] x [py - r, py + r]; when its four
-// corners project with a positive depth to at least 0.01 pixel inside the clamp range, every tap
-// does (the projective map is affine in the depth and sends the rectangle to the convex hull of
-// the corner images), and the taps skip the clamp, which would be the identity.
-__device__ __forceinline__ bool window_inside(const PMArgs &a, const float H[9], int px, int py, int r) {
-  const float lo = -1.0f + 0.01f, hx = (float)(a.W - 1) - 0.01f, hy = (float)(a.H - 1) - 0.01f;
-  bool in = true;
-#pragma unroll
-  for (int c = 0; c < 4; ++c) {
-    const float x = (float)(px + ((c & 1) ? r : -r)), y = (float)(py + ((c & 2) ? r : -r));
-    const float X = H[0] * x + H[1] * y + H[2], Y = H[3] * x + H[4] * y + H[5], Z = H[6] * x + H[7] * y + H[8];
-    in = in && Z > 0.0f && X >= lo * Z && X <= hx * Z && Y >= lo * Z && Y <= hy * Z;
-  }
-  return in;
-}
 template <bool kClamp, class Src, int kUnroll>
 __device__ __forceinline__ void strong_window(const PMArgs &a, int px, int py, const float H[9], const Src &src,
                                               const RefWindow &rw, float &s_s, float &s_ss, float &s_rs) {
@@ -515,10 +498,9 @@ template <class Src, int kUnroll>
 __device__ __forceinline__ float ncc_strong_src(const PMArgs &a, int px, int py, const float H[9], const Src &src,
                                                 const RefWindow &rw) {
   float s_s = 0.f, s_ss = 0.f, s_rs = 0.f;
-  if (window_inside(a, H, px, py, a.P.strong_radius))
-    strong_window<false, Src, kUnroll>(a, px, py, H, src, rw, s_s, s_ss, s_rs);
-  else
-    strong_window<true, Src, kUnroll>(a, px, py, H, src, rw, s_s, s_ss, s_rs);
+  // (a clamp-free copy of the loop for windows that project inside the source measured slower:
+  // the second copy costs registers under the strong update's occupancy bound)
+  strong_window<true, Src, kUnroll>(a, px, py, H, src, rw, s_s, s_ss, s_rs);
   const float m_s = s_s * rw.inv_wsum;
   const float var_s = s_ss * rw.inv_wsum - m_s * m_s;
   if (rw.var_r < 1e-5f || var_s < 1e-5f) return 2.0f;

@@ -4,7 +4,6 @@
 enum KernelId {
   KID_INIT_STATE = 0,
   KID_GEN_EDGE_INFORM,
-  KID_LIST_WEAK,
   KID_FIND_NEAREST,
   KID_GEN_NEIGHBOURS,
   KID_NEIGHBOUR_UPDATE,
@@ -29,7 +28,7 @@ enum KernelId {
 };
 
 static const char *const kKernelNames[KID_COUNT] = {
-    "k_init_state",    "k_gen_edge_inform", "k_list_weak", "k_find_nearest_strong", "k_gen_neighbours", "k_neighbour_update",
+    "k_init_state",    "k_gen_edge_inform", "k_find_nearest_strong", "k_gen_neighbours", "k_neighbour_update",
     "k_random_init",   "k_strong_update",   "k_ransac_fit_plane",    "k_weak_prepare",   "k_weak_eval",
     "k_weak_decide",   "k_weak_finish",     "k_get_depth_normal",
     "k_filter_strong", "k_depth_to_weak",   "k_local_refine",        "k_pad_image",      "k_ncc_queries",

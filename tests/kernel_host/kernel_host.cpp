@@ -44,6 +44,11 @@ static inline unsigned long long atomicAdd(unsigned long long *p, unsigned long 
   *p += v;
   return o;
 }
+static inline unsigned int __float_as_uint(float f) {
+  unsigned int u;
+  std::memcpy(&u, &f, 4);
+  return u;
+}
 static inline float __uint_as_float(unsigned int u) {
   float f;
   std::memcpy(&f, &u, 4);
@@ -110,14 +115,9 @@ extern "C" int host_pm_run(const dpe_problem *p, dpe_pm_out *out) {
   int acc = 0;
   for (size_t i = 0; i < L; ++i) { a.nmap[i] = acc; acc += weak_flag[i]; }
   launch(fg, fb, k_gen_edge_inform, one);
-  std::vector<int> wall(L), wall_count(1);
-  a.wall = wall.data();
-  a.wall_count = wall_count.data();
-  launch(fg, fb, k_list_weak, one);
-  for (size_t i = 0; i < L; ++i) a.nearest[i] = make_short2(-1, -1);
+  launch(fg, fb, k_find_nearest_strong, one);
+  launch(fg, fb, k_gen_neighbours, one);
   const dim3 lg(7), lb(32);  // strided work lists: any grid covers them
-  launch(lg, lb, k_find_nearest_strong, one);
-  launch(lg, lb, k_gen_neighbours, one);
   launch(fg, fb, k_neighbour_update, one);
   // WEAK pixels per colour in raster order (the cub select of dpe_pm_run)
   const size_t wcap = (L + 1) / 2;
@@ -146,7 +146,7 @@ extern "C" int host_pm_run(const dpe_problem *p, dpe_pm_out *out) {
       if (a.P.use_edge) { memcpy(a.plane_snap, a.plane, L * 16); memcpy(a.cost_snap, a.cost, L * 4); }
       launch(hg, hb, k_strong_update<DPE_STAGE_FP32, false>, one, it, parity);
     }
-    launch(lg, lb, k_ransac_fit_plane, one);
+    launch(fg, fb, k_ransac_fit_plane, one);
     if (a.P.use_APD)
       for (int parity = 0; parity < 2; ++parity) {
         launch(lg, lb, k_weak_prepare, one, parity);
