@@ -624,45 +624,6 @@ __device__ __forceinline__ int find_min_cost_index(const float *c, int n) {
   return idx;
 }
 
-// ------------------------------------------------------------------ candidate cost reuse
-// Propagation copies planes unchanged, so a pixel's neighbours often carry planes with the same
-// bits, and a neighbour's plane is often the pixel's own.  The same plane gives the same costs, so
-// a plane already evaluated for this pixel (a row of its candidate cost array) is looked up
-// instead of evaluated again.  The values and the order of every sum are those of evaluating.
-__device__ __forceinline__ bool same_plane(float4 p, float4 q) {
-  return __float_as_uint(p.x) == __float_as_uint(q.x) && __float_as_uint(p.y) == __float_as_uint(q.y) &&
-         __float_as_uint(p.z) == __float_as_uint(q.z) && __float_as_uint(p.w) == __float_as_uint(q.w);
-}
-__device__ __forceinline__ int find_row(float4 cp, const float4 *row_plane, const bool *row_set) {
-  for (int d = 0; d < 8; ++d)
-    if (row_set[d] && same_plane(row_plane[d], cp)) return d;
-  return -1;
-}
-// Costs of plane cp against every source into out.
-template <int kStage>
-__device__ __forceinline__ void candidate_costs(const PMArgs &a, int px, int py, float4 cp, const RefWindow &rw,
-                                                const float4 *row_plane, const bool *row_set,
-                                                const float (*rows)[kMaxSrc], float *out) {
-  const int d = find_row(cp, row_plane, row_set);
-  if (d < 0) {
-    ncc_all_sources<kStage>(a, px, py, cp, rw, out);
-    return;
-  }
-  for (int j = 0; j < a.N - 1; ++j) out[j] = rows[d][j];
-}
-// weighted_ncc of plane pl, from a row when one holds its costs.
-template <int kStage>
-__device__ __forceinline__ float candidate_weighted(const PMArgs &a, int px, int py, float4 pl, const RefWindow &rw,
-                                                    const int *act, int na, const uint8_t *vw,
-                                                    const float4 *row_plane, const bool *row_set,
-                                                    const float (*rows)[kMaxSrc]) {
-  const int d = find_row(pl, row_plane, row_set);
-  if (d < 0) return weighted_ncc<kStage>(a, px, py, pl, rw, act, na, vw);
-  float tc = 0.0f;
-  for (int q = 0; q < na; ++q) tc += vw[act[q]] * rows[d][act[q]];
-  return tc;
-}
-
 // ------------------------------------------------------------------ Gauss-Newton plane hypothesis
 // The differentiation form's refinement step (no reference counterpart; dpe_options::gn_refine).
 // Around the current plane (n, depth) it takes the cost of each sampled source j and its gradient
@@ -746,9 +707,6 @@ __global__ void __launch_bounds__(128, DPE_STRONG_MIN_BLOCKS) k_strong_update(co
   cost_array[0][0] = 2.0f;  // `= {2.0f}` initialises only the first element (quirk Q2)
   bool flag[8] = {false, false, false, false, false, false, false, false};
   int positions[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  // the plane whose costs row d of cost_array holds, once evaluated (candidate_costs reuses rows)
-  float4 row_plane[8];
-  bool row_set[8] = {false, false, false, false, false, false, false, false};
   const float4 *cand_plane = a.P.use_edge ? a.plane_snap : a.plane;
   const float *cand_cost = a.P.use_edge ? a.cost_snap : a.cost;
 
@@ -787,9 +745,7 @@ __global__ void __launch_bounds__(128, DPE_STRONG_MIN_BLOCKS) k_strong_update(co
         flag[d] = true;
         positions[d] = mp;
         const float4 cp = G(cand_plane, mp, L, 205);
-        candidate_costs<kStage>(a, px, py, cp, rw, row_plane, row_set, cost_array, cost_array[d]);
-        row_plane[d] = cp;
-        row_set[d] = true;
+        ncc_all_sources<kStage>(a, px, py, cp, rw, cost_array[d]);
       }
     }
     if (!on_edge) {
@@ -813,7 +769,7 @@ __global__ void __launch_bounds__(128, DPE_STRONG_MIN_BLOCKS) k_strong_update(co
           flag[d] = true;
           float tca[kMaxSrc];
           const float4 cp = G(cand_plane, mp, L, 205);
-          candidate_costs<kStage>(a, px, py, cp, rw, row_plane, row_set, cost_array, tca);
+          ncc_all_sources<kStage>(a, px, py, cp, rw, tca);
           int g0 = 0, g1 = 0, b0 = 0, b1 = 0;
           for (int j = 0; j < n; ++j) {
             if (cost_array[d][j] < good_thr) g0++;
@@ -824,8 +780,6 @@ __global__ void __launch_bounds__(128, DPE_STRONG_MIN_BLOCKS) k_strong_update(co
           if (!had || g1 > g0 || (g1 == g0 && b1 < b0)) {
             positions[d] = mp;
             for (int j = 0; j < n; ++j) cost_array[d][j] = tca[j];
-            row_plane[d] = cp;
-            row_set[d] = true;
           }
         }
       }
@@ -887,9 +841,7 @@ __global__ void __launch_bounds__(128, DPE_STRONG_MIN_BLOCKS) k_strong_update(co
     for (int d = 0; d < 8; ++d) {
       if (!flag[d]) continue;
       const float4 cp = G(a.plane, positions[d], L, 210);
-      candidate_costs<kStage>(a, px, py, cp, rw, row_plane, row_set, cost_array, cost_array[d]);
-      row_plane[d] = cp;
-      row_set[d] = true;
+      ncc_all_sources<kStage>(a, px, py, cp, rw, cost_array[d]);
     }
   }
 #ifdef DPE_CHECKED
@@ -941,7 +893,7 @@ __global__ void __launch_bounds__(128, DPE_STRONG_MIN_BLOCKS) k_strong_update(co
   int na = 0;
   for (int i = 0; i < n; ++i)
     if (vw[i] > 0) act[na++] = i;
-  float cost_now = candidate_weighted<kStage>(a, px, py, pl_cur, rw, act, na, vw, row_plane, row_set, cost_array);
+  float cost_now = weighted_ncc<kStage>(a, px, py, pl_cur, rw, act, na, vw);
   cost_now /= wn;
   const float cost_written = cost_now;
   float depth_now = depth_from_plane(rc, pl_cur, px, py);
@@ -968,7 +920,7 @@ __global__ void __launch_bounds__(128, DPE_STRONG_MIN_BLOCKS) k_strong_update(co
     for (int h = 0; h < 5; ++h) {
       float4 t = normals[h];
       t.w = dist_to_origin(rc, px, py, depths[h], t);
-      float tc = candidate_weighted<kStage>(a, px, py, t, rw, act, na, vw, row_plane, row_set, cost_array);
+      float tc = weighted_ncc<kStage>(a, px, py, t, rw, act, na, vw);
       tc /= wn;
       const float db = depth_from_plane(rc, t, px, py);
       if (db >= dmin && db <= dmax && tc < cost_now) { depth_now = db; pl_now = t; cost_now = tc; }
