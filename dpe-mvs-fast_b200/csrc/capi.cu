@@ -303,12 +303,6 @@ int setup_problem(dpe_ctx *ctx, const dpe_problem *p, int index, ProblemState *p
   a.lab_bound = get((short2 *)0, "lab_bound", L * 8);
   a.edge_neigh = get((short2 *)0, "edge_neigh", L * 8);
   a.nearest = get((short2 *)0, "nearest", L);
-  a.sw_tab = get((float2 *)0, "sweep_tab", L * kWinTaps);
-  a.sw_win = get((float4 *)0, "sweep_win", L);
-  a.sw_pl = get((float4 *)0, "sweep_pl", L);
-  a.sw_par = get((float4 *)0, "sweep_par", L);
-  a.sw_valid = get((int *)0, "sweep_valid", L);
-  a.sw_cost = get((float *)0, "sweep_cost", L * 61);
   const size_t wcap = ps->wcap;
   if (a.P.use_APD) {
     const int n = N - 1;
@@ -413,9 +407,9 @@ int setup_problem(dpe_ctx *ctx, const dpe_problem *p, int index, ProblemState *p
 // Grids of one kernel sequence: for one problem the 2D pixel grids; for a batch one 1D grid per
 // kind over all problems, with the prefix tables the kernels resolve their problem from.
 struct SequenceGrids {
-  Launch full, half, prep, eval, sweep;
+  Launch full, half, prep, eval;
   dim3 fg, hg;
-  unsigned gp = 0, ge = 0, gs = 0;
+  unsigned gp = 0, ge = 0;
   const dim3 fb = kFullBlock, hb = kHalfBlock;
 };
 
@@ -506,16 +500,10 @@ int run_sequence(dpe_ctx *ctx, ProblemState *ps, int n, const PMArgs *d_args, co
     DPE_TIMED(ctx, KID_FILTER, s, k_filter_strong<<<g.hg, g.hb, 0, s>>>(g.half, parity));
     PM_LAUNCHED("k_filter_strong", s);
   }
-  DPE_TIMED(ctx, KID_DEPTH_TO_WEAK, s, with_stage(staging, [&](auto st) { k_sweep_prepare<decltype(st)::value><<<g.fg, g.fb, 0, s>>>(g.full); }));
-  PM_LAUNCHED("k_sweep_prepare", s);
-  DPE_TIMED(ctx, KID_DEPTH_TO_WEAK, s, with_stage(staging, [&](auto st) { k_sweep_eval<decltype(st)::value, kSweepClassify><<<g.gs, 128, 0, s>>>(g.sweep); }));
-  PM_LAUNCHED("k_sweep_eval", s);
-  DPE_TIMED(ctx, KID_DEPTH_TO_WEAK, s, k_sweep_classify<<<g.fg, g.fb, 0, s>>>(g.full));
-  PM_LAUNCHED("k_sweep_classify", s);
-  DPE_TIMED(ctx, KID_LOCAL_REFINE, s, with_stage(staging, [&](auto st) { k_sweep_eval<decltype(st)::value, kSweepRefine><<<g.gs, 128, 0, s>>>(g.sweep); }));
-  PM_LAUNCHED("k_sweep_eval", s);
-  DPE_TIMED(ctx, KID_LOCAL_REFINE, s, k_sweep_refine<<<g.fg, g.fb, 0, s>>>(g.full));
-  PM_LAUNCHED("k_sweep_refine", s);
+  DPE_TIMED(ctx, KID_DEPTH_TO_WEAK, s, with_stage(staging, [&](auto st) { k_depth_to_weak<decltype(st)::value><<<g.fg, g.fb, 0, s>>>(g.full); }));
+  PM_LAUNCHED("k_depth_to_weak", s);
+  DPE_TIMED(ctx, KID_LOCAL_REFINE, s, with_stage(staging, [&](auto st) { k_local_refine<decltype(st)::value><<<g.fg, g.fb, 0, s>>>(g.full); }));
+  PM_LAUNCHED("k_local_refine", s);
   return DPE_OK;
 }
 
@@ -539,7 +527,7 @@ int pm_run_problems(dpe_ctx *ctx, const dpe_problem *const *problems, int n, dpe
   std::vector<ProblemState> ps(n);
   unsigned long long *counters = A.get<unsigned long long>("counters", 2 * KID_COUNT);
   PMArgs *d_args = A.get<PMArgs>("pm_args", n);
-  int *d_start = n > 1 ? A.get<int>("batch_start", 5 * (n + 1)) : nullptr;
+  int *d_start = n > 1 ? A.get<int>("batch_start", 4 * (n + 1)) : nullptr;
   if (!counters || !d_args || (n > 1 && !d_start)) return DPE_ERR_OUT_OF_MEMORY;
   if (ctx->count_evals) DPE_TRY(cudaMemsetAsync(counters, 0, 16 * KID_COUNT, s));
   for (int b = 0; b < n; ++b) {
@@ -573,15 +561,14 @@ int pm_run_problems(dpe_ctx *ctx, const dpe_problem *const *problems, int n, dpe
   if (n == 1) {
     const PMArgs &a = ps[0].a;
     const Launch one{d_args, nullptr, 1};
-    g.full = g.half = g.prep = g.eval = g.sweep = one;
+    g.full = g.half = g.prep = g.eval = one;
     g.fg = full_grid(a.W, a.H);
     g.hg = half_grid(a.W, a.H);
     g.gp = list_grid(ctx, (long long)ps[0].wcap);
     g.ge = list_grid(ctx, (long long)ps[0].wcap * 10 * (a.N - 1));
-    g.gs = list_grid(ctx, (long long)ps[0].L * 61);
   } else {
     // the problems' grids laid end to end: prefix tables per grid kind
-    std::vector<int> start(5 * (n + 1), 0);
+    std::vector<int> start(4 * (n + 1), 0);
     for (int b = 0; b < n; ++b) {
       const PMArgs &a = ps[b].a;
       const dim3 f = full_grid(a.W, a.H), h = half_grid(a.W, a.H);
@@ -590,19 +577,16 @@ int pm_run_problems(dpe_ctx *ctx, const dpe_problem *const *problems, int n, dpe
       start[2 * (n + 1) + b + 1] = start[2 * (n + 1) + b] + (int)list_grid(ctx, (long long)ps[b].wcap);
       start[3 * (n + 1) + b + 1] =
           start[3 * (n + 1) + b] + (int)list_grid(ctx, (long long)ps[b].wcap * 10 * (a.N - 1));
-      start[4 * (n + 1) + b + 1] = start[4 * (n + 1) + b] + (int)list_grid(ctx, (long long)ps[b].L * 61);
     }
     DPE_TRY(cudaMemcpyAsync(d_start, start.data(), start.size() * sizeof(int), cudaMemcpyHostToDevice, s));
     g.full = Launch{d_args, d_start + 0 * (n + 1), n};
     g.half = Launch{d_args, d_start + 1 * (n + 1), n};
     g.prep = Launch{d_args, d_start + 2 * (n + 1), n};
     g.eval = Launch{d_args, d_start + 3 * (n + 1), n};
-    g.sweep = Launch{d_args, d_start + 4 * (n + 1), n};
     g.fg = dim3(start[0 * (n + 1) + n]);
     g.hg = dim3(start[1 * (n + 1) + n]);
     g.gp = (unsigned)start[2 * (n + 1) + n];
     g.ge = (unsigned)start[3 * (n + 1) + n];
-    g.gs = (unsigned)start[4 * (n + 1) + n];
     // blocks keep the single-problem shapes (16x8 full, 32x4 half): only the block index is 1D
   }
   DPE_TRY(cudaEventRecord(ctx->ev0, s));
@@ -840,10 +824,8 @@ extern "C" int dpe_kernel_info(char *buf, int len) {
   add("k_weak_decide", (const void *)k_weak_decide);
   add("k_weak_finish", (const void *)k_weak_finish<DPE_STAGE_FP32>);
   add("k_filter_strong", (const void *)k_filter_strong);
-  add("k_sweep_prepare", (const void *)k_sweep_prepare<DPE_STAGE_FP32>);
-  add("k_sweep_eval", (const void *)k_sweep_eval<DPE_STAGE_FP32, kSweepClassify>);
-  add("k_sweep_classify", (const void *)k_sweep_classify);
-  add("k_sweep_refine", (const void *)k_sweep_refine);
+  add("k_depth_to_weak", (const void *)k_depth_to_weak<DPE_STAGE_FP32>);
+  add("k_local_refine", (const void *)k_local_refine<DPE_STAGE_FP32>);
   size_t stack = 0;
   cudaDeviceGetLimit(&stack, cudaLimitStackSize);
   char line[96];

@@ -31,9 +31,6 @@ constexpr int kMaxWin = 6;  // taps per window side for radius 5 / step 2 (DPE.c
 #ifndef DPE_STRONG_MIN_BLOCKS
 #define DPE_STRONG_MIN_BLOCKS 6
 #endif
-#ifndef DPE_SWEEP_MIN_BLOCKS
-#define DPE_SWEEP_MIN_BLOCKS 1
-#endif
 // Unrolling of a window column's taps (the reference window, radius 5 / step 2, has 6 per column)
 // in the kernels that sweep one plane family over all sources: measured, unrolling by 3 speeds
 // DepthToWeak, LocalRefine and the random initialisation by 8-15 %, and slows the strong update,
@@ -96,14 +93,6 @@ struct PMArgs {
   float *wcost_r;     // [slot][5][N-1] deformable NCC of the random hypotheses
   float *wgeom_r;     // [slot][5][N-1] geometric cost of the random hypotheses
   float4 *wstate;     // [slot][2] plane after the candidate and fit-plane steps; (depth, cost, cost0, wn)
-  // DepthToWeak / LocalRefine sweeps (per pixel): the reference window and the sweep parameters,
-  // and the costs of the samples (61, then 11 reusing the same rows).
-  float2 *sw_tab;   // [pixel][36]
-  float4 *sw_win;   // [pixel] (centre value, 1 / weight sum, reference mean, reference variance)
-  float4 *sw_pl;    // [pixel] plane in reference-camera coordinates
-  float4 *sw_par;   // [pixel] (depth, current cost sum, baseline sum, weight sum)
-  int *sw_valid;    // [pixel] selected sources with a baseline
-  float *sw_cost;   // [pixel][61]
 };
 
 // Relative pose of source s with respect to the reference, computed once per call on the host
@@ -430,15 +419,6 @@ struct RefWindow {
 };
 #define DPE_REF_WINDOW(rw) ::dpe::RefWindow rw
 
-// The same window read from a per-pixel table in global memory (the sweep kernels tabulate it once
-// per pixel; the lanes of a warp that share a pixel read one tap with one broadcast load).
-struct TabWindow {
-  const float2 *t_;
-  float center, inv_wsum, mean_r, var_r;
-  unsigned long long *cnt;
-  __device__ __forceinline__ float2 tap(int k) const { return t_[k]; }
-};
-
 __device__ __forceinline__ void build_ref_window(const PMArgs &a, int px, int py, RefWindow &rw, int kid) {
   rw.cnt = a.counters ? a.counters + 2 * kid : nullptr;
   const int r = a.P.strong_radius, inc = a.P.strong_increment;
@@ -476,8 +456,8 @@ __device__ __forceinline__ float tap_rcp(float z) {
 }
 // One tap of the strong window: sample the source at the projected tap and accumulate the
 // hypothesis-dependent moments (sums of w*s, w*s^2, w*(r-c)*s over s = sample - c).
-template <bool kClamp, class Src, class Win>
-__device__ __forceinline__ void strong_tap(const PMArgs &a, const float H[9], const Src &src, const Win &rw,
+template <bool kClamp, class Src>
+__device__ __forceinline__ void strong_tap(const PMArgs &a, const float H[9], const Src &src, const RefWindow &rw,
                                            float bx, float by, float bz, float y, int k, float &s_s, float &s_ss,
                                            float &s_rs) {
   const float X = H[1] * y + bx, Y = H[4] * y + by, Z = H[7] * y + bz;
@@ -491,9 +471,9 @@ __device__ __forceinline__ void strong_tap(const PMArgs &a, const float H[9], co
 }
 // ComputeBilateralNCCOld (DPE.cu:696-782) with the reference window precomputed; the window loop
 // for one source sampler.
-template <bool kClamp, class Src, int kUnroll, class Win>
+template <bool kClamp, class Src, int kUnroll>
 __device__ __forceinline__ void strong_window(const PMArgs &a, int px, int py, const float H[9], const Src &src,
-                                              const Win &rw, float &s_s, float &s_ss, float &s_rs) {
+                                              const RefWindow &rw, float &s_s, float &s_ss, float &s_rs) {
   const int r = a.P.strong_radius, inc = a.P.strong_increment;
   if (kUnroll > 0 && r == 5 && inc == 2) {
     for (int ii = 0; ii < 6; ++ii) {
@@ -514,28 +494,28 @@ __device__ __forceinline__ void strong_window(const PMArgs &a, int px, int py, c
     }
   }
 }
-template <class Src, int kUnroll, class Win>
+template <class Src, int kUnroll>
 __device__ __forceinline__ float ncc_strong_src(const PMArgs &a, int px, int py, const float H[9], const Src &src,
-                                                const Win &rw) {
+                                                const RefWindow &rw) {
   float s_s = 0.f, s_ss = 0.f, s_rs = 0.f;
   // (a clamp-free copy of the loop for windows that project inside the source measured slower:
   // the second copy costs registers under the strong update's occupancy bound)
-  strong_window<true, Src, kUnroll, Win>(a, px, py, H, src, rw, s_s, s_ss, s_rs);
+  strong_window<true, Src, kUnroll>(a, px, py, H, src, rw, s_s, s_ss, s_rs);
   const float m_s = s_s * rw.inv_wsum;
   const float var_s = s_ss * rw.inv_wsum - m_s * m_s;
   if (rw.var_r < 1e-5f || var_s < 1e-5f) return 2.0f;
   const float cov = s_rs * rw.inv_wsum - rw.mean_r * m_s;
   return fmaxf(0.0f, fminf(2.0f, 1.0f - cov / sqrtf(rw.var_r * var_s)));
 }
-template <int kStage = DPE_STAGE_FP32, int kUnroll = 0, class Win = RefWindow>
-__device__ __forceinline__ float ncc_strong(const PMArgs &a, int px, int py, int s, float4 pl, const Win &rw) {
+template <int kStage = DPE_STAGE_FP32, int kUnroll = 0>
+__device__ __forceinline__ float ncc_strong(const PMArgs &a, int px, int py, int s, float4 pl, const RefWindow &rw) {
   float H[9];
   homography(a, s, pl, H);
   const float2 pt = project(H, px, py);
   const dpe_camera &sc = a.cam[s];
   if (pt.x >= sc.width || pt.x < 0.0f || pt.y >= sc.height || pt.y < 0.0f) return 2.0f;
   if (rw.cnt) atomicAdd(rw.cnt, 1ull);
-  return ncc_strong_src<decltype(SrcOf<kStage>::make(a, s)), kUnroll, Win>(a, px, py, H, SrcOf<kStage>::make(a, s), rw);
+  return ncc_strong_src<decltype(SrcOf<kStage>::make(a, s)), kUnroll>(a, px, py, H, SrcOf<kStage>::make(a, s), rw);
 }
 
 // ------------------------------------------------------------------ strong NCC adjoint

@@ -1417,104 +1417,44 @@ __device__ __forceinline__ void sweep_setup(const PMArgs &a, int px, int py, con
   }
 }
 
-// ------------------------------------------------------------------ DepthToWeak, LocalRefine (DPE.cu:2597-2839)
-// Both sweep the pixel's plane over depths evenly spaced in disparity (61 samples to classify the
-// pixel, 11 to refine its depth) and weigh each sample's strong costs over the selected sources.
-// The per-pixel sweep is split so that the cost evaluations run as small, high-occupancy work
-// items:
-//   k_sweep_prepare  per pixel: the reference window (tabulated) and the sweep parameters of
-//                    sweep_setup (plane, depth, baseline sum, weight sum, current cost);
-//   k_sweep_eval<NS> per (pixel, depth sample): the sample's weighted cost over the selected
-//                    sources, summed in source order as the per-pixel loop sums it;
-//   k_sweep_classify DepthToWeak's peak analysis of the 61 costs (pixel state);
-//   k_sweep_refine   LocalRefine's choice among its 11 costs (plane depth).
-// LocalRefine reads the plane and views DepthToWeak leaves unchanged, so one preparation serves
-// both sweeps.
-constexpr int kSweepClassify = 61, kSweepRefine = 11;
-
+// DepthToWeak (DPE.cu:2597-2751)
 template <int kStage>
-__global__ void __launch_bounds__(128) k_sweep_prepare(const Launch lc) {
-  const Blk B = resolve<kGridFull>(lc);
-  const PMArgs &a = *B.a;
-  int px, py;
-  if (!full_pixel(a, B, &px, &py)) return;
-  const int center = px + py * a.W;
-  DPE_REF_WINDOW(rw);
-  build_ref_window(a, px, py, rw, KID_DEPTH_TO_WEAK);
-  Sweep s;
-  sweep_setup<kStage>(a, px, py, rw, s);
-  float2 *tab = a.sw_tab + (size_t)center * kWinTaps;
-  for (int k = 0; k < kWinTaps; ++k) tab[k] = rw.t_[k];
-  a.sw_win[center] = make_float4(rw.center, rw.inv_wsum, rw.mean_r, rw.var_r);
-  a.sw_pl[center] = s.pl;
-  a.sw_par[center] = make_float4(s.depth, s.cost_now, s.base_line, s.weight_normal);
-  a.sw_valid[center] = s.valid;
-}
-
-// kNS = 61: DepthToWeak's samples (cost min(2, sum / weights), out-of-range depth 2);
-// kNS = 11: LocalRefine's (cost sum / weights, out-of-range depth +inf: never chosen).
-template <int kStage, int kNS>
-__global__ void __launch_bounds__(128, DPE_SWEEP_MIN_BLOCKS) k_sweep_eval(const Launch lc) {
-  const Blk B = resolve<kGridList>(lc);
-  const PMArgs &a = *B.a;
-  const int W = a.W, H = a.H, margin = 6;
-  const bool classify = kNS == kSweepClassify;
-  const int R = (kNS - 1) / 2;
-  const long long total = (long long)W * H * kNS;
-  const dpe_camera &rc = a.cam[0];
-  const bool geom = a.P.geom_consistency != 0;
-  const float gf = a.P.geom_factor;
-  for (long long t = (long long)B.x * blockDim.x + threadIdx.x; t < total; t += (long long)B.gx * blockDim.x) {
-    const int center = (int)(t / kNS), sample = (int)(t - (long long)center * kNS);
-    const int px = center % W, py = center / W;
-    const float4 par = a.sw_par[center];
-    const int valid = a.sw_valid[center];
-    if (classify && (px < margin || py < margin || px >= W - margin || py >= H - margin)) continue;
-    if (par.x == 0 || valid == 0 || (!classify && par.w == 0)) continue;
-    const float base_line = par.z / valid;
-    const float disp = rc.K[0] * base_line / par.x;
-    const float pdep = rc.K[0] * base_line / (disp + (sample - R));
-    float out;
-    if (pdep < a.P.depth_min || pdep > a.P.depth_max) {
-      out = classify ? 2.0f : __uint_as_float(0x7f800000u);
-    } else {
-      const float4 win = a.sw_win[center];
-      const TabWindow tw{a.sw_tab + (size_t)center * kWinTaps, win.x, win.y, win.z, win.w,
-                         a.counters ? a.counters + 2 * (classify ? KID_DEPTH_TO_WEAK : KID_LOCAL_REFINE) : nullptr};
-      float4 pl = a.sw_pl[center];
-      pl.w = dist_to_origin(rc, px, py, pdep, pl);
-      const uint32_t views = a.views[center];
-      const uint4 vw = a.vweight[center];
-      float cost = 0.0f;
-      for (int vi = 0; vi < a.N - 1; ++vi) {
-        if (!isSet(views, vi)) continue;
-        const int w = vweight_at(vw, vi);
-        if (classify) {
-          float tc = ncc_strong<kStage, kSweepUnroll>(a, px, py, vi + 1, pl, tw);
-          if (geom) tc += gf * geom_cost(a, px, py, vi + 1, pl);
-          cost += tc * w;
-        } else {
-          cost += ncc_strong<kStage, kSweepUnroll>(a, px, py, vi + 1, pl, tw) * w;
-          if (geom) cost += gf * geom_cost(a, px, py, vi + 1, pl) * w;
-        }
-      }
-      cost /= par.w;
-      out = classify ? cvmin(2.0f, cost) : cost;
-    }
-    a.sw_cost[(size_t)center * kSweepClassify + sample] = out;
-  }
-}
-
-__global__ void k_sweep_classify(const Launch lc) {
+__global__ void __launch_bounds__(128, DPE_COST_MIN_BLOCKS) k_depth_to_weak(const Launch lc) {
   const Blk B = resolve<kGridFull>(lc);
   const PMArgs &a = *B.a;
   int px, py;
   if (!full_pixel(a, B, &px, &py)) return;
   const int W = a.W, H = a.H, center = px + py * W, margin = 6;
   if (px < margin || py < margin || px >= W - margin || py >= H - margin) { a.weak[center] = DPE_UNKNOWN; return; }
-  if (a.sw_par[center].x == 0 || a.sw_valid[center] == 0) { a.weak[center] = DPE_UNKNOWN; return; }
-  constexpr int R = 30, NS = kSweepClassify;
-  const float *pc = a.sw_cost + (size_t)center * kSweepClassify;
+  const dpe_camera &rc = a.cam[0];
+  DPE_REF_WINDOW(rw);
+  build_ref_window(a, px, py, rw, KID_DEPTH_TO_WEAK);
+  Sweep s;
+  sweep_setup<kStage>(a, px, py, rw, s);
+  if (s.depth == 0 || s.valid == 0) { a.weak[center] = DPE_UNKNOWN; return; }
+  s.cost_now /= s.weight_normal;
+  s.base_line /= s.valid;
+  const float disp = rc.K[0] * s.base_line / s.depth;
+  int act[kMaxSrc];  // selected sources, ascending
+  int na = 0;
+  for (int vi = 0; vi < a.N - 1; ++vi)
+    if (isSet(s.views, vi)) act[na++] = vi;
+  constexpr int R = 30, NS = 61;
+  float pc[NS];
+  for (int pd = -R; pd <= R; ++pd) {
+    const float pdep = rc.K[0] * s.base_line / (disp + pd);
+    if (pdep < a.P.depth_min || pdep > a.P.depth_max) { pc[pd + R] = 2.0f; continue; }
+    float4 t = s.pl;
+    t.w = dist_to_origin(rc, px, py, pdep, t);
+    float cost = 0.0f;
+    for (int q = 0; q < na; ++q) {
+      float tc = ncc_strong<kStage, kSweepUnroll>(a, px, py, act[q] + 1, t, rw);
+      if (a.P.geom_consistency) tc += a.P.geom_factor * geom_cost(a, px, py, act[q] + 1, t);
+      cost += tc * vweight_at(s.vw, act[q]);
+    }
+    cost /= s.weight_normal;
+    pc[pd + R] = cvmin(2.0f, cost);
+  }
   int peaks = 0, min_peak = 0;
   float min_cost = 2.0f;
   uint64_t peak_mask = 0;
@@ -1537,28 +1477,45 @@ __global__ void k_sweep_classify(const Launch lc) {
   a.weak[center] = res;
 }
 
-__global__ void k_sweep_refine(const Launch lc) {
+// LocalRefine (DPE.cu:2753-2839)
+template <int kStage>
+__global__ void __launch_bounds__(128, DPE_COST_MIN_BLOCKS) k_local_refine(const Launch lc) {
   const Blk B = resolve<kGridFull>(lc);
   const PMArgs &a = *B.a;
   int px, py;
   if (!full_pixel(a, B, &px, &py)) return;
   const int center = px + py * a.W;
-  const float4 par = a.sw_par[center];
-  const int valid = a.sw_valid[center];
-  if (par.x == 0) return;
-  if (par.w == 0 || valid == 0) return;
   const dpe_camera &rc = a.cam[0];
-  const float cost_now = par.y / par.w;
-  const float base_line = par.z / valid;
-  const float disp = rc.K[0] * base_line / par.x;
-  const float *tc = a.sw_cost + (size_t)center * kSweepClassify;
-  float min_cost = 2.0f, best = par.x;
+  DPE_REF_WINDOW(rw);
+  build_ref_window(a, px, py, rw, KID_LOCAL_REFINE);
+  Sweep s;
+  sweep_setup<kStage>(a, px, py, rw, s);
+  if (s.depth == 0) return;
+  if (s.weight_normal == 0 || s.valid == 0) return;
+  s.cost_now /= s.weight_normal;
+  s.base_line /= s.valid;
+  const float disp = rc.K[0] * s.base_line / s.depth;
+  int act[kMaxSrc];  // selected sources, ascending
+  int na = 0;
+  for (int vi = 0; vi < a.N - 1; ++vi)
+    if (isSet(s.views, vi)) act[na++] = vi;
+  float min_cost = 2.0f, best = s.depth;
   for (int pd = -5; pd <= 5; ++pd) {
-    const float pdep = rc.K[0] * base_line / (disp + pd);
+    const float pdep = rc.K[0] * s.base_line / (disp + pd);
     if (pdep < a.P.depth_min || pdep > a.P.depth_max) continue;
-    if (tc[pd + 5] < min_cost) { min_cost = tc[pd + 5]; best = pdep; }
+    float4 t = s.pl;
+    t.w = dist_to_origin(rc, px, py, pdep, t);
+    float tc = 0.0f;
+    for (int q = 0; q < na; ++q) {
+      const int vi = act[q];
+      const int w = vweight_at(s.vw, vi);
+      tc += ncc_strong<kStage, kSweepUnroll>(a, px, py, vi + 1, t, rw) * w;
+      if (a.P.geom_consistency) tc += a.P.geom_factor * geom_cost(a, px, py, vi + 1, t) * w;
+    }
+    tc /= s.weight_normal;
+    if (tc < min_cost) { min_cost = tc; best = pdep; }
   }
-  if ((double)(cost_now - min_cost) > 0.1) a.plane[center].w = best;
+  if ((double)(s.cost_now - min_cost) > 0.1) a.plane[center].w = best;
 }
 
 }  // namespace dpe

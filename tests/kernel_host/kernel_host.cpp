@@ -158,17 +158,8 @@ extern "C" int host_pm_run(const dpe_problem *p, dpe_pm_out *out) {
   }
   launch(fg, fb, k_get_depth_normal, one);
   for (int parity = 0; parity < 2; ++parity) launch(hg, hb, k_filter_strong, one, parity);
-  std::vector<float2> sw_tab(L * kWinTaps);
-  std::vector<float4> sw_win(L), sw_pl(L), sw_par(L);
-  std::vector<int> sw_valid(L);
-  std::vector<float> sw_cost(L * 61);
-  a.sw_tab = sw_tab.data(); a.sw_win = sw_win.data(); a.sw_pl = sw_pl.data(); a.sw_par = sw_par.data();
-  a.sw_valid = sw_valid.data(); a.sw_cost = sw_cost.data();
-  launch(fg, fb, k_sweep_prepare<DPE_STAGE_FP32>, one);
-  launch(lg, lb, k_sweep_eval<DPE_STAGE_FP32, kSweepClassify>, one);
-  launch(fg, fb, k_sweep_classify, one);
-  launch(lg, lb, k_sweep_eval<DPE_STAGE_FP32, kSweepRefine>, one);
-  launch(fg, fb, k_sweep_refine, one);
+  launch(fg, fb, k_depth_to_weak<DPE_STAGE_FP32>, one);
+  launch(fg, fb, k_local_refine<DPE_STAGE_FP32>, one);
   memcpy(out->plane, a.plane, L * 16);
   memcpy(out->weak, a.weak, L);
   memcpy(out->selected_views, a.views, L * 4);
