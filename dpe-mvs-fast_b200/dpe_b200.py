@@ -25,6 +25,7 @@ WEAK, STRONG, UNKNOWN = 0, 1, 2
 FIRST_INIT, REFINE_INIT, REFINE_ITER = 0, 1, 2
 MEM_HOST, MEM_DEVICE = 0, 1
 FUSE_FP64, FUSE_FLOAT = 0, 1
+TAT_INTERMEDIATE, TAT_ADVANCED = 0, 1
 STAGE_FP32, STAGE_FP16, STAGE_BF16 = 0, 1, 2
 
 
@@ -116,7 +117,7 @@ class Limits(C.Structure):
 EXPORTED = ["dpe_status_string", "dpe_last_error", "dpe_params_default", "dpe_ctx_create", "dpe_ctx_destroy", "dpe_pm_run",
             "dpe_fuse", "dpe_ncc_eval", "dpe_ctx_set_eval_counting", "dpe_scene_run", "dpe_ctx_set_profiling",
             "dpe_ctx_reset_kernel_stats", "dpe_ctx_get_kernel_stats", "dpe_launch_count", "dpe_fp32_peak",
-            "dpe_ncc_eval_noalloc", "dpe_ncc_grad", "dpe_ctx_set_options", "dpe_pm_run_batch"]
+            "dpe_ncc_eval_noalloc", "dpe_ncc_grad", "dpe_ctx_set_options", "dpe_pm_run_batch", "dpe_fuse_tat"]
 
 _lib = None
 
@@ -139,6 +140,7 @@ def load_library(path: Optional[str] = None) -> C.CDLL:
     lib.dpe_ctx_destroy.argtypes = [C.c_void_p]
     lib.dpe_pm_run.argtypes = [C.c_void_p, C.POINTER(Problem), C.POINTER(PMOut)]
     lib.dpe_fuse.argtypes = [C.c_void_p, C.POINTER(FusionIn), C.POINTER(FusionOut)]
+    lib.dpe_fuse_tat.argtypes = [C.c_void_p, C.POINTER(FusionIn), C.c_int, C.POINTER(FusionOut)]
     lib.dpe_ncc_eval.argtypes = [C.c_void_p, C.POINTER(NCCQuery), C.c_void_p]
     lib.dpe_ctx_set_eval_counting.argtypes = [C.c_void_p, C.c_int]
     lib.dpe_scene_run.argtypes = [C.c_void_p, C.POINTER(SceneIn), C.POINTER(Schedule), C.POINTER(SceneOut)]
@@ -219,6 +221,49 @@ def build_problem(images: Sequence, cameras: Sequence[Dict], params: Params, *, 
     pr.seed = int(seed) & 0xFFFFFFFFFFFFFFFF
     pr.memory = memory
     return pr
+
+
+def fusion_input(views: List[Dict], mode: int, memory: int, min_consistent: int, capacity: Optional[int]):
+    """dpe_fusion_in for a list of views (dicts with depth, normal, bgr, camera, src and optional
+    weak and block); returns it, the arrays it points into, and the point capacity (default: every
+    pixel)."""
+    arr = (FusionView * len(views))()
+    keep = [arr]
+    total = 0
+    for i, v in enumerate(views):
+        fv = arr[i]
+        H, W = v["depth"].shape[:2]
+        fv.width, fv.height = W, H
+        fv.depth = _ptr(v["depth"])
+        fv.normal = _ptr(v["normal"])
+        fv.weak = _ptr(v.get("weak"))
+        fv.bgr = _ptr(v["bgr"])
+        fv.block_mask = _ptr(v.get("block"))
+        fv.camera = make_camera(v["camera"])
+        src = np.ascontiguousarray(np.asarray(v["src"], dtype=np.int32))
+        keep.append(src)
+        fv.num_src = len(src)
+        fv.src_views = _ptr(src) if len(src) else None
+        total += W * H
+    cap = total if capacity is None else capacity
+    return FusionIn(len(views), arr, mode, memory, min_consistent), keep, cap
+
+
+def fusion_output(cap: int):
+    """dpe_fusion_out with host buffers for `cap` points (xyz, bgr, origin, num_consistent)."""
+    arrays = dict(xyz=np.zeros((max(cap, 1), 3), np.float32), bgr=np.zeros((max(cap, 1), 3), np.uint8),
+                  origin=np.zeros((max(cap, 1), 2), np.int32), num_consistent=np.zeros(max(cap, 1), np.uint8))
+    fo = FusionOut()
+    fo.capacity = cap
+    fo.xyz, fo.bgr = _ptr(arrays["xyz"]), _ptr(arrays["bgr"])
+    fo.origin, fo.num_consistent = _ptr(arrays["origin"]), _ptr(arrays["num_consistent"])
+    return fo, arrays
+
+
+def fusion_result(fo, arrays: Dict, **extra) -> Dict:
+    n = int(fo.count)
+    k = min(n, int(fo.capacity))
+    return dict(count=n, **{name: a[:k] for name, a in arrays.items()}, **extra)
 
 
 class Context:
@@ -318,38 +363,24 @@ class Context:
     # ------------------------------------------------------------------ fusion
     def fuse(self, views: List[Dict], mode: int = FUSE_FP64, capacity: Optional[int] = None,
              memory: int = MEM_HOST, min_consistent: int = 1) -> Dict:
-        arr = (FusionView * len(views))()
-        keep = []
-        total = 0
-        for i, v in enumerate(views):
-            fv = arr[i]
-            H, W = v["depth"].shape[:2]
-            fv.width, fv.height = W, H
-            fv.depth = _ptr(v["depth"])
-            fv.normal = _ptr(v["normal"])
-            fv.weak = _ptr(v["weak"])
-            fv.bgr = _ptr(v["bgr"])
-            fv.block_mask = _ptr(v.get("block"))
-            fv.camera = make_camera(v["camera"])
-            src = np.ascontiguousarray(np.asarray(v["src"], dtype=np.int32))
-            keep.append(src)
-            fv.num_src = len(src)
-            fv.src_views = _ptr(src) if len(src) else None
-            total += W * H
-        cap = total if capacity is None else capacity
-        xyz = np.zeros((max(cap, 1), 3), np.float32)
-        bgr = np.zeros((max(cap, 1), 3), np.uint8)
-        origin = np.zeros((max(cap, 1), 2), np.int32)
-        ncons = np.zeros(max(cap, 1), np.uint8)
-        fin = FusionIn(len(views), arr, mode, memory, min_consistent)
-        fo = FusionOut()
-        fo.capacity = cap
-        fo.xyz, fo.bgr, fo.origin, fo.num_consistent = _ptr(xyz), _ptr(bgr), _ptr(origin), _ptr(ncons)
+        """RunFusion (DPE.cpp:1387-1548) through dpe_fuse."""
+        fin, keep, cap = fusion_input(views, mode, memory, min_consistent, capacity)
+        fo, arrays = fusion_output(cap)
         st = self.lib.dpe_fuse(self.handle, C.byref(fin), C.byref(fo))
         if st != OK:
             raise DPEError(st, "dpe_fuse")
-        n = int(fo.count)
-        return dict(count=n, xyz=xyz[:n], bgr=bgr[:n], origin=origin[:n], num_consistent=ncons[:n], gpu_ms=fo.gpu_ms)
+        return fusion_result(fo, arrays, gpu_ms=fo.gpu_ms)
+
+    def fuse_tat(self, views: List[Dict], variant: int = TAT_INTERMEDIATE, mode: int = FUSE_FLOAT,
+                 capacity: Optional[int] = None, memory: int = MEM_HOST) -> Dict:
+        """RunFusion_TAT_Intermediate / RunFusion_TAT_advanced (DPE.cpp:1550-1867) through
+        dpe_fuse_tat; the views' "weak" maps are not needed."""
+        fin, keep, cap = fusion_input(views, mode, memory, 1, capacity)
+        fo, arrays = fusion_output(cap)
+        st = self.lib.dpe_fuse_tat(self.handle, C.byref(fin), variant, C.byref(fo))
+        if st != OK:
+            raise DPEError(st, "dpe_fuse_tat")
+        return fusion_result(fo, arrays, gpu_ms=fo.gpu_ms)
 
     # ------------------------------------------------------------------ whole scene
     def scene_run(self, gray, bgr, cameras, srcs, edges=None, labels=None, *, num_levels=0, refine_calls=3,

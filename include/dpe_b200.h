@@ -270,6 +270,24 @@ int dpe_pm_run_batch(dpe_ctx *ctx, const dpe_problem *problems, int count, dpe_p
  * (ExportPointCloud, DPE.cpp:532-572). */
 int dpe_fuse(dpe_ctx *ctx, const dpe_fusion_in *in, dpe_fusion_out *out);
 
+/* The two Tanks-and-Temples fusion rules, which the reference declares beside RunFusion
+ * (DPE.h:97-98) for its TAT runs:
+ *   DPE_TAT_INTERMEDIATE  RunFusion_TAT_Intermediate (DPE.cpp:1550-1718): a pixel is kept at the
+ *                         first k in 2..num_src for which at least k sources have reprojection
+ *                         error < 0.25 k, relative depth difference < k / 3500 and normal angle
+ *                         < 3k + 4 degrees; its colour is the mean of the reference pixel and
+ *                         those sources' pixels.
+ *   DPE_TAT_ADVANCED      RunFusion_TAT_advanced (DPE.cpp:1720-1867): the same without the angle
+ *                         bound, relative depth < k / 3000, colour of the reference pixel only.
+ * As in the reference, a source's differences persist from pixel to pixel within a view: a
+ * source that is out of the image, masked or without depth at a pixel counts with the values of
+ * the last pixel of the view where it was tested (the difference vector is set once per view,
+ * DPE.cpp:1640 / 1804).  A kept pixel masks itself; only the masks of sources are read.
+ * `weak` may be NULL and `min_consistent` is not used; `num_consistent` receives the number of
+ * sources counted at the accepting k.  Views, points and errors otherwise as dpe_fuse. */
+enum { DPE_TAT_INTERMEDIATE = 0, DPE_TAT_ADVANCED = 1 };
+int dpe_fuse_tat(dpe_ctx *ctx, const dpe_fusion_in *in, int variant, dpe_fusion_out *out);
+
 /* Replaces main()'s PatchMatch schedule and fusion (main.cpp:385-461) for a whole scene, with every
  * view's state kept in device memory between calls: per level the float image pyramid
  * (SceneCache::GetGrayFloatImage, DPE.cpp:720-737), one FIRST_INIT / REFINE_INIT call and

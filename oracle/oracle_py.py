@@ -38,6 +38,7 @@ def load() -> C.CDLL:
     lib.oracle_ncc_strong.argtypes = [C.POINTER(D.NCCQuery), C.c_int, C.c_void_p]
     lib.oracle_pm_run.argtypes = [C.POINTER(D.Problem), C.POINTER(D.PMOut), C.c_int]
     lib.oracle_fuse.argtypes = [C.POINTER(D.FusionIn), C.POINTER(D.FusionOut)]
+    lib.oracle_fuse_tat.argtypes = [C.POINTER(D.FusionIn), C.c_int, C.POINTER(D.FusionOut)]
     lib.oracle_set_raw_moments.argtypes = [C.c_int]
     lib.oracle_ncc_strong_grad.argtypes = [C.POINTER(D.NCCQuery), C.c_void_p, C.c_void_p, C.c_void_p]
     _lib = lib
@@ -96,37 +97,22 @@ def pm_run(images, cameras, params, threads: int = 0, **kw) -> Dict:
 
 
 def fuse(views: List[Dict], mode: int = D.FUSE_FP64, capacity: Optional[int] = None, min_consistent: int = 1) -> Dict:
-    arr = (D.FusionView * len(views))()
-    keep = []
-    total = 0
-    for i, v in enumerate(views):
-        fv = arr[i]
-        H, W = v["depth"].shape[:2]
-        fv.width, fv.height = W, H
-        fv.depth = v["depth"].ctypes.data
-        fv.normal = v["normal"].ctypes.data
-        fv.weak = v["weak"].ctypes.data
-        fv.bgr = v["bgr"].ctypes.data
-        fv.block_mask = v["block"].ctypes.data if v.get("block") is not None else None
-        fv.camera = D.make_camera(v["camera"])
-        src = np.ascontiguousarray(np.asarray(v["src"], dtype=np.int32))
-        keep.append(src)
-        fv.num_src = len(src)
-        fv.src_views = src.ctypes.data if len(src) else None
-        total += W * H
-    cap = total if capacity is None else capacity
-    xyz = np.zeros((max(cap, 1), 3), np.float32)
-    bgr = np.zeros((max(cap, 1), 3), np.uint8)
-    origin = np.zeros((max(cap, 1), 2), np.int32)
-    ncons = np.zeros(max(cap, 1), np.uint8)
-    fin = D.FusionIn(len(views), arr, mode, D.MEM_HOST, min_consistent)
-    fo = D.FusionOut()
-    fo.capacity = cap
-    fo.xyz, fo.bgr, fo.origin, fo.num_consistent = xyz.ctypes.data, bgr.ctypes.data, origin.ctypes.data, ncons.ctypes.data
+    """The CPU restatement of RunFusion (DPE.cpp:1387-1548)."""
+    fin, keep, cap = D.fusion_input(views, mode, D.MEM_HOST, min_consistent, capacity)
+    fo, arrays = D.fusion_output(cap)
     st = load().oracle_fuse(C.byref(fin), C.byref(fo))
-    n = int(fo.count)
     if st not in (0, D.ERR_CAPACITY):
         raise RuntimeError(f"oracle_fuse failed with status {st}")
-    n_keep = min(n, cap)
-    return dict(count=n, status=st, xyz=xyz[:n_keep], bgr=bgr[:n_keep], origin=origin[:n_keep],
-                num_consistent=ncons[:n_keep])
+    return D.fusion_result(fo, arrays, status=st)
+
+
+def fuse_tat(views: List[Dict], variant: int = D.TAT_INTERMEDIATE, mode: int = D.FUSE_FLOAT,
+             capacity: Optional[int] = None) -> Dict:
+    """The CPU restatement of RunFusion_TAT_Intermediate / RunFusion_TAT_advanced
+    (DPE.cpp:1550-1867)."""
+    fin, keep, cap = D.fusion_input(views, mode, D.MEM_HOST, 1, capacity)
+    fo, arrays = D.fusion_output(cap)
+    st = load().oracle_fuse_tat(C.byref(fin), variant, C.byref(fo))
+    if st not in (0, D.ERR_CAPACITY):
+        raise RuntimeError(f"oracle_fuse_tat failed with status {st}")
+    return D.fusion_result(fo, arrays, status=st)

@@ -14,6 +14,8 @@ Fixtures:
   pm_tiny.npz          FIRST_INIT call, then a REFINE_ITER call with APD, edges, labels and the
                        geometric term, on the 64x48 3-view scene
   fusion_tiny.npz      fusion of noisy ground-truth depth maps, FP64 and float modes
+  fusion_tat_tiny.npz  both TAT fusion rules, FP64 and float modes, on the 64x48 3-view scene with
+                       depth holes, a source band without depth and a block mask
 """
 from __future__ import annotations
 
@@ -124,6 +126,34 @@ def make_fusion(path: str) -> None:
     np.savez_compressed(path, **out)
 
 
+def make_fusion_tat(path: str) -> None:
+    from test_fusion_tat import tat_views
+
+    sc = S.make_scene("tiny", seed=5)
+    views = tat_views(sc, noise=2e-4, seed=19)
+    out = dict(depth=np.stack([v["depth"] for v in views]), normal=np.stack([v["normal"] for v in views]),
+               bgr=np.stack([v["bgr"] for v in views]), cams=cams_to_array([v["camera"] for v in views]),
+               src=np.array([v["src"] for v in views], np.int32),
+               has_block=np.array([v["block"] is not None for v in views]),
+               block=np.stack([v["block"] if v["block"] is not None else np.full(v["depth"].shape, 255, np.uint8)
+                               for v in views]))
+    for vname, variant in (("inter", D.TAT_INTERMEDIATE), ("adv", D.TAT_ADVANCED)):
+        for mname, mode in (("fp64", D.FUSE_FP64), ("float", D.FUSE_FLOAT)):
+            r = O.fuse_tat(views, variant, mode)
+            tag = f"{vname}_{mname}"
+            for k in ("xyz", "bgr", "origin", "num_consistent"):
+                out[f"{tag}_{k}"] = r[k]
+            out[f"{tag}_count"] = np.int64(r["count"])
+    np.savez_compressed(path, **out)
+
+
+def fusion_tat_views_from(z) -> list:
+    cams = cams_from_array(z["cams"])
+    return [dict(depth=np.ascontiguousarray(z["depth"][v]), normal=np.ascontiguousarray(z["normal"][v]),
+                 bgr=np.ascontiguousarray(z["bgr"][v]), camera=cams[v], src=[int(s) for s in z["src"][v]],
+                 block=np.ascontiguousarray(z["block"][v]) if z["has_block"][v] else None) for v in range(len(cams))]
+
+
 def fusion_views_from(z) -> list:
     cams = cams_from_array(z["cams"])
     return [dict(depth=np.ascontiguousarray(z["depth"][v]), normal=np.ascontiguousarray(z["normal"][v]),
@@ -136,6 +166,7 @@ def main() -> int:
     make_ncc(os.path.join(HERE, "ncc_small.npz"))
     make_pm(os.path.join(HERE, "pm_tiny.npz"))
     make_fusion(os.path.join(HERE, "fusion_tiny.npz"))
+    make_fusion_tat(os.path.join(HERE, "fusion_tat_tiny.npz"))
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)), "bytes")

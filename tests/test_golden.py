@@ -82,6 +82,20 @@ def test_golden_fusion_oracle_reproduces():
             assert np.array_equal(r[k], z[f"{tag}_{k}"]), (tag, k)
 
 
+TAT_CASES = [(f"{vn}_{mn}", var, mode) for vn, var in (("inter", D.TAT_INTERMEDIATE), ("adv", D.TAT_ADVANCED))
+             for mn, mode in (("fp64", D.FUSE_FP64), ("float", D.FUSE_FLOAT))]
+
+
+def test_golden_fusion_tat_oracle_reproduces():
+    z = _load("fusion_tat_tiny.npz")
+    views = G.fusion_tat_views_from(z)
+    for tag, variant, mode in TAT_CASES:
+        r = O.fuse_tat(views, variant, mode)
+        assert r["count"] == int(z[f"{tag}_count"]), tag
+        for k in ("xyz", "bgr", "origin", "num_consistent"):
+            assert np.array_equal(r[k], z[f"{tag}_{k}"]), (tag, k)
+
+
 # ------------------------------------------------------------------ the kernels against the fixtures (GPU)
 @pytest.mark.gpu
 def test_golden_ncc_gpu(ctx):
@@ -122,3 +136,17 @@ def test_golden_fusion_gpu(ctx):
             assert np.array_equal(r[k], z[f"{tag}_{k}"]), (tag, k)
     r = ctx.fuse(views, D.FUSE_FLOAT)
     assert abs(r["count"] - int(z["float_count"])) <= 2
+
+
+@pytest.mark.gpu
+def test_golden_fusion_tat_gpu(ctx):
+    z = _load("fusion_tat_tiny.npz")
+    views = G.fusion_tat_views_from(z)
+    for tag, variant, mode in TAT_CASES:
+        r = ctx.fuse_tat(views, variant, mode)
+        if mode == D.FUSE_FLOAT:  # float acos: last-bit differences may move a point
+            assert abs(r["count"] - int(z[f"{tag}_count"])) <= 2, tag
+            continue
+        assert r["count"] == int(z[f"{tag}_count"]), tag
+        for k in ("xyz", "bgr", "origin", "num_consistent"):
+            assert np.array_equal(r[k], z[f"{tag}_{k}"]), (tag, k)
