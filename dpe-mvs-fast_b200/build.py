@@ -27,6 +27,7 @@ UNITS = {
     "capi.cu": [],
     "scene.cu": [],
     "fusion.cu": ["-fmad=false"],
+    "edges.cu": [],
 }
 
 

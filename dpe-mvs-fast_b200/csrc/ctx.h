@@ -145,3 +145,11 @@ struct dpe_ctx {
       (ctx)->pending.push_back(dpe_ctx::Pending{kid, t0_, t1_});    \
     }                                                               \
   } while (0)
+
+// Edge maps of EdgeSegment mode 0 on the device (edges.cu).  dpe_edge_reserve sizes the scratch
+// for images of up to `pixels`; dpe_edge_map_device enqueues the pipeline on ctx->stream for an
+// 8-bit image, or for a float level image (converted like convertTo(CV_8UC1)) when `level` is
+// given; dpe_edge_check reports the union-find guard after the stream has been synchronised.
+int dpe_edge_reserve(dpe_ctx *ctx, size_t pixels);
+int dpe_edge_map_device(dpe_ctx *ctx, const float *level, const uint8_t *image, int w, int h, uint8_t *edge);
+int dpe_edge_check(dpe_ctx *ctx);

@@ -135,13 +135,16 @@ extern "C" int dpe_scene_run(dpe_ctx *ctx, const dpe_scene *sc, const dpe_schedu
   if (sch->refine_calls < 0 || sch->max_iterations < 0) return DPE_ERR_INVALID_ARGUMENT;
   if (sch->batch_views != 0 && sch->batch_views != 1) return DPE_ERR_INVALID_ARGUMENT;
   if (sch->batch_views && sc->num_views > DPE_MAX_BATCH) return DPE_ERR_INVALID_ARGUMENT;
-  const bool have_edges = sc->views[0].edges != nullptr, have_labels = sc->views[0].labels != nullptr;
+  if (sch->device_edges != 0 && sch->device_edges != 1) return DPE_ERR_INVALID_ARGUMENT;
+  const bool given_edges = sc->views[0].edges != nullptr, have_labels = sc->views[0].labels != nullptr;
+  if (sch->device_edges && given_edges) return DPE_ERR_INVALID_ARGUMENT;
+  const bool have_edges = given_edges || sch->device_edges;
   for (int v = 0; v < V; ++v) {
     const dpe_scene_view &sv = sc->views[v];
     if (!sv.gray || sv.num_src < 1 || sv.num_src > DPE_MAX_IMAGES - 1 || !sv.src_views) return DPE_ERR_INVALID_ARGUMENT;
     for (int j = 0; j < sv.num_src; ++j)
       if (sv.src_views[j] < 0 || sv.src_views[j] >= V || sv.src_views[j] == v) return DPE_ERR_INVALID_ARGUMENT;
-    if ((sv.edges != nullptr) != have_edges || (sv.labels != nullptr) != have_labels) return DPE_ERR_INVALID_ARGUMENT;
+    if ((sv.edges != nullptr) != given_edges || (sv.labels != nullptr) != have_labels) return DPE_ERR_INVALID_ARGUMENT;
     if (sch->fuse_mode >= 0 && !sv.bgr) return DPE_ERR_INVALID_ARGUMENT;
   }
   DPE_TRY(cudaSetDevice(ctx->device));
@@ -188,14 +191,17 @@ extern "C" int dpe_scene_run(dpe_ctx *ctx, const dpe_scene *sc, const dpe_schedu
   if (have_edges || have_labels) {
     size_t per_view = 0;
     for (int l = 0; l < L; ++l) per_view += (size_t)lw[l] * lh[l];
-    uint8_t *e_dev = (host && have_edges) ? A.get<uint8_t>("sc_edges", per_view * V) : nullptr;
+    uint8_t *e_dev = ((host && given_edges) || sch->device_edges) ? A.get<uint8_t>("sc_edges", per_view * V) : nullptr;
+    if (sch->device_edges && dpe_edge_reserve(ctx, (size_t)lw[L - 1] * lh[L - 1]) != DPE_OK) return DPE_ERR_OUT_OF_MEMORY;
     int32_t *l_dev = (host && have_labels) ? A.get<int32_t>("sc_labels", per_view * V) : nullptr;
     if (!A.ok()) return DPE_ERR_OUT_OF_MEMORY;
     size_t off = 0;
     for (int v = 0; v < V; ++v)
       for (int l = 0; l < L; ++l) {
         const size_t n = (size_t)lw[l] * lh[l];
-        if (have_edges) {
+        if (sch->device_edges) {
+          edge[v][l] = e_dev + off;  // made when the level image is
+        } else if (have_edges) {
           if (host) {
             DPE_TRY(cudaMemcpyAsync(e_dev + off, sc->views[v].edges[l], n, cudaMemcpyHostToDevice, s));
             edge[v][l] = e_dev + off;
@@ -247,6 +253,11 @@ extern "C" int dpe_scene_run(dpe_ctx *ctx, const dpe_scene *sc, const dpe_schedu
       } else {
         k_resize_linear<<<g2, b2, 0, s>>>(gray_full + LF * v, W, H, st[v].img, w, h, (double)W / w, (double)H / h);
         DPE_LAUNCHED("k_resize_linear", s);
+      }
+      // the level's edge map (GetProblemEdges computes it from this same resize, main.cpp:170-178)
+      if (sch->device_edges) {
+        const int est = dpe_edge_map_device(ctx, st[v].img, nullptr, w, h, const_cast<uint8_t *>(edge[v][l]));
+        if (est != DPE_OK) return est;
       }
     }
     // state from the previous level, rescaled (DPE::InuputInitialization, DPE.cpp:1019-1052)
@@ -416,6 +427,10 @@ extern "C" int dpe_scene_run(dpe_ctx *ctx, const dpe_scene *sc, const dpe_schedu
       DPE_TRY(cudaMemcpyAsync(out->selected_views[v], st[v].views, nf * 4, d2o, s));
   }
   DPE_TRY(cudaStreamSynchronize(s));
+  if (sch->device_edges) {
+    const int est = dpe_edge_check(ctx);
+    if (est != DPE_OK) return est;
+  }
   float ms = 0.f;
   DPE_TRY(cudaEventElapsedTime(&ms, e0, e1));
   out->gpu_ms = ms;

@@ -48,7 +48,7 @@ def connect(binary: np.ndarray):
 
 
 def _border_fix(d: np.ndarray) -> None:
-    """Zero the image border where the adjacent inner pixel is zero (DPE.cpp:242-253)."""
+    """Zero the image border where the adjacent inner pixel is zero (DPE.cpp:239-250)."""
     rows, cols = d.shape
     for y in range(rows):
         if d[y, 1] == 0:
@@ -102,7 +102,9 @@ def edge_segment(scale: int, src: np.ndarray, mode: int, use_canny: bool, high_r
             if acc > half:
                 median = i
                 break
-        t1 = int((1 - 0.67) * median)
+        # `const float sigma = 0.67; int threshold1 = (1 - sigma) * median_val;` in float (the double
+        # form truncates 32.99999 to 32 at median 100, and 65 at 200)
+        t1 = int(np.float32(np.float32(1.0) - np.float32(0.67)) * np.float32(median))
         t2 = median
         dst = cv2.Canny(src, t1, t2, apertureSize=3, L2gradient=True)
     if mode == 0:

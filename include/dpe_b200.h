@@ -190,6 +190,9 @@ typedef struct dpe_schedule {
   int batch_views;      /* 0: views one after another within a call, each reading the depths its
                            predecessors wrote (the reference's order); 1: all views of a call in one
                            dpe_pm_run_batch, each reading the previous call's depths            */
+  int device_edges;     /* 1: each level's edge map is made on the device from the level image
+                           (GetProblemEdges' EdgeSegment mode 0, main.cpp:170-197; dpe_edge_map);
+                           views[].edges must then be NULL                                       */
 } dpe_schedule;
 
 typedef struct dpe_scene {
@@ -287,6 +290,15 @@ int dpe_fuse(dpe_ctx *ctx, const dpe_fusion_in *in, dpe_fusion_out *out);
  * sources counted at the accepting k.  Views, points and errors otherwise as dpe_fuse. */
 enum { DPE_TAT_INTERMEDIATE = 0, DPE_TAT_ADVANCED = 1 };
 int dpe_fuse_tat(dpe_ctx *ctx, const dpe_fusion_in *in, int variant, dpe_fusion_out *out);
+
+/* The edge map of EdgeSegment (DPE.cpp:136-250) as GetProblemEdges requests it for a pyramid level
+ * (EdgeSegment(scale, image, 0, true, high_res_img), main.cpp:182-197): cv::Canny with aperture 3,
+ * the L2 gradient and thresholds (1 - 0.67) * median and median of the image's histogram, then the
+ * border rule of DPE.cpp:239-250.  `image` is the level image converted to 8 bits (width*height,
+ * row-major), `edge_out` receives width*height values 0 / 255; both in `memory`.  The reference
+ * writes the result to edges_<scale>.dmb; dpe_scene_run can make these maps itself
+ * (dpe_schedule.device_edges). */
+int dpe_edge_map(dpe_ctx *ctx, const uint8_t *image, int width, int height, int memory, uint8_t *edge_out);
 
 /* Replaces main()'s PatchMatch schedule and fusion (main.cpp:385-461) for a whole scene, with every
  * view's state kept in device memory between calls: per level the float image pyramid
