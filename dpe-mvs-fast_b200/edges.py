@@ -3,8 +3,9 @@
 Restates EdgeSegment / Roberts / Connect (DPE.cpp:9-291) and GetProblemEdges (main.cpp:166-221)
 with the same OpenCV calls through cv2: Canny with a median-derived threshold for the edge map
 (mode 0), and for the label map (mode 1) a Roberts gradient on the 4x-downsampled image,
-connected components, Hough-line closure of large weak regions, a second labelling at the
-target scale and small regions marked -1.  The reference caches these per scale as
+the reference's region labelling (Connect, whose lossy joins can split a region), Hough-line
+closure of large weak regions, a second labelling at the target scale and small regions marked
+-1.  The reference caches these per scale as
 edges_<scale>.dmb / labels_<scale>.dmb.
 """
 from __future__ import annotations
@@ -36,15 +37,77 @@ def roberts(src: np.ndarray) -> np.ndarray:
 
 
 def connect(binary: np.ndarray):
-    """Connected components of the zero pixels, 4-connected (Connect, DPE.cpp:27-134).
+    """Connect (DPE.cpp:27-134): the reference's labelling of the pixels other than 255.
 
-    Returns (labels int32, counts) with label 0 for the 255 pixels and components numbered in
-    raster order of their first pixel."""
-    from scipy import ndimage
+    Not plain connected components.  The reference scans in raster order with provisional labels
+    (a pixel joins its left and upper neighbours when both it and they are 0, taking the smaller
+    label; otherwise it opens a new label) and records a join of two different labels as
+    connection[larger] = smaller, overwriting any earlier join of that label; the final label of a
+    provisional label is the end of its connection chain, renumbered in increasing order.  An
+    overwritten join is lost, so a region can end up split.  Returns (labels int32, counts per
+    label), label 0 being the 255 pixels.
 
-    lab, n = ndimage.label(binary == 0, structure=[[0, 1, 0], [1, 1, 1], [0, 1, 0]])
-    counts = np.bincount(lab.ravel(), minlength=n + 1)
-    return lab.astype(np.int32), counts
+    Evaluated a row at a time: along a run of left-joined pixels the provisional label is the
+    running minimum of the run's opening label and the upper labels where the pixel joins upwards
+    (a segmented minimum-scan), new labels are numbered by a prefix count of the run openings
+    without an upper join, and for each label only the last join in raster order is kept."""
+    d = np.asarray(binary)
+    rows, cols = d.shape
+    lab = np.zeros((rows, cols), np.int64)
+    nxt = 1
+    last_join = {}  # larger provisional label -> smaller label of its last join
+    zero_prev = None
+    lab_prev = None
+    xs = np.arange(cols)
+    BIG = np.int64(1) << 40
+    for y in range(rows):
+        row = d[y]
+        labelled = row != 255
+        zero = row == 0
+        leftj = np.zeros(cols, bool)
+        leftj[1:] = zero[1:] & zero[:-1]
+        upj = zero & zero_prev if zero_prev is not None else np.zeros(cols, bool)
+        opens = labelled & ~leftj & ~upj
+        new_ids = nxt + np.cumsum(opens) - 1
+        nxt += int(opens.sum())
+        up = lab_prev if lab_prev is not None else np.zeros(cols, np.int64)
+        # value contributed at each pixel: its upper label where it joins up, its new label where
+        # it opens one, +inf otherwise (a left-joined pixel takes the running value)
+        val = np.where(upj, up, np.where(opens, new_ids, BIG))
+        run = np.cumsum(~leftj) - 1  # run index; a run restarts wherever there is no left join
+        shifted = val - run * (BIG * 4)
+        lrow = np.minimum.accumulate(shifted) + run * (BIG * 4)
+        lrow = np.where(labelled, lrow, 0)
+        # joins: both neighbours joined and their labels differ (the left pixel's final label)
+        both = leftj & upj
+        if both.any():
+            xb = xs[both]
+            left_lab = lrow[xb - 1]
+            up_lab = up[xb]
+            diff = left_lab != up_lab
+            big_l = np.maximum(left_lab, up_lab)[diff]
+            small_l = np.minimum(left_lab, up_lab)[diff]
+            for t, v in zip(big_l.tolist(), small_l.tolist()):
+                last_join[t] = v
+        lab[y] = lrow
+        zero_prev, lab_prev = zero, lrow
+    conn = np.arange(nxt, dtype=np.int64)
+    if last_join:
+        t = np.fromiter(last_join.keys(), np.int64)
+        conn[t] = np.fromiter(last_join.values(), np.int64)
+    while True:  # chain ends: every join points to a smaller label, so this converges
+        nc = conn[conn]
+        if np.array_equal(nc, conn):
+            break
+        conn = nc
+    is_root = conn == np.arange(nxt)
+    is_root[0] = False
+    mapping = np.zeros(nxt, np.int64)
+    mapping[is_root] = np.arange(1, int(is_root.sum()) + 1)
+    final = mapping[conn]
+    out = final[lab]
+    counts = np.bincount(out.ravel(), minlength=int(is_root.sum()) + 1)
+    return out.astype(np.int32), counts
 
 
 def _border_fix(d: np.ndarray) -> None:

@@ -39,6 +39,7 @@ def load() -> C.CDLL:
     lib.oracle_pm_run.argtypes = [C.POINTER(D.Problem), C.POINTER(D.PMOut), C.c_int]
     lib.oracle_fuse.argtypes = [C.POINTER(D.FusionIn), C.POINTER(D.FusionOut)]
     lib.oracle_fuse_tat.argtypes = [C.POINTER(D.FusionIn), C.c_int, C.POINTER(D.FusionOut)]
+    lib.oracle_connect.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
     lib.oracle_set_raw_moments.argtypes = [C.c_int]
     lib.oracle_ncc_strong_grad.argtypes = [C.POINTER(D.NCCQuery), C.c_void_p, C.c_void_p, C.c_void_p]
     _lib = lib
@@ -116,3 +117,17 @@ def fuse_tat(views: List[Dict], variant: int = D.TAT_INTERMEDIATE, mode: int = D
     if st not in (0, D.ERR_CAPACITY):
         raise RuntimeError(f"oracle_fuse_tat failed with status {st}")
     return D.fusion_result(fo, arrays, status=st)
+
+
+def connect(img: np.ndarray):
+    """The CPU restatement of Connect (DPE.cpp:27-134): (labels int32, counts per label)."""
+    img = np.ascontiguousarray(img, dtype=np.uint8)
+    rows, cols = img.shape
+    labels = np.zeros((rows, cols), np.int32)
+    cap = rows * cols + 1
+    counts = np.zeros(cap, np.int32)
+    n = C.c_int(0)
+    st = load().oracle_connect(img.ctypes.data, cols, rows, labels.ctypes.data, counts.ctypes.data, cap, C.byref(n))
+    if st != 0:
+        raise RuntimeError(f"oracle_connect failed with status {st}")
+    return labels, counts[: n.value].copy()
