@@ -40,6 +40,10 @@ def load() -> C.CDLL:
     lib.oracle_fuse.argtypes = [C.POINTER(D.FusionIn), C.POINTER(D.FusionOut)]
     lib.oracle_fuse_tat.argtypes = [C.POINTER(D.FusionIn), C.c_int, C.POINTER(D.FusionOut)]
     lib.oracle_connect.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
+    lib.oracle_resize_u8.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int]
+    lib.oracle_hough_lines_p.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int,
+                                         C.c_void_p]
+    lib.oracle_edge_labels.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int]
     lib.oracle_set_raw_moments.argtypes = [C.c_int]
     lib.oracle_ncc_strong_grad.argtypes = [C.POINTER(D.NCCQuery), C.c_void_p, C.c_void_p, C.c_void_p]
     _lib = lib
@@ -131,3 +135,39 @@ def connect(img: np.ndarray):
     if st != 0:
         raise RuntimeError(f"oracle_connect failed with status {st}")
     return labels, counts[: n.value].copy()
+
+
+def resize_u8(img: np.ndarray, width: int, height: int) -> np.ndarray:
+    """cv::resize(img, (width, height), INTER_LINEAR) for an 8-bit image, restated."""
+    img = np.ascontiguousarray(img, dtype=np.uint8)
+    out = np.zeros((height, width), np.uint8)
+    if load().oracle_resize_u8(img.ctypes.data, img.shape[1], img.shape[0], out.ctypes.data, width, height) != 0:
+        raise RuntimeError("oracle_resize_u8 failed")
+    return out
+
+
+def hough_lines_p(img: np.ndarray, threshold: int, min_line_length: int, max_line_gap: int) -> List:
+    """cv::HoughLinesP(img, 1, CV_PI / 180, threshold, min_line_length, max_line_gap), restated."""
+    img = np.ascontiguousarray(img, dtype=np.uint8)
+    cap = 1 << 16
+    buf = np.zeros((cap, 4), np.int32)
+    n = C.c_int(0)
+    st = load().oracle_hough_lines_p(img.ctypes.data, img.shape[1], img.shape[0], threshold, min_line_length,
+                                     max_line_gap, buf.ctypes.data, cap, C.byref(n))
+    if st != 0:
+        raise RuntimeError(f"oracle_hough_lines_p failed with status {st}")
+    return [tuple(int(v) for v in r) for r in buf[: n.value]]
+
+
+def edge_labels(gray: np.ndarray, scale: int, high_res_img: bool = True) -> np.ndarray:
+    """EdgeSegment(scale, gray, 1, false, high_res_img) (DPE.cpp:136-291), restated: the int32 label
+    map at the level size, 0 on edges and -1 on small regions."""
+    gray = np.ascontiguousarray(gray, dtype=np.uint8)
+    rows, cols = gray.shape
+    f = np.float32(1.0) / np.float32(1 << scale)
+    w, h = int(np.round(np.float32(cols) * f)), int(np.round(np.float32(rows) * f))
+    out = np.zeros((h, w), np.int32)
+    if load().oracle_edge_labels(gray.ctypes.data, cols, rows, scale, 1 if high_res_img else 0, out.ctypes.data,
+                                 w, h) != 0:
+        raise RuntimeError("oracle_edge_labels failed")
+    return out

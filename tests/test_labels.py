@@ -111,3 +111,68 @@ def test_joins_are_lossy():
             assert np.array_equal(lab, connect_literal(m)[0]) and np.array_equal(lab, E.connect(m)[0])
             return
     pytest.fail("no lossy 8x8 case found")
+
+
+# ------------------------------------------------------------------ the OpenCV parts and the whole map
+def test_resize_u8_matches_opencv():
+    rng = np.random.default_rng(4)
+    for (sh, sw, dh, dw) in [(1200, 1600, 600, 800), (600, 800, 300, 400), (75, 100, 300, 400), (37, 51, 150, 200),
+                             (300, 400, 1200, 1600), (20, 30, 77, 93), (301, 401, 150, 200), (7, 9, 300, 301),
+                             (150, 200, 75, 100), (33, 47, 33, 47)]:
+        img = rng.integers(0, 256, (sh, sw), dtype=np.uint8)
+        for use_ipp in (True, False):
+            cv2.ipp.setUseIPP(use_ipp)
+            try:
+                ref = cv2.resize(img, (dw, dh), interpolation=cv2.INTER_LINEAR)
+            finally:
+                cv2.ipp.setUseIPP(True)
+            assert np.array_equal(O.resize_u8(img, dw, dh), ref), ((sh, sw, dh, dw), use_ipp)
+
+
+def _weak_region_borders(gray, scale=0):
+    """EdgeSegment's Hough inputs: the outer border of each large weak region (DPE.cpp:164-187)."""
+    rows, cols = gray.shape
+    weak_tex_num = int(1.0 * rows * cols / (1024 << scale << scale))
+    d = cv2.resize(gray, (cols // 2, rows // 2), interpolation=cv2.INTER_LINEAR)
+    d = cv2.resize(d, (d.shape[1] // 2, d.shape[0] // 2), interpolation=cv2.INTER_LINEAR)
+    thr = int(int(min(d.shape)) / 30.0)
+    _, d = cv2.threshold(E.roberts(d), 4, 255, cv2.THRESH_BINARY)
+    lab, cnt = E.connect(d)
+    out = []
+    for k in range(1, len(cnt)):
+        if cnt[k] < weak_tex_num:
+            continue
+        inside = lab == k
+        border = np.zeros_like(inside)
+        border[:, 1:] |= inside[:, :-1]
+        border[:, :-1] |= inside[:, 1:]
+        border[1:, :] |= inside[:-1, :]
+        border[:-1, :] |= inside[1:, :]
+        out.append((np.where(border & ~inside, 255, 0).astype(np.uint8), thr))
+    return out
+
+
+def test_hough_lines_p_matches_opencv():
+    import math
+
+    n = 0
+    for name in ("small_weak", "c2_small"):
+        sc = h.S.make_scene(name, seed=2)
+        for v in range(3):
+            for img, thr in _weak_region_borders(sc.gray[v]):
+                ref = cv2.HoughLinesP(img, 1, math.pi / 180, thr, minLineLength=thr, maxLineGap=thr)
+                ref = [] if ref is None else [tuple(int(t) for t in r) for r in ref[:, 0, :]]
+                assert O.hough_lines_p(img, thr, thr, thr) == ref
+                n += len(ref)
+    assert n > 200
+
+
+@pytest.mark.parametrize("name,scale", [("small_weak", 0), ("c2_small", 0), ("c2_small", 1), ("c2_small", 2)])
+def test_edge_labels_match_host_preprocessing(name, scale):
+    """The whole label map: the oracle's restatement against edges.py, which runs the same
+    sequence with cv2's resize, threshold, HoughLinesP and line."""
+    sc = h.S.make_scene(name, seed=2)
+    for v in range(2):
+        o = O.edge_labels(sc.gray[v], scale)
+        ref = E.edge_segment(scale, sc.gray[v], 1, False)
+        assert o.shape == ref.shape and np.array_equal(o, ref), (v, int((o != ref).sum()))
