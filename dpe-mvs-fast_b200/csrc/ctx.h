@@ -153,3 +153,9 @@ struct dpe_ctx {
 int dpe_edge_reserve(dpe_ctx *ctx, size_t pixels);
 int dpe_edge_map_device(dpe_ctx *ctx, const float *level, const uint8_t *image, int w, int h, uint8_t *edge);
 int dpe_edge_check(dpe_ctx *ctx);
+// Label maps of EdgeSegment mode 1 on the device (edges.cu): from the full-resolution 8-bit image
+// `gray` (W x H, device memory) the int32 map at the level size ow x oh of `scale`; the stream is
+// synchronised once inside (the number of large weak regions sizes the Hough launch).
+int dpe_edge_labels_device(dpe_ctx *ctx, const uint8_t *gray, int W, int H, int scale, int high_res_img, int32_t *out,
+                           int ow, int oh);
+int dpe_edge_labels_check(dpe_ctx *ctx);

@@ -25,6 +25,7 @@ enum KernelId {
   KID_FUSE_EMIT,
   KID_FUSE_TAT,
   KID_EDGE_MAP,
+  KID_EDGE_LABELS,
   KID_SCENE_MISC,
   KID_COUNT
 };
@@ -35,4 +36,4 @@ static const char *const kKernelNames[KID_COUNT] = {
     "k_weak_decide",   "k_weak_finish",     "k_get_depth_normal",
     "k_filter_strong", "k_depth_to_weak",   "k_local_refine",        "k_pad_image",      "k_ncc_queries",
     "k_fuse_entries",  "k_fuse_waves",      "k_fuse_emit",           "k_fuse_tat",       "k_edge_map",
-    "k_scene_misc"};
+    "k_edge_labels",   "k_scene_misc"};

@@ -136,15 +136,17 @@ extern "C" int dpe_scene_run(dpe_ctx *ctx, const dpe_scene *sc, const dpe_schedu
   if (sch->batch_views != 0 && sch->batch_views != 1) return DPE_ERR_INVALID_ARGUMENT;
   if (sch->batch_views && sc->num_views > DPE_MAX_BATCH) return DPE_ERR_INVALID_ARGUMENT;
   if (sch->device_edges != 0 && sch->device_edges != 1) return DPE_ERR_INVALID_ARGUMENT;
-  const bool given_edges = sc->views[0].edges != nullptr, have_labels = sc->views[0].labels != nullptr;
-  if (sch->device_edges && given_edges) return DPE_ERR_INVALID_ARGUMENT;
+  if (sch->device_labels != 0 && sch->device_labels != 1) return DPE_ERR_INVALID_ARGUMENT;
+  const bool given_edges = sc->views[0].edges != nullptr, given_labels = sc->views[0].labels != nullptr;
+  if ((sch->device_edges && given_edges) || (sch->device_labels && given_labels)) return DPE_ERR_INVALID_ARGUMENT;
   const bool have_edges = given_edges || sch->device_edges;
+  const bool have_labels = given_labels || sch->device_labels;
   for (int v = 0; v < V; ++v) {
     const dpe_scene_view &sv = sc->views[v];
     if (!sv.gray || sv.num_src < 1 || sv.num_src > DPE_MAX_IMAGES - 1 || !sv.src_views) return DPE_ERR_INVALID_ARGUMENT;
     for (int j = 0; j < sv.num_src; ++j)
       if (sv.src_views[j] < 0 || sv.src_views[j] >= V || sv.src_views[j] == v) return DPE_ERR_INVALID_ARGUMENT;
-    if ((sv.edges != nullptr) != given_edges || (sv.labels != nullptr) != have_labels) return DPE_ERR_INVALID_ARGUMENT;
+    if ((sv.edges != nullptr) != given_edges || (sv.labels != nullptr) != given_labels) return DPE_ERR_INVALID_ARGUMENT;
     if (sch->fuse_mode >= 0 && !sv.bgr) return DPE_ERR_INVALID_ARGUMENT;
   }
   DPE_TRY(cudaSetDevice(ctx->device));
@@ -152,6 +154,16 @@ extern "C" int dpe_scene_run(dpe_ctx *ctx, const dpe_scene *sc, const dpe_schedu
   Arena &A = ctx->arena;
   const bool host = sc->memory == DPE_MEM_HOST;
   const size_t LF = (size_t)W * H;
+
+  // PatchMatchParams::high_res_img, which selects EdgeSegment's downsampling
+  int high_res_img = 1;
+  {
+    dpe_params d;
+    dpe_params_default(&d);
+    high_res_img = d.high_res_img ? 1 : 0;
+  }
+  if (sch->device_labels && ((W / (high_res_img ? 4 : 2)) < 1 || (H / (high_res_img ? 4 : 2)) < 1))
+    return DPE_ERR_INVALID_ARGUMENT;
 
   // level sizes (SceneCache::GetGrayFloatImage: round(cols / scale_size))
   std::vector<int> lw(L), lh(L), lscale(L);
@@ -193,7 +205,7 @@ extern "C" int dpe_scene_run(dpe_ctx *ctx, const dpe_scene *sc, const dpe_schedu
     for (int l = 0; l < L; ++l) per_view += (size_t)lw[l] * lh[l];
     uint8_t *e_dev = ((host && given_edges) || sch->device_edges) ? A.get<uint8_t>("sc_edges", per_view * V) : nullptr;
     if (sch->device_edges && dpe_edge_reserve(ctx, (size_t)lw[L - 1] * lh[L - 1]) != DPE_OK) return DPE_ERR_OUT_OF_MEMORY;
-    int32_t *l_dev = (host && have_labels) ? A.get<int32_t>("sc_labels", per_view * V) : nullptr;
+    int32_t *l_dev = ((host && given_labels) || sch->device_labels) ? A.get<int32_t>("sc_labels", per_view * V) : nullptr;
     if (!A.ok()) return DPE_ERR_OUT_OF_MEMORY;
     size_t off = 0;
     for (int v = 0; v < V; ++v)
@@ -209,7 +221,9 @@ extern "C" int dpe_scene_run(dpe_ctx *ctx, const dpe_scene *sc, const dpe_schedu
             edge[v][l] = sc->views[v].edges[l];
           }
         }
-        if (have_labels) {
+        if (sch->device_labels) {
+          label[v][l] = l_dev + off;  // made at the start of the level
+        } else if (have_labels) {
           if (host) {
             DPE_TRY(cudaMemcpyAsync(l_dev + off, sc->views[v].labels[l], n * 4, cudaMemcpyHostToDevice, s));
             label[v][l] = l_dev + off;
@@ -258,6 +272,13 @@ extern "C" int dpe_scene_run(dpe_ctx *ctx, const dpe_scene *sc, const dpe_schedu
       if (sch->device_edges) {
         const int est = dpe_edge_map_device(ctx, st[v].img, nullptr, w, h, const_cast<uint8_t *>(edge[v][l]));
         if (est != DPE_OK) return est;
+      }
+      // and its label map, from the full-resolution 8-bit image (main.cpp:199-214)
+      if (sch->device_labels) {
+        const uint8_t *g8 = host ? gray_dev + LF * v : sc->views[v].gray;
+        const int lst = dpe_edge_labels_device(ctx, g8, W, H, L - 1 - l, high_res_img, const_cast<int32_t *>(label[v][l]),
+                                               w, h);
+        if (lst != DPE_OK) return lst;
       }
     }
     // state from the previous level, rescaled (DPE::InuputInitialization, DPE.cpp:1019-1052)
@@ -430,6 +451,10 @@ extern "C" int dpe_scene_run(dpe_ctx *ctx, const dpe_scene *sc, const dpe_schedu
   if (sch->device_edges) {
     const int est = dpe_edge_check(ctx);
     if (est != DPE_OK) return est;
+  }
+  if (sch->device_labels) {
+    const int lst = dpe_edge_labels_check(ctx);
+    if (lst != DPE_OK) return lst;
   }
   float ms = 0.f;
   DPE_TRY(cudaEventElapsedTime(&ms, e0, e1));

@@ -88,7 +88,7 @@ class SceneView(C.Structure):
 class Schedule(C.Structure):
     _fields_ = [("num_levels", C.c_int), ("refine_calls", C.c_int), ("max_iterations", C.c_int),
                 ("fuse_mode", C.c_int), ("min_consistent", C.c_int), ("seed", C.c_uint64), ("batch_views", C.c_int),
-                ("device_edges", C.c_int)]
+                ("device_edges", C.c_int), ("device_labels", C.c_int)]
 
 
 class KernelStat(C.Structure):
@@ -118,7 +118,7 @@ class Limits(C.Structure):
 EXPORTED = ["dpe_status_string", "dpe_last_error", "dpe_params_default", "dpe_ctx_create", "dpe_ctx_destroy", "dpe_pm_run",
             "dpe_fuse", "dpe_ncc_eval", "dpe_ctx_set_eval_counting", "dpe_scene_run", "dpe_ctx_set_profiling",
             "dpe_ctx_reset_kernel_stats", "dpe_ctx_get_kernel_stats", "dpe_launch_count", "dpe_fp32_peak",
-            "dpe_ncc_eval_noalloc", "dpe_ncc_grad", "dpe_ctx_set_options", "dpe_pm_run_batch", "dpe_fuse_tat", "dpe_edge_map"]
+            "dpe_ncc_eval_noalloc", "dpe_ncc_grad", "dpe_ctx_set_options", "dpe_pm_run_batch", "dpe_fuse_tat", "dpe_edge_map", "dpe_edge_labels"]
 
 _lib = None
 
@@ -143,6 +143,7 @@ def load_library(path: Optional[str] = None) -> C.CDLL:
     lib.dpe_fuse.argtypes = [C.c_void_p, C.POINTER(FusionIn), C.POINTER(FusionOut)]
     lib.dpe_fuse_tat.argtypes = [C.c_void_p, C.POINTER(FusionIn), C.c_int, C.POINTER(FusionOut)]
     lib.dpe_edge_map.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p]
+    lib.dpe_edge_labels.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p]
     lib.dpe_ncc_eval.argtypes = [C.c_void_p, C.POINTER(NCCQuery), C.c_void_p]
     lib.dpe_ctx_set_eval_counting.argtypes = [C.c_void_p, C.c_int]
     lib.dpe_scene_run.argtypes = [C.c_void_p, C.POINTER(SceneIn), C.POINTER(Schedule), C.POINTER(SceneOut)]
@@ -402,14 +403,36 @@ class Context:
             raise DPEError(st, "dpe_edge_map")
         return out
 
+    def edge_labels(self, gray, scale: int, high_res_img: bool = True, memory: int = MEM_HOST):
+        """EdgeSegment's label map (mode 1) of a full-resolution 8-bit image through dpe_edge_labels:
+        int32 labels at the level size of `scale` (0 edges, -1 small regions), as numpy
+        (memory=MEM_HOST) or as a CUDA tensor (MEM_DEVICE)."""
+        H, W = gray.shape[:2]
+        f = np.float32(1.0) / np.float32(1 << scale)
+        w, h = int(np.round(np.float32(W) * f)), int(np.round(np.float32(H) * f))
+        if memory == MEM_HOST:
+            img = np.ascontiguousarray(gray, dtype=np.uint8)
+            out = np.zeros((h, w), np.int32)
+        else:
+            import torch
+
+            img = gray.contiguous()
+            out = torch.empty((h, w), dtype=torch.int32, device=gray.device)
+        st = self.lib.dpe_edge_labels(self.handle, _ptr(img), W, H, scale, 1 if high_res_img else 0, memory, _ptr(out))
+        if st != OK:
+            raise DPEError(st, "dpe_edge_labels")
+        return out
+
     # ------------------------------------------------------------------ whole scene
     def scene_run(self, gray, bgr, cameras, srcs, edges=None, labels=None, *, num_levels=0, refine_calls=3,
                   max_iterations=3, fuse_mode=FUSE_FP64, min_consistent=1, seed=1, memory=MEM_HOST,
-                  want_maps=True, point_capacity=None, batch_views=False, device_edges=False) -> Dict:
+                  want_maps=True, point_capacity=None, batch_views=False, device_edges=False,
+                  device_labels=False) -> Dict:
         """The reference's full schedule over all views (dpe_scene_run).  gray[v]: (H, W) uint8,
         bgr[v]: (H, W, 3) uint8, cameras[v]: full-resolution camera dicts, srcs[v]: source view
         indices, edges[v][level] / labels[v][level]: per-level maps (level 0 = coarsest).
-        device_edges=True: the edge maps are made on the device (edges must be None)."""
+        device_edges=True / device_labels=True: the edge / label maps are made on the device (edges /
+        labels must then be None)."""
         V = len(gray)
         H, W = int(gray[0].shape[0]), int(gray[0].shape[1])
         arr = (SceneView * V)()
@@ -433,7 +456,8 @@ class Context:
                 sv.labels = C.cast(la, C.POINTER(C.c_void_p))
         sc = SceneIn(V, W, H, arr, memory)
         sch = Schedule(num_levels, refine_calls, max_iterations, fuse_mode if fuse_mode is not None else -1,
-                       min_consistent, seed, 1 if batch_views else 0, 1 if device_edges else 0)
+                       min_consistent, seed, 1 if batch_views else 0, 1 if device_edges else 0,
+                       1 if device_labels else 0)
         so = SceneOut()
         so.out_memory = MEM_HOST
         res = {}

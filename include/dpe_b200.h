@@ -193,6 +193,9 @@ typedef struct dpe_schedule {
   int device_edges;     /* 1: each level's edge map is made on the device from the level image
                            (GetProblemEdges' EdgeSegment mode 0, main.cpp:170-197; dpe_edge_map);
                            views[].edges must then be NULL                                       */
+  int device_labels;    /* 1: each level's label map is made on the device from the full-resolution
+                           image (GetProblemEdges' EdgeSegment mode 1, main.cpp:199-214;
+                           dpe_edge_labels); views[].labels must then be NULL                      */
 } dpe_schedule;
 
 typedef struct dpe_scene {
@@ -299,6 +302,21 @@ int dpe_fuse_tat(dpe_ctx *ctx, const dpe_fusion_in *in, int variant, dpe_fusion_
  * writes the result to edges_<scale>.dmb; dpe_scene_run can make these maps itself
  * (dpe_schedule.device_edges). */
 int dpe_edge_map(dpe_ctx *ctx, const uint8_t *image, int width, int height, int memory, uint8_t *edge_out);
+
+/* The label map of EdgeSegment (DPE.cpp:136-291) as GetProblemEdges requests it for a pyramid level
+ * (EdgeSegment(scale, image_uint, 1, false, high_res_img), main.cpp:199-214): from the
+ * full-resolution 8-bit image `gray` (width*height), halved when high_res_img and halved again, a
+ * Roberts gradient thresholded at 4 (6 without high_res_img), the reference's region labelling
+ * Connect, Hough segments drawn across the outer border of every weak region of at least
+ * width*height / (1024 << 2*scale) pixels, the map resized to the level, thresholded,
+ * border-ruled and labelled again.  `labels_out` receives round(width / 2^scale) *
+ * round(height / 2^scale) int32 labels: 0 on edges, -1 on regions of at most that many pixels,
+ * otherwise the region number.  The resize, Hough transform and line drawing are OpenCV's
+ * (cv::resize INTER_LINEAR, cv::HoughLinesP, cv::line) in their integer forms, bit for bit.  The
+ * reference writes the result to labels_<scale>.dmb; dpe_scene_run can make these maps itself
+ * (dpe_schedule.device_labels). */
+int dpe_edge_labels(dpe_ctx *ctx, const uint8_t *gray, int width, int height, int scale, int high_res_img, int memory,
+                    int32_t *labels_out);
 
 /* Replaces main()'s PatchMatch schedule and fusion (main.cpp:385-461) for a whole scene, with every
  * view's state kept in device memory between calls: per level the float image pyramid
