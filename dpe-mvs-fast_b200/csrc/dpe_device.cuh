@@ -188,14 +188,32 @@ __device__ __forceinline__ float texel(const PMArgs &a, int im, int x, int y) {
   y = min(max(y, 0), a.H - 1);
   return img_ld(a.img[im], (long long)(y + 1) * a.pad_w + (x + 1), (long long)a.pad_w * (a.H + 2), 101);
 }
+// floor(x) as a float and as an int, for -1 <= x < 2^22 (a clamped sample coordinate).  On the
+// device, x + 1.5 * 2^23 rounded toward -inf is exactly 1.5 * 2^23 + floor(x): the sum lies in
+// [2^23, 2^24), where float spacing is 1.  So the floor is one FADD with a rounding mode on the FMA
+// pipe, and the int is an integer subtract, instead of a round and a float-to-int conversion on the
+// conversion pipe (16 per clock per SM, the bound of the tap loops).  Same value as floorf.
+__device__ __forceinline__ float floor_split(float x, int *ix) {
+#ifdef __CUDA_ARCH__
+  const float f = __fadd_rd(x, 12582912.0f);
+  *ix = __float_as_int(f) - 0x4B400000;
+  return f - 12582912.0f;
+#else
+  const float f = floorf(x);
+  *ix = (int)f;
+  return f;
+#endif
+}
+
 // tex2D(x+0.5, y+0.5) with linear filtering and clamp-to-edge addressing, exact FP32 weights.
 // The padded border makes the four reads branch-free for x0 in [-1, W-1].
 __device__ __forceinline__ float bilinear(const float *__restrict__ img, int pad_w, int W, int H, float x, float y) {
   const float xc = fminf(fmaxf(x, -1.0f), (float)(W - 1));
   const float yc = fminf(fmaxf(y, -1.0f), (float)(H - 1));
-  const float fx = floorf(xc), fy = floorf(yc);
+  int ix, iy;
+  const float fx = floor_split(xc, &ix), fy = floor_split(yc, &iy);
   const float ax = xc - fx, ay = yc - fy;
-  const long long o = (long long)((int)fy + 1) * pad_w + ((int)fx + 1);
+  const long long o = (long long)(iy + 1) * pad_w + (ix + 1);
   const long long n = (long long)pad_w * (H + 2);
   const float v00 = img_ld(img, o, n, 102), v10 = img_ld(img, o + 1, n, 103);
   const float v01 = img_ld(img, o + pad_w, n, 104), v11 = img_ld(img, o + pad_w + 1, n, 105);
@@ -253,9 +271,10 @@ template <class Src, bool kClamp = true>
 __device__ __forceinline__ float bilinear_s(const Src &src, int W, int H, float x, float y) {
   const float xc = kClamp ? fminf(fmaxf(x, -1.0f), (float)(W - 1)) : x;
   const float yc = kClamp ? fminf(fmaxf(y, -1.0f), (float)(H - 1)) : y;
-  const float fx = floorf(xc), fy = floorf(yc);
+  int ix, iy;
+  const float fx = floor_split(xc, &ix), fy = floor_split(yc, &iy);
   const float ax = xc - fx, ay = yc - fy;
-  const float4 v = src.fetch(((int)fy + 1) * src.pw + ((int)fx + 1));
+  const float4 v = src.fetch((iy + 1) * src.pw + (ix + 1));
   const float top = (1.0f - ax) * v.x + ax * v.y;
   const float bot = (1.0f - ax) * v.z + ax * v.w;
   return (1.0f - ay) * top + ay * bot;
@@ -391,6 +410,21 @@ __device__ __forceinline__ float2 project(const float H[9], int x, int y) {
   const float Z = H[6] * fx + H[7] * fy + H[8];
   return make_float2(X / Z, Y / Z);
 }
+// project() at a tap of a deformable window, float coordinates.  The fast device build divides by
+// the hardware reciprocal (as the strong window's taps do); the exact build and host builds keep
+// the IEEE quotients X / Z and Y / Z.
+__device__ __forceinline__ float tap_rcp(float z);
+__device__ __forceinline__ float2 project_tap(const float H[9], float fx, float fy) {
+  const float X = H[0] * fx + H[1] * fy + H[2];
+  const float Y = H[3] * fx + H[4] * fy + H[5];
+  const float Z = H[6] * fx + H[7] * fy + H[8];
+#if defined(__CUDA_ARCH__) && !defined(DPE_EXACT)
+  const float iz = tap_rcp(Z);
+  return make_float2(X * iz, Y * iz);
+#else
+  return make_float2(X / Z, Y / Z);
+#endif
+}
 
 __device__ __forceinline__ float bilateral_weight(float dx, float dy, float pix, float center, float ss, float sc) {
   const float spatial = sqrtf(dx * dx + dy * dy);
@@ -475,22 +509,27 @@ template <bool kClamp, class Src, int kUnroll>
 __device__ __forceinline__ void strong_window(const PMArgs &a, int px, int py, const float H[9], const Src &src,
                                               const RefWindow &rw, float &s_s, float &s_ss, float &s_rs) {
   const int r = a.P.strong_radius, inc = a.P.strong_increment;
+  // Tap coordinates are whole numbers far below 2^24, so stepping them by float adds gives the
+  // same floats as converting each integer, without a conversion per tap.
   if (kUnroll > 0 && r == 5 && inc == 2) {
+    const float x0 = (float)(px - 5), y0 = (float)(py - 5);
     for (int ii = 0; ii < 6; ++ii) {
-      const float x = (float)(px - 5 + 2 * ii);
+      const float x = x0 + (float)(2 * ii);
       const float bx = H[0] * x + H[2], by = H[3] * x + H[5], bz = H[6] * x + H[8];
 #pragma unroll(kUnroll > 0 ? kUnroll : 1)
       for (int jj = 0; jj < 6; ++jj)
-        strong_tap<kClamp>(a, H, src, rw, bx, by, bz, (float)(py - 5 + 2 * jj), 6 * ii + jj, s_s, s_ss, s_rs);
+        strong_tap<kClamp>(a, H, src, rw, bx, by, bz, y0 + (float)(2 * jj), 6 * ii + jj, s_s, s_ss, s_rs);
     }
   } else {
     int k = 0;
-    for (int i = -r; i <= r; i += inc) {
-      const float x = (float)(px + i);
+    const float finc = (float)inc, y0 = (float)(py - r);
+    float x = (float)(px - r);
+    for (int i = -r; i <= r; i += inc, x += finc) {
       // column x is fixed while y walks the window: the projective numerators are affine in y
       const float bx = H[0] * x + H[2], by = H[3] * x + H[5], bz = H[6] * x + H[8];
-      for (int j = -r; j <= r; j += inc)
-        strong_tap<kClamp>(a, H, src, rw, bx, by, bz, (float)(py + j), k++, s_s, s_ss, s_rs);
+      float y = y0;
+      for (int j = -r; j <= r; j += inc, y += finc)
+        strong_tap<kClamp>(a, H, src, rw, bx, by, bz, y, k++, s_s, s_ss, s_rs);
     }
   }
 }
@@ -683,10 +722,14 @@ __device__ __forceinline__ float window_ncc_tab(const PMArgs &a, const float H[9
                                                 float4 win) {
   float s_s = 0, s_ss = 0, s_rs = 0;
   int t = 0;
-  for (int i = -radius; i <= radius; i += inc) {
+  // whole-number tap coordinates stepped by exact float adds (no conversion per tap)
+  const float finc = (float)inc, y0 = (float)(cy - radius);
+  float x = (float)(cx - radius);
+  for (int i = -radius; i <= radius; i += inc, x += finc) {
     float r_s = 0, r_ss = 0, r_rs = 0;
-    for (int j = -radius; j <= radius; j += inc) {
-      const float2 sp = project(H, cx + i, cy + j);
+    float y = y0;
+    for (int j = -radius; j <= radius; j += inc, y += finc) {
+      const float2 sp = project_tap(H, x, y);
       const float sv = bilinear_s(src, a.W, a.H, sp.x, sp.y) - ref_center;
       const float2 e = tab[t++];
       r_s += e.x * sv; r_ss += e.x * sv * sv; r_rs += e.y * sv;
