@@ -200,6 +200,8 @@ dim3 full_grid(int W, int H) { return dim3((W + 15) / 16, (H + 7) / 8); }
 const dim3 kFullBlock(16, 8);
 dim3 half_grid(int W, int H) { return dim3((W + 31) / 32, ((H + 1) / 2 + 3) / 4); }
 const dim3 kHalfBlock(32, 4);
+// the cooperative strong update: 16 pixels of one colour per block (kCoopPix), one half-grid row
+dim3 coop_grid(int W, int H) { return dim3((W + kCoopPix - 1) / kCoopPix, (H + 1) / 2); }
 
 // Blocks of 128 threads for a strided work list of up to `items` entries: enough to fill every
 // multiprocessor, no more than the list needs.
@@ -217,10 +219,11 @@ template <class F> void with_stage(int staging, F &&f) {
   else f(std::integral_constant<int, DPE_STAGE_FP32>{});
 }
 
-void launch_strong_update(int staging, bool gn, dim3 grid, cudaStream_t s, const Launch args, int it, int parity) {
+void launch_strong_update(int staging, bool gn, dim3 grid, size_t smem, cudaStream_t s, const Launch args, int it,
+                          int parity) {
   with_stage(staging, [&](auto st) {
-    if (gn) k_strong_update<decltype(st)::value, true><<<grid, kHalfBlock, 0, s>>>(args, it, parity);
-    else k_strong_update<decltype(st)::value, false><<<grid, kHalfBlock, 0, s>>>(args, it, parity);
+    if (gn) k_strong_update<decltype(st)::value, true><<<grid, kCoopThreads, smem, s>>>(args, it, parity);
+    else k_strong_update<decltype(st)::value, false><<<grid, kCoopThreads, smem, s>>>(args, it, parity);
   });
 }
 
@@ -407,8 +410,9 @@ int setup_problem(dpe_ctx *ctx, const dpe_problem *p, int index, ProblemState *p
 // Grids of one kernel sequence: for one problem the 2D pixel grids; for a batch one 1D grid per
 // kind over all problems, with the prefix tables the kernels resolve their problem from.
 struct SequenceGrids {
-  Launch full, half, prep, eval;
-  dim3 fg, hg;
+  Launch full, half, prep, eval, coop;
+  dim3 fg, hg, cg;
+  size_t coop_smem = 0;  // dynamic shared bytes of the strong update (largest source count)
   unsigned gp = 0, ge = 0;
   const dim3 fb = kFullBlock, hb = kHalfBlock;
 };
@@ -475,7 +479,7 @@ int run_sequence(dpe_ctx *ctx, ProblemState *ps, int n, const PMArgs *d_args, co
           DPE_TRY(cudaMemcpyAsync(a.plane_snap, a.plane, ps[b].L * sizeof(float4), cudaMemcpyDeviceToDevice, s));
           DPE_TRY(cudaMemcpyAsync(a.cost_snap, a.cost, ps[b].L * 4, cudaMemcpyDeviceToDevice, s));
         }
-      DPE_TIMED(ctx, KID_STRONG_UPDATE, s, launch_strong_update(staging, gn, g.hg, s, g.half, it, parity));
+      DPE_TIMED(ctx, KID_STRONG_UPDATE, s, launch_strong_update(staging, gn, g.cg, g.coop_smem, s, g.coop, it, parity));
       PM_LAUNCHED("k_strong_update", s);
     }
     DPE_TIMED(ctx, KID_RANSAC, s, k_ransac_fit_plane<<<g.fg, g.fb, 0, s>>>(g.full));
@@ -527,7 +531,7 @@ int pm_run_problems(dpe_ctx *ctx, const dpe_problem *const *problems, int n, dpe
   std::vector<ProblemState> ps(n);
   unsigned long long *counters = A.get<unsigned long long>("counters", 2 * KID_COUNT);
   PMArgs *d_args = A.get<PMArgs>("pm_args", n);
-  int *d_start = n > 1 ? A.get<int>("batch_start", 4 * (n + 1)) : nullptr;
+  int *d_start = n > 1 ? A.get<int>("batch_start", 5 * (n + 1)) : nullptr;
   if (!counters || !d_args || (n > 1 && !d_start)) return DPE_ERR_OUT_OF_MEMORY;
   if (ctx->count_evals) DPE_TRY(cudaMemsetAsync(counters, 0, 16 * KID_COUNT, s));
   for (int b = 0; b < n; ++b) {
@@ -561,17 +565,21 @@ int pm_run_problems(dpe_ctx *ctx, const dpe_problem *const *problems, int n, dpe
   if (n == 1) {
     const PMArgs &a = ps[0].a;
     const Launch one{d_args, nullptr, 1};
-    g.full = g.half = g.prep = g.eval = one;
+    g.full = g.half = g.prep = g.eval = g.coop = one;
     g.fg = full_grid(a.W, a.H);
     g.hg = half_grid(a.W, a.H);
+    g.cg = coop_grid(a.W, a.H);
+    g.coop_smem = coop_smem_bytes(a.N - 1);
     g.gp = list_grid(ctx, (long long)ps[0].wcap);
     g.ge = list_grid(ctx, (long long)ps[0].wcap * 10 * (a.N - 1));
   } else {
     // the problems' grids laid end to end: prefix tables per grid kind
-    std::vector<int> start(4 * (n + 1), 0);
+    std::vector<int> start(5 * (n + 1), 0);
     for (int b = 0; b < n; ++b) {
       const PMArgs &a = ps[b].a;
-      const dim3 f = full_grid(a.W, a.H), h = half_grid(a.W, a.H);
+      const dim3 f = full_grid(a.W, a.H), h = half_grid(a.W, a.H), cg = coop_grid(a.W, a.H);
+      start[4 * (n + 1) + b + 1] = start[4 * (n + 1) + b] + (int)(cg.x * cg.y);
+      g.coop_smem = std::max(g.coop_smem, coop_smem_bytes(a.N - 1));
       start[0 * (n + 1) + b + 1] = start[0 * (n + 1) + b] + (int)(f.x * f.y);
       start[1 * (n + 1) + b + 1] = start[1 * (n + 1) + b] + (int)(h.x * h.y);
       start[2 * (n + 1) + b + 1] = start[2 * (n + 1) + b] + (int)list_grid(ctx, (long long)ps[b].wcap);
@@ -583,6 +591,8 @@ int pm_run_problems(dpe_ctx *ctx, const dpe_problem *const *problems, int n, dpe
     g.half = Launch{d_args, d_start + 1 * (n + 1), n};
     g.prep = Launch{d_args, d_start + 2 * (n + 1), n};
     g.eval = Launch{d_args, d_start + 3 * (n + 1), n};
+    g.coop = Launch{d_args, d_start + 4 * (n + 1), n};
+    g.cg = dim3(start[4 * (n + 1) + n]);
     g.fg = dim3(start[0 * (n + 1) + n]);
     g.hg = dim3(start[1 * (n + 1) + n]);
     g.gp = (unsigned)start[2 * (n + 1) + n];

@@ -452,6 +452,17 @@ struct RefWindow {
   __device__ __forceinline__ float wr(int k) const { return tap(k).y; }
 };
 #define DPE_REF_WINDOW(rw) ::dpe::RefWindow rw
+// The same window held once per pixel in shared memory, read by every thread that evaluates a
+// hypothesis of that pixel (the cooperative strong update).  The threads of one pixel read the
+// same tap together, so a warp's read is one broadcast per pixel.
+struct SmemWindow {
+  const float2 *t_;
+  float center, inv_wsum, mean_r, var_r;
+  unsigned long long *cnt;
+  __device__ __forceinline__ float2 tap(int k) const { return t_[k]; }
+  __device__ __forceinline__ float w(int k) const { return t_[k].x; }
+  __device__ __forceinline__ float wr(int k) const { return t_[k].y; }
+};
 
 __device__ __forceinline__ void build_ref_window(const PMArgs &a, int px, int py, RefWindow &rw, int kid) {
   rw.cnt = a.counters ? a.counters + 2 * kid : nullptr;
@@ -490,8 +501,8 @@ __device__ __forceinline__ float tap_rcp(float z) {
 }
 // One tap of the strong window: sample the source at the projected tap and accumulate the
 // hypothesis-dependent moments (sums of w*s, w*s^2, w*(r-c)*s over s = sample - c).
-template <bool kClamp, class Src>
-__device__ __forceinline__ void strong_tap(const PMArgs &a, const float H[9], const Src &src, const RefWindow &rw,
+template <bool kClamp, class Src, class RW>
+__device__ __forceinline__ void strong_tap(const PMArgs &a, const float H[9], const Src &src, const RW &rw,
                                            float bx, float by, float bz, float y, int k, float &s_s, float &s_ss,
                                            float &s_rs) {
   const float X = H[1] * y + bx, Y = H[4] * y + by, Z = H[7] * y + bz;
@@ -505,9 +516,9 @@ __device__ __forceinline__ void strong_tap(const PMArgs &a, const float H[9], co
 }
 // ComputeBilateralNCCOld (DPE.cu:696-782) with the reference window precomputed; the window loop
 // for one source sampler.
-template <bool kClamp, class Src, int kUnroll>
+template <bool kClamp, class Src, int kUnroll, class RW>
 __device__ __forceinline__ void strong_window(const PMArgs &a, int px, int py, const float H[9], const Src &src,
-                                              const RefWindow &rw, float &s_s, float &s_ss, float &s_rs) {
+                                              const RW &rw, float &s_s, float &s_ss, float &s_rs) {
   const int r = a.P.strong_radius, inc = a.P.strong_increment;
   // Tap coordinates are whole numbers far below 2^24, so stepping them by float adds gives the
   // same floats as converting each integer, without a conversion per tap.
@@ -533,9 +544,9 @@ __device__ __forceinline__ void strong_window(const PMArgs &a, int px, int py, c
     }
   }
 }
-template <class Src, int kUnroll>
+template <class Src, int kUnroll, class RW>
 __device__ __forceinline__ float ncc_strong_src(const PMArgs &a, int px, int py, const float H[9], const Src &src,
-                                                const RefWindow &rw) {
+                                                const RW &rw) {
   float s_s = 0.f, s_ss = 0.f, s_rs = 0.f;
   // (a clamp-free copy of the loop for windows that project inside the source measured slower:
   // the second copy costs registers under the strong update's occupancy bound)
@@ -546,15 +557,15 @@ __device__ __forceinline__ float ncc_strong_src(const PMArgs &a, int px, int py,
   const float cov = s_rs * rw.inv_wsum - rw.mean_r * m_s;
   return fmaxf(0.0f, fminf(2.0f, 1.0f - cov / sqrtf(rw.var_r * var_s)));
 }
-template <int kStage = DPE_STAGE_FP32, int kUnroll = 0>
-__device__ __forceinline__ float ncc_strong(const PMArgs &a, int px, int py, int s, float4 pl, const RefWindow &rw) {
+template <int kStage = DPE_STAGE_FP32, int kUnroll = 0, class RW>
+__device__ __forceinline__ float ncc_strong(const PMArgs &a, int px, int py, int s, float4 pl, const RW &rw) {
   float H[9];
   homography(a, s, pl, H);
   const float2 pt = project(H, px, py);
   const dpe_camera &sc = a.cam[s];
   if (pt.x >= sc.width || pt.x < 0.0f || pt.y >= sc.height || pt.y < 0.0f) return 2.0f;
   if (rw.cnt) atomicAdd(rw.cnt, 1ull);
-  return ncc_strong_src<decltype(SrcOf<kStage>::make(a, s)), kUnroll>(a, px, py, H, SrcOf<kStage>::make(a, s), rw);
+  return ncc_strong_src<decltype(SrcOf<kStage>::make(a, s)), kUnroll, RW>(a, px, py, H, SrcOf<kStage>::make(a, s), rw);
 }
 
 // ------------------------------------------------------------------ strong NCC adjoint
@@ -566,8 +577,9 @@ __device__ __forceinline__ float ncc_strong(const PMArgs &a, int px, int py, int
 //           the projected point, through the projection to the homography entries.
 // dC/dH then goes through H = K_s (R - t n^T / w) K_r^-1 to the plane.  Where the cost is the
 // constant 2 (centre outside the source, flat window) or clamped to [0, 2], the gradient is zero.
+template <class RW>
 __device__ __forceinline__ float ncc_strong_adjoint(const PMArgs &a, int px, int py, int s, float4 pl,
-                                                    const RefWindow &rw, float g[4], float *gimg) {
+                                                    const RW &rw, float g[4], float *gimg) {
   g[0] = g[1] = g[2] = g[3] = 0.0f;
   float H[9];
   homography(a, s, pl, H);
@@ -674,14 +686,14 @@ __device__ __forceinline__ float ncc_strong_adjoint(const PMArgs &a, int px, int
 }
 
 // Strong costs of plane pl against every source: out[j] = cost against source j + 1.
-template <int kStage, int kUnroll = 0>
-__device__ __forceinline__ void ncc_all_sources(const PMArgs &a, int px, int py, float4 pl, const RefWindow &rw,
+template <int kStage, int kUnroll = 0, class RW>
+__device__ __forceinline__ void ncc_all_sources(const PMArgs &a, int px, int py, float4 pl, const RW &rw,
                                                 float *out) {
   for (int j = 0; j < a.N - 1; ++j) out[j] = ncc_strong<kStage, kUnroll>(a, px, py, j + 1, pl, rw);
 }
 // Sum over the listed sources act[0..na) (ascending) of vw[j] * cost(j), in list order.
-template <int kStage>
-__device__ __forceinline__ float weighted_ncc(const PMArgs &a, int px, int py, float4 pl, const RefWindow &rw,
+template <int kStage, class RW>
+__device__ __forceinline__ float weighted_ncc(const PMArgs &a, int px, int py, float4 pl, const RW &rw,
                                              const int *act, int na, const uint8_t *vw) {
   float tc = 0.0f;
   for (int q = 0; q < na; ++q) tc += vw[act[q]] * ncc_strong<kStage>(a, px, py, act[q] + 1, pl, rw);

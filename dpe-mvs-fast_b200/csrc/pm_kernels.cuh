@@ -632,8 +632,8 @@ __device__ __forceinline__ int find_min_cost_index(const float *c, int n) {
 // equations  (J^T V J + lambda diag(J^T V J)) theta = -J^T V c  (V = the sample counts).  The
 // resulting plane is a hypothesis like the random ones: kept only when its cost is lower and its
 // depth lies in range.  It draws no random numbers, so the rest of the update is unchanged.
-template <int kStage>
-__device__ __forceinline__ void gn_hypothesis(const PMArgs &a, int px, int py, const RefWindow &rw, const int *act,
+template <int kStage, class RW>
+__device__ __forceinline__ void gn_hypothesis(const PMArgs &a, int px, int py, const RW &rw, const int *act,
                                               int na, const uint8_t *vw, float wn, float4 *pl_now, float *depth_now,
                                               float *cost_now) {
   const dpe_camera &rc = a.cam[0];
@@ -688,248 +688,400 @@ __device__ __forceinline__ void gn_hypothesis(const PMArgs &a, int px, int py, c
 }
 
 // ------------------------------------------------------------------ strong update (DPE.cu:1218-1670, 1069-1122)
-template <int kStage, bool kGN>
-__global__ void __launch_bounds__(128, DPE_STRONG_MIN_BLOCKS) k_strong_update(const Launch lc, int iter, int parity) {
-  const Blk B = resolve<kGridHalf>(lc);
-  const PMArgs &a = *B.a;
-  int px, py;
-  if (!colour_pixel(a, B, parity, &px, &py)) return;
-  const int W = a.W, H = a.H, n = a.N - 1;
-  const int center = py * W + px;
-  const long long L = (long long)W * H;
-  if (G(a.weak, center, L, 201) == DPE_WEAK) return;
-  const dpe_camera &rc = a.cam[0];
-  DPE_REF_WINDOW(rw);
-  build_ref_window(a, px, py, rw, KID_STRONG_UPDATE);
-  float cost_array[8][kMaxSrc];
-  for (int d = 0; d < 8; ++d)
-    for (int j = 0; j < n; ++j) cost_array[d][j] = 0.0f;
-  cost_array[0][0] = 2.0f;  // `= {2.0f}` initialises only the first element (quirk Q2)
-  bool flag[8] = {false, false, false, false, false, false, false, false};
-  int positions[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  const float4 *cand_plane = a.P.use_edge ? a.plane_snap : a.plane;
-  const float *cand_cost = a.P.use_edge ? a.cost_snap : a.cost;
+// Block-cooperative: a block holds kCoopPix pixels of one colour (consecutive x on one row of the
+// half grid) and kCoopLanes threads per pixel.  The pixel's reference window and its candidate
+// cost matrix live once in shared memory; the threads of a pixel evaluate its hypotheses side by
+// side (lane d: candidate d; then the sampled sources of the current plane and of the five
+// refinement planes), and one thread per pixel takes every decision in the reference's order, so
+// the random draws and the order of each weighted sum are those of one thread doing it all.
+//
+// Phases, separated by block barriers:
+//   0  window taps (lanes split the taps)           4  current plane's costs (lanes split sources)
+//   1  window sums (lane 0); candidate search       5  candidate acceptance, refinement planes (lane 0)
+//   2  candidate costs (lane d: candidate d)        6  refinement costs (lanes split plane x source)
+//   3  view sampling, best candidate (lane 0)       7  refinement decisions, outputs (lane 0)
+constexpr int kCoopPix = 16, kCoopLanes = 8, kCoopThreads = kCoopPix * kCoopLanes;
 
-  if (a.P.use_edge) {
-    const short2 *en = &G(a.edge_neigh, (long long)center * 8, L * 8, 202);
-    const float max_edge_dist = cvmax(H, W) / 30.0f;
-    const int min_step = 2;
-    const bool on_edge = G(a.edge, center, L, 203) != 0;
-    for (int d = 0; d < 8; ++d) {
-      const int dx = kDir[d][0], dy = kDir[d][1];
-      const int sx = cvmax(1, 5 - 2 * iter) * dx, sy = cvmax(1, 5 - 2 * iter) * dy;
-      const short2 e = en[d];
-      const double ex = (double)(e.x - px), ey = (double)(e.y - py);
-      float dist = (float)sqrt(ex * ex + ey * ey);
-      if (d >= 4) dist = (float)(dist / sqrt(2.0));
-      if (on_edge) dist = 11 * min_step;
-      else if (e.x == -1 || e.y == -1 || dist > max_edge_dist) {
-        dist = max_edge_dist;
-        if (d >= 4) dist = (float)(dist / sqrt(2.0));
+// Decision state of one pixel, in shared memory.
+struct CoopPixel {
+  float2 win[kWinTaps];  // (w, w * (r - c)) per tap
+  float rc[kWinTaps];    // r - c per tap
+  float4 pl_cur, pl_now, hyp[5];
+  float center, inv_wsum, mean_r, var_r;
+  float wn, cost_now, cost_written, depth_now, fcost_mi;
+  int pos[8];
+  int act[kMaxSrc];
+  int na, mi;
+  uint32_t views_new, temp_sel, rng_ctr;
+  uint8_t flag[8];
+  uint8_t vw[32];
+};
+// Shared bytes of one block: the pixels' states, then per pixel 8 candidate cost rows and 6
+// hypothesis cost rows of n = N - 1 floats.
+__host__ __device__ inline size_t coop_smem_bytes(int n) {
+  return sizeof(CoopPixel) * kCoopPix + sizeof(float) * (size_t)kCoopPix * 14 * n;
+}
+
+struct CoopCtx {
+  const PMArgs *a;
+  int slot, lane, px, py, center, n;
+  bool live;  // a pixel of this colour inside the image, not WEAK
+  CoopPixel *P;
+  float *cost;  // 8 rows of n
+  float *hc;    // 6 rows of n: the current plane, then the five refinement planes
+  __device__ __forceinline__ SmemWindow window() const {
+    return SmemWindow{P->win, P->center, P->inv_wsum, P->mean_r, P->var_r,
+                      a->counters ? a->counters + 2 * KID_STRONG_UPDATE : nullptr};
+  }
+};
+
+__device__ __forceinline__ CoopCtx coop_ctx(const Launch &lc, int parity, void *smem) {
+  const Blk B = resolve<kGridFull>(lc);  // kGridFull's block-row width, (W + 15) / 16, is ours too
+  const PMArgs &a = *B.a;
+  CoopCtx c;
+  c.a = B.a;
+  c.slot = (int)threadIdx.x / kCoopLanes;
+  c.lane = (int)threadIdx.x % kCoopLanes;
+  c.n = a.N - 1;
+  c.px = B.x * kCoopPix + c.slot;
+  c.py = 2 * B.y + ((c.px + parity) & 1);
+  c.center = c.py * a.W + c.px;
+  c.live = c.px < a.W && c.py < a.H;
+  if (c.live) c.live = G(a.weak, c.center, (long long)a.W * a.H, 201) != DPE_WEAK;
+  CoopPixel *base = static_cast<CoopPixel *>(smem);
+  c.P = base + c.slot;
+  float *rows = reinterpret_cast<float *>(base + kCoopPix);
+  c.cost = rows + (size_t)c.slot * 8 * c.n;
+  c.hc = rows + (size_t)kCoopPix * 8 * c.n + (size_t)c.slot * 6 * c.n;
+  return c;
+}
+
+// Phase 0: the window taps of build_ref_window, split over the lanes.
+__device__ __forceinline__ void strong_p0(const CoopCtx &c) {
+  if (!c.live) return;
+  const PMArgs &a = *c.a;
+  const int r = a.P.strong_radius, inc = a.P.strong_increment, side = 2 * r / inc + 1;
+  const float center = texel(a, 0, c.px, c.py);
+  for (int k = c.lane; k < side * side; k += kCoopLanes) {
+    const int i = -r + (k / side) * inc, j = -r + (k % side) * inc;
+    const float rp = texel(a, 0, c.px + i, c.py + j);
+    const float w = bilateral_weight((float)i, (float)j, rp, center, a.P.sigma_spatial, a.P.sigma_color);
+    const float rc = rp - center;
+    G(c.P->win, k, kWinTaps, 320) = make_float2(w, w * rc);
+    c.P->rc[k] = rc;
+  }
+  if (c.lane == 0) c.P->center = center;
+}
+
+// Candidate search of the non-edge propagation (8 slots: 0 up_near, 1 up_far, 2 down_near,
+// 3 down_far, 4 left_near, 5 left_far, 6 right_near, 7 right_far), slot d only.
+__device__ __forceinline__ int strong_search_plain(const PMArgs &a, int px, int py, int center, int d) {
+  const int W = a.W, H = a.H;
+  [[maybe_unused]] const long long L = (long long)W * H;
+  const int f = d >> 1;
+  if (d & 1) {  // far: every second pixel from distance 3 on
+    const int starts[4] = {center - 3 * W, center + 3 * W, center - 3, center + 3};
+    const int strides[4] = {-W, W, -1, 1};
+    const bool oks[4] = {py > 2, py < H - 3, px > 2, px < W - 3};
+    if (!oks[f]) return -1;
+    float m = G(a.cost, starts[f], L, 206);
+    int mp = starts[f];
+    for (int i = 1; i < 11; ++i) {
+      bool ok;
+      switch (f) {
+        case 0: ok = py > 2 + 2 * i; break;
+        case 1: ok = py < H - 3 - 2 * i; break;
+        case 2: ok = px > 2 + 2 * i; break;
+        default: ok = px < W - 3 - 2 * i; break;
       }
-      const int step_num = cvmin(cvmax(11, (int)(1.0f * dist / min_step)), 22);
-      int step_len = cvmax((int)(1.0f * dist / step_num), min_step);
-      if (d < 4 && step_len % 2 == 1) step_len -= 1;
+      if (ok) {
+        const int t = starts[f] + 2 * i * strides[f];
+        const float ct = G(a.cost, t, L, 207);
+        if (ct < m) { m = ct; mp = t; }
+      }
+    }
+    return mp;
+  }
+  // near: base pixel one step away, then diagonal pairs at distance 1..3
+  const int nbase[4] = {center - W, center + W, center - 1, center + 1};
+  const bool nok[4] = {py > 0, py < H - 1, px > 0, px < W - 1};
+  if (!nok[f]) return -1;
+  float m = G(a.cost, nbase[f], L, 208);
+  int mp = nbase[f];
+  for (int i = 0; i < 3; ++i)
+    for (int side = 0; side < 2; ++side) {
+      bool ok;
+      int t;
+      const int k = 1 + i;
+      switch (f) {
+        case 0: t = nbase[0] - k * W + (side ? k : -k); ok = py > 1 + i && (side ? px < W - 1 - i : px > i); break;
+        case 1: t = nbase[1] + k * W + (side ? k : -k); ok = py < H - 2 - i && (side ? px < W - 1 - i : px > i); break;
+        case 2: t = nbase[2] - k + (side ? k * W : -k * W); ok = px > 1 + i && (side ? py < H - 1 - i : py > i); break;
+        default: t = nbase[3] + k + (side ? k * W : -k * W); ok = px < W - 2 - i && (side ? py < H - 1 - i : py > i); break;
+      }
+      if (ok) {
+        const float ct = G(a.cost, t, L, 209);
+        if (ct < m) { m = ct; mp = t; }
+      }
+    }
+  return mp;
+}
+
+// The edge-aware propagation's first search for direction d: steps along d up to the stored edge
+// distance (DPE.cu:1262-1301).  Returns the position or -1.
+__device__ __forceinline__ int strong_search_edge(const PMArgs &a, int px, int py, int center, int d, int iter) {
+  const int W = a.W, H = a.H;
+  [[maybe_unused]] const long long L = (long long)W * H;
+  const float *cand_cost = a.cost_snap;
+  const short2 e = G(a.edge_neigh, (long long)center * 8 + d, L * 8, 202);
+  const float max_edge_dist = cvmax(H, W) / 30.0f;
+  const int min_step = 2;
+  const bool on_edge = G(a.edge, center, L, 203) != 0;
+  const int dx = kDir[d][0], dy = kDir[d][1];
+  const int sx = cvmax(1, 5 - 2 * iter) * dx, sy = cvmax(1, 5 - 2 * iter) * dy;
+  const double ex = (double)(e.x - px), ey = (double)(e.y - py);
+  float dist = (float)sqrt(ex * ex + ey * ey);
+  if (d >= 4) dist = (float)(dist / sqrt(2.0));
+  if (on_edge) dist = 11 * min_step;
+  else if (e.x == -1 || e.y == -1 || dist > max_edge_dist) {
+    dist = max_edge_dist;
+    if (d >= 4) dist = (float)(dist / sqrt(2.0));
+  }
+  const int step_num = cvmin(cvmax(11, (int)(1.0f * dist / min_step)), 22);
+  int step_len = cvmax((int)(1.0f * dist / step_num), min_step);
+  if (d < 4 && step_len % 2 == 1) step_len -= 1;
+  float mc = FLT_MAX;
+  int mp = -1;
+  int fx = 0, fy = 0;
+  if (d > 4) { if (d % 2) fx = dx; else fy = dy; }
+  for (int s = 0; s < step_num; ++s) {
+    const int tx = px + sx + s * step_len * dx + fx, ty = py + sy + s * step_len * dy + fy;
+    if (!(tx >= 0 && ty >= 0 && tx < W && ty < H)) continue;
+    const int tc = tx + ty * W;
+    const float cc = G(cand_cost, tc, L, 204);
+    if (mc > cc) { mp = tc; mc = cc; }
+  }
+  return mc < FLT_MAX ? mp : -1;
+}
+
+// Phase 1: window sums in tap order (lane 0), as build_ref_window accumulates them; every lane
+// searches its candidate direction (the non-edge form; the edge form searches in phase 2).
+__device__ __forceinline__ void strong_p1(const CoopCtx &c) {
+  if (!c.live) return;
+  const PMArgs &a = *c.a;
+  if (c.lane == 0) {
+    const int r = a.P.strong_radius, inc = a.P.strong_increment, side = 2 * r / inc + 1;
+    float sw = 0.f, swr = 0.f, swrr = 0.f;
+    for (int k = 0; k < side * side; ++k) {
+      const float2 t = c.P->win[k];
+      sw += t.x; swr += t.y; swrr += t.y * c.P->rc[k];
+    }
+    c.P->inv_wsum = 1.0f / sw;
+    c.P->mean_r = swr * c.P->inv_wsum;
+    c.P->var_r = swrr * c.P->inv_wsum - c.P->mean_r * c.P->mean_r;
+  }
+  if (!a.P.use_edge) c.P->pos[c.lane] = strong_search_plain(a, c.px, c.py, c.center, c.lane);
+}
+
+// Phase 2: candidate d's costs against every source (lane d), with the edge form's second search
+// and its replacement rule (DPE.cu:1302-1366).
+template <int kStage>
+__device__ __forceinline__ void strong_p2(const CoopCtx &c, int iter) {
+  if (!c.live) return;
+  const PMArgs &a = *c.a;
+  const int n = c.n, d = c.lane;
+  [[maybe_unused]] const long long L = (long long)a.W * a.H;
+  float *row = c.cost + d * n;
+  for (int j = 0; j < n; ++j) row[j] = 0.0f;
+  if (d == 0) row[0] = 2.0f;  // `= {2.0f}` initialises only the first element (quirk Q2)
+  const SmemWindow rw = c.window();
+  bool flag = false;
+  int pos = -1;
+  if (a.P.use_edge) {
+    pos = strong_search_edge(a, c.px, c.py, c.center, d, iter);
+    if (pos >= 0) {
+      flag = true;
+      ncc_all_sources<kStage>(a, c.px, c.py, G(a.plane_snap, pos, L, 205), rw, row);
+    }
+    if (G(a.edge, c.center, L, 203) == 0) {
+      const float good_thr = 0.8f * dpe_expf((float)(iter * iter) / (-90.0f));
+      const int dx = kDir[d][0], dy = kDir[d][1], min_step = 2;
+      const int sx = cvmax(1, 5 - 2 * iter) * dx, sy = cvmax(1, 5 - 2 * iter) * dy;
+      const bool had = flag;
       float mc = FLT_MAX;
       int mp = -1;
       int fx = 0, fy = 0;
       if (d > 4) { if (d % 2) fx = dx; else fy = dy; }
-      for (int s = 0; s < step_num; ++s) {
-        const int tx = px + sx + s * step_len * dx + fx, ty = py + sy + s * step_len * dy + fy;
-        if (!(tx >= 0 && ty >= 0 && tx < W && ty < H)) continue;
-        const int tc = tx + ty * W;
-        const float cc = G(cand_cost, tc, L, 204);
+      for (int s = 0; s < 11; ++s) {
+        const int tx = c.px + sx + s * min_step * dx + fx, ty = c.py + sy + s * min_step * dy + fy;
+        if (!(tx >= 0 && ty >= 0 && tx < a.W && ty < a.H)) continue;
+        const int tc = tx + ty * a.W;
+        const float cc = G(a.cost_snap, tc, L, 204);
         if (mc > cc) { mp = tc; mc = cc; }
       }
       if (mc < FLT_MAX) {
-        flag[d] = true;
-        positions[d] = mp;
-        const float4 cp = G(cand_plane, mp, L, 205);
-        ncc_all_sources<kStage>(a, px, py, cp, rw, cost_array[d]);
-      }
-    }
-    if (!on_edge) {
-      const float good_thr = 0.8f * dpe_expf((float)(iter * iter) / (-90.0f));
-      for (int d = 0; d < 8; ++d) {
-        const int dx = kDir[d][0], dy = kDir[d][1];
-        const int sx = cvmax(1, 5 - 2 * iter) * dx, sy = cvmax(1, 5 - 2 * iter) * dy;
-        const bool had = flag[d];
-        float mc = FLT_MAX;
-        int mp = -1;
-        int fx = 0, fy = 0;
-        if (d > 4) { if (d % 2) fx = dx; else fy = dy; }
-        for (int s = 0; s < 11; ++s) {
-          const int tx = px + sx + s * min_step * dx + fx, ty = py + sy + s * min_step * dy + fy;
-          if (!(tx >= 0 && ty >= 0 && tx < W && ty < H)) continue;
-          const int tc = tx + ty * W;
-          const float cc = G(cand_cost, tc, L, 204);
-          if (mc > cc) { mp = tc; mc = cc; }
+        flag = true;
+        float tca[kMaxSrc];
+        ncc_all_sources<kStage>(a, c.px, c.py, G(a.plane_snap, mp, L, 205), rw, tca);
+        int g0 = 0, g1 = 0, b0 = 0, b1 = 0;
+        for (int j = 0; j < n; ++j) {
+          if (row[j] < good_thr) g0++;
+          if (row[j] > 1.2f) b0++;
+          if (tca[j] < good_thr) g1++;
+          if (tca[j] > 1.2f) b1++;
         }
-        if (mc < FLT_MAX) {
-          flag[d] = true;
-          float tca[kMaxSrc];
-          const float4 cp = G(cand_plane, mp, L, 205);
-          ncc_all_sources<kStage>(a, px, py, cp, rw, tca);
-          int g0 = 0, g1 = 0, b0 = 0, b1 = 0;
-          for (int j = 0; j < n; ++j) {
-            if (cost_array[d][j] < good_thr) g0++;
-            if (cost_array[d][j] > 1.2f) b0++;
-            if (tca[j] < good_thr) g1++;
-            if (tca[j] > 1.2f) b1++;
-          }
-          if (!had || g1 > g0 || (g1 == g0 && b1 < b0)) {
-            positions[d] = mp;
-            for (int j = 0; j < n; ++j) cost_array[d][j] = tca[j];
-          }
+        if (!had || g1 > g0 || (g1 == g0 && b1 < b0)) {
+          pos = mp;
+          for (int j = 0; j < n; ++j) row[j] = tca[j];
         }
       }
     }
   } else {
-    // 0 up_near, 1 up_far, 2 down_near, 3 down_far, 4 left_near, 5 left_far, 6 right_near, 7 right_far
-    const int starts[4] = {center - 3 * W, center + 3 * W, center - 3, center + 3};
-    const int strides[4] = {-W, W, -1, 1};
-    const bool oks[4] = {py > 2, py < H - 3, px > 2, px < W - 3};
-    for (int f = 0; f < 4; ++f) {
-      if (!oks[f]) continue;
-      const int slot = 2 * f + 1;
-      flag[slot] = true;
-      float m = G(a.cost, starts[f], L, 206);
-      int mp = starts[f];
-      for (int i = 1; i < 11; ++i) {
-        bool ok;
-        switch (f) {
-          case 0: ok = py > 2 + 2 * i; break;
-          case 1: ok = py < H - 3 - 2 * i; break;
-          case 2: ok = px > 2 + 2 * i; break;
-          default: ok = px < W - 3 - 2 * i; break;
-        }
-        if (ok) {
-          const int t = starts[f] + 2 * i * strides[f];
-          const float ct = G(a.cost, t, L, 207);
-          if (ct < m) { m = ct; mp = t; }
-        }
-      }
-      positions[slot] = mp;
-    }
-    // near: base pixel one step away, then diagonal pairs at distance 1..3
-    const int nbase[4] = {center - W, center + W, center - 1, center + 1};
-    const bool nok[4] = {py > 0, py < H - 1, px > 0, px < W - 1};
-    for (int f = 0; f < 4; ++f) {
-      if (!nok[f]) continue;
-      const int slot = 2 * f;
-      flag[slot] = true;
-      float m = G(a.cost, nbase[f], L, 208);
-      int mp = nbase[f];
-      for (int i = 0; i < 3; ++i)
-        for (int side = 0; side < 2; ++side) {
-          bool ok;
-          int t;
-          const int k = 1 + i;
-          switch (f) {
-            case 0: t = nbase[0] - k * W + (side ? k : -k); ok = py > 1 + i && (side ? px < W - 1 - i : px > i); break;
-            case 1: t = nbase[1] + k * W + (side ? k : -k); ok = py < H - 2 - i && (side ? px < W - 1 - i : px > i); break;
-            case 2: t = nbase[2] - k + (side ? k * W : -k * W); ok = px > 1 + i && (side ? py < H - 1 - i : py > i); break;
-            default: t = nbase[3] + k + (side ? k * W : -k * W); ok = px < W - 2 - i && (side ? py < H - 1 - i : py > i); break;
-          }
-          if (ok) {
-            const float ct = G(a.cost, t, L, 209);
-            if (ct < m) { m = ct; mp = t; }
-          }
-        }
-      positions[slot] = mp;
-    }
-    for (int d = 0; d < 8; ++d) {
-      if (!flag[d]) continue;
-      const float4 cp = G(a.plane, positions[d], L, 210);
-      ncc_all_sources<kStage>(a, px, py, cp, rw, cost_array[d]);
+    pos = c.P->pos[d];
+    if (pos >= 0) {
+      flag = true;
+      ncc_all_sources<kStage>(a, c.px, c.py, G(a.plane, pos, L, 210), rw, row);
     }
   }
-#ifdef DPE_CHECKED
-  for (int d = 0; d < 8; ++d)
-    if (flag[d]) (void)G(a.plane, positions[d], L, 311 + d);
-#endif
+  c.P->flag[d] = flag ? 1 : 0;
+  c.P->pos[d] = pos;
+}
 
+// Phase 3 (lane 0): view-selection priors and sampling, the best candidate, the sampled sources.
+__device__ __forceinline__ void strong_p3(const CoopCtx &c, int iter) {
+  if (!c.live || c.lane != 0) return;
+  const PMArgs &a = *c.a;
+  const int W = a.W, n = c.n, center = c.center;
+  [[maybe_unused]] const long long L = (long long)W * a.H;
+  CoopPixel &P = *c.P;
   float priors[kMaxSrc], probs[kMaxSrc];
   for (int j = 0; j < n; ++j) priors[j] = 0.0f;
-  const long total = (long)W * H;
+  const long total = (long)W * a.H;
   const long nbr[4] = {(long)center - W, (long)center + W, (long)center - 1, (long)center + 1};
   for (int i = 0; i < 4; ++i)
-    if (flag[2 * i]) {
+    if (P.flag[2 * i]) {
       const uint32_t sv = (nbr[i] >= 0 && nbr[i] < total) ? G(a.views, nbr[i], L, 211) : 0u;
       for (int j = 0; j < n; ++j) priors[j] += isSet(sv, j) == 1 ? 0.9f : 0.1f;
     }
-#ifdef DPE_CHECKED
-  for (int d = 0; d < 8; ++d)
-    if (flag[d]) (void)G(a.plane, positions[d], L, 331 + d);
-#endif
   Rng rng = make_rng(a, center);
-  uint8_t vw[32];
   uint32_t temp_sel = 0;
-  const float wn = sample_views(a, rng, iter, &cost_array[0][0], kMaxSrc, priors, vw, &temp_sel, probs);
-#ifdef DPE_CHECKED
-  for (int d = 0; d < 8; ++d)
-    if (flag[d]) (void)G(a.plane, positions[d], L, 341 + d);
-#endif
+  const float wn = sample_views(a, rng, iter, c.cost, n, priors, P.vw, &temp_sel, probs);
   float final_costs[8];
   for (int i = 0; i < 8; ++i) {
     float fc = 0.0f;
     for (int j = 0; j < n; ++j)
-      if (vw[j] > 0) fc += vw[j] * cost_array[i][j];
+      if (P.vw[j] > 0) fc += P.vw[j] * c.cost[i * n + j];
     final_costs[i] = fc / wn;
   }
-#ifdef DPE_CHECKED
-  for (int d = 0; d < 8; ++d)
-    if (flag[d]) (void)G(a.plane, positions[d], L, 351 + d);
-#endif
   const int mi = find_min_cost_index(final_costs, 8);
-#ifdef DPE_CHECKED
-  (void)G(flag, mi, 8, 300);
-  for (int d = 0; d < 8; ++d)
-    if (flag[d]) (void)G(a.plane, positions[d], L, 301 + d);
-#endif
-  const float4 pl_cur = G(a.plane, center, L, 212);
-  // sampled sources in ascending order: views with no samples contribute 0 * (finite cost)
-  int act[kMaxSrc];
   int na = 0;
   for (int i = 0; i < n; ++i)
-    if (vw[i] > 0) act[na++] = i;
-  float cost_now = weighted_ncc<kStage>(a, px, py, pl_cur, rw, act, na, vw);
-  cost_now /= wn;
-  const float cost_written = cost_now;
-  float depth_now = depth_from_plane(rc, pl_cur, px, py);
+    if (P.vw[i] > 0) P.act[na++] = i;
+  P.na = na;
+  P.mi = mi;
+  P.fcost_mi = final_costs[mi];
+  P.wn = wn;
+  P.temp_sel = temp_sel;
+  P.rng_ctr = rng.ctr;
+  P.pl_cur = G(a.plane, center, L, 212);
+}
+
+// Phase 4: the current plane's cost against each sampled source (lanes split the sources).
+template <int kStage>
+__device__ __forceinline__ void strong_p4(const CoopCtx &c) {
+  if (!c.live) return;
+  const SmemWindow rw = c.window();
+  const int na = c.P->na;
+  const float4 pl = c.P->pl_cur;
+  for (int q = c.lane; q < na; q += kCoopLanes)
+    c.hc[q] = ncc_strong<kStage>(*c.a, c.px, c.py, c.P->act[q] + 1, pl, rw);
+}
+
+// Phase 5 (lane 0): the current cost, candidate acceptance, and the five refinement planes of
+// PlaneHypothesisRefinementStrong (DPE.cu:1069-1122) with their random draws.
+__device__ __forceinline__ void strong_p5(const CoopCtx &c) {
+  if (!c.live || c.lane != 0) return;
+  const PMArgs &a = *c.a;
+  const dpe_camera &rc = a.cam[0];
+  [[maybe_unused]] const long long L = (long long)a.W * a.H;
+  CoopPixel &P = *c.P;
+  const int na = P.na;
+  float cost_now = 0.0f;
+  for (int q = 0; q < na; ++q) cost_now += P.vw[P.act[q]] * c.hc[q];
+  cost_now /= P.wn;
+  P.cost_written = cost_now;
+  const float4 pl_cur = P.pl_cur;
+  float depth_now = depth_from_plane(rc, pl_cur, c.px, c.py);
   float4 pl_now = pl_cur;
-  uint32_t views_new = G(a.views, center, L, 213);
-  if (flag[mi]) {
-    const float4 cand = G(cand_plane, positions[mi], L, 214);
-    const float db = depth_from_plane(rc, cand, px, py);
-    if (db >= a.P.depth_min && db <= a.P.depth_max && final_costs[mi] < cost_now) {
-      depth_now = db; pl_now = cand; cost_now = final_costs[mi];
-      views_new = temp_sel;
+  uint32_t views_new = G(a.views, c.center, L, 213);
+  const int mi = P.mi;
+  if (P.flag[mi]) {
+    const float4 cand = G(a.P.use_edge ? a.plane_snap : a.plane, P.pos[mi], L, 214);
+    const float db = depth_from_plane(rc, cand, c.px, c.py);
+    if (db >= a.P.depth_min && db <= a.P.depth_max && P.fcost_mi < cost_now) {
+      depth_now = db; pl_now = cand; cost_now = P.fcost_mi;
+      views_new = P.temp_sel;
     }
   }
-  // PlaneHypothesisRefinementStrong (DPE.cu:1069-1122)
-  {
-    const float dmin = a.P.depth_min, dmax = a.P.depth_max;
-    const float depth_rand = rng.uniform() * (dmax - dmin) + dmin;
-    const float4 n_rand = random_normal(rc, px, py, rng, depth_now);
-    const float lo = (1 - 0.02f) * depth_now, hi = (1 + 0.02f) * depth_now;
-    const float depth_pert = rng.uniform() * (hi - lo) + lo;
-    const float4 n_pert = perturbed_normal(rc, px, py, pl_now, rng, (float)(0.02f * 3.14159265358979323846));
-    const float depths[5] = {depth_rand, depth_now, depth_rand, depth_now, depth_pert};
-    const float4 normals[5] = {pl_now, n_rand, n_rand, n_pert, pl_now};
-    for (int h = 0; h < 5; ++h) {
-      float4 t = normals[h];
-      t.w = dist_to_origin(rc, px, py, depths[h], t);
-      float tc = weighted_ncc<kStage>(a, px, py, t, rw, act, na, vw);
-      tc /= wn;
-      const float db = depth_from_plane(rc, t, px, py);
-      if (db >= dmin && db <= dmax && tc < cost_now) { depth_now = db; pl_now = t; cost_now = tc; }
-    }
+  Rng rng{a.key[0], a.key[1], (uint32_t)c.center, P.rng_ctr};
+  const float dmin = a.P.depth_min, dmax = a.P.depth_max;
+  const float depth_rand = rng.uniform() * (dmax - dmin) + dmin;
+  const float4 n_rand = random_normal(rc, c.px, c.py, rng, depth_now);
+  const float lo = (1 - 0.02f) * depth_now, hi = (1 + 0.02f) * depth_now;
+  const float depth_pert = rng.uniform() * (hi - lo) + lo;
+  const float4 n_pert = perturbed_normal(rc, c.px, c.py, pl_now, rng, (float)(0.02f * 3.14159265358979323846));
+  const float depths[5] = {depth_rand, depth_now, depth_rand, depth_now, depth_pert};
+  const float4 normals[5] = {pl_now, n_rand, n_rand, n_pert, pl_now};
+  for (int h = 0; h < 5; ++h) {
+    float4 t = normals[h];
+    t.w = dist_to_origin(rc, c.px, c.py, depths[h], t);
+    P.hyp[h] = t;
   }
-  if (kGN && na > 0) gn_hypothesis<kStage>(a, px, py, rw, act, na, vw, wn, &pl_now, &depth_now, &cost_now);
-  G(a.rng_ctr, center, L, 215) = rng.ctr;
-  G(a.views, center, L, 216) = views_new;
-  store_vweight(&G(a.vweight, center, L, 217), vw);
+  P.pl_now = pl_now;
+  P.depth_now = depth_now;
+  P.cost_now = cost_now;
+  P.views_new = views_new;
+  P.rng_ctr = rng.ctr;
+}
+
+// Phase 6: the refinement planes' costs, (plane, sampled source) pairs split over the lanes.
+template <int kStage>
+__device__ __forceinline__ void strong_p6(const CoopCtx &c) {
+  if (!c.live) return;
+  const SmemWindow rw = c.window();
+  const int na = c.P->na, n = c.n;
+  for (int i = c.lane; i < 5 * na; i += kCoopLanes) {
+    const int h = i / na, q = i - h * na;
+    c.hc[(1 + h) * n + q] = ncc_strong<kStage>(*c.a, c.px, c.py, c.P->act[q] + 1, c.P->hyp[h], rw);
+  }
+}
+
+// Phase 7 (lane 0): the refinement decisions in order, the optional Gauss-Newton plane, outputs.
+template <int kStage, bool kGN>
+__device__ __forceinline__ void strong_p7(const CoopCtx &c) {
+  if (!c.live || c.lane != 0) return;
+  const PMArgs &a = *c.a;
+  const dpe_camera &rc = a.cam[0];
+  [[maybe_unused]] const long long L = (long long)a.W * a.H;
+  const int center = c.center, na = c.P->na, n = c.n;
+  CoopPixel &P = *c.P;
+  const float dmin = a.P.depth_min, dmax = a.P.depth_max;
+  float depth_now = P.depth_now, cost_now = P.cost_now;
+  float4 pl_now = P.pl_now;
+  for (int h = 0; h < 5; ++h) {
+    const float4 t = P.hyp[h];
+    float tc = 0.0f;
+    for (int q = 0; q < na; ++q) tc += P.vw[P.act[q]] * c.hc[(1 + h) * n + q];
+    tc /= P.wn;
+    const float db = depth_from_plane(rc, t, c.px, c.py);
+    if (db >= dmin && db <= dmax && tc < cost_now) { depth_now = db; pl_now = t; cost_now = tc; }
+  }
+  if (kGN && na > 0)
+    gn_hypothesis<kStage>(a, c.px, c.py, c.window(), P.act, na, P.vw, P.wn, &pl_now, &depth_now, &cost_now);
+  G(a.rng_ctr, center, L, 215) = P.rng_ctr;
+  G(a.views, center, L, 216) = P.views_new;
+  store_vweight(&G(a.vweight, center, L, 217), P.vw);
+  const float cost_written = P.cost_written;
   if (a.P.state == DPE_REFINE_INIT) {
     if ((double)cost_now < (double)cost_written - 0.1) { G(a.cost, center, L, 218) = cost_now; G(a.plane, center, L, 219) = pl_now; }
     else G(a.cost, center, L, 220) = cost_written;
@@ -938,6 +1090,47 @@ __global__ void __launch_bounds__(128, DPE_STRONG_MIN_BLOCKS) k_strong_update(co
     G(a.plane, center, L, 222) = pl_now;
   }
 }
+
+// One phase for one thread (host builds of this source run the phases in lock-step over a block).
+template <int kStage, bool kGN>
+__device__ __forceinline__ void strong_update_phase(int phase, const Launch &lc, int iter, int parity, void *smem) {
+  const CoopCtx c = coop_ctx(lc, parity, smem);
+  switch (phase) {
+    case 0: strong_p0(c); break;
+    case 1: strong_p1(c); break;
+    case 2: strong_p2<kStage>(c, iter); break;
+    case 3: strong_p3(c, iter); break;
+    case 4: strong_p4<kStage>(c); break;
+    case 5: strong_p5(c); break;
+    case 6: strong_p6<kStage>(c); break;
+    default: strong_p7<kStage, kGN>(c); break;
+  }
+}
+constexpr int kStrongPhases = 8;
+
+// Grid: ((W + 15) / 16, (H + 1) / 2) blocks of kCoopThreads; coop_smem_bytes(N - 1) dynamic shared
+// bytes (the largest N of a batch).
+template <int kStage, bool kGN>
+__global__ void __launch_bounds__(kCoopThreads, DPE_STRONG_MIN_BLOCKS) k_strong_update(const Launch lc, int iter, int parity) {
+  extern __shared__ float4 coop_smem[];
+  const CoopCtx c = coop_ctx(lc, parity, coop_smem);
+  strong_p0(c);
+  __syncthreads();
+  strong_p1(c);
+  __syncthreads();
+  strong_p2<kStage>(c, iter);
+  __syncthreads();
+  strong_p3(c, iter);
+  __syncthreads();
+  strong_p4<kStage>(c);
+  __syncthreads();
+  strong_p5(c);
+  __syncthreads();
+  strong_p6<kStage>(c);
+  __syncthreads();
+  strong_p7<kStage, kGN>(c);
+}
+
 
 // ------------------------------------------------------------------ RANSACToGetFitPlane (DPE.cu:2895-3128)
 __device__ __forceinline__ void ransac_fit_plane_pixel(const PMArgs &a, int px, int py) {

@@ -33,6 +33,9 @@ static dim3 blockIdx, threadIdx, blockDim, gridDim;
 #define __restrict__
 static inline unsigned __umulhi(unsigned a, unsigned b) { return (unsigned)(((unsigned long long)a * b) >> 32); }
 template <class T> static inline T __ldg(const T *p) { return *p; }
+// Kernels with block barriers run here only through launch_phased (their phases in lock-step); a
+// sequential launch of one would ignore its barriers, so the stand-in refuses to run.
+static inline void __syncthreads() { std::abort(); }
 // the device's correctly rounded, never-contracted arithmetic intrinsics
 static inline float __fmul_rn(float a, float b) { volatile float r = a * b; return r; }
 static inline float __fadd_rn(float a, float b) { volatile float r = a + b; return r; }
@@ -75,6 +78,24 @@ template <class K, class... Args> static void launch(dim3 grid, dim3 block, K k,
           threadIdx = dim3(tx, ty, 1);
           k(args...);
         }
+}
+// A block-cooperative kernel given as phases (the code between its barriers): every thread of a
+// block runs phase p before any runs phase p + 1, over one zeroed shared-memory buffer per block.
+template <class F> static void launch_phased(dim3 grid, dim3 block, size_t smem_bytes, int phases, F phase) {
+  blockDim = block;
+  gridDim = grid;
+  std::vector<float4> smem((smem_bytes + 15) / 16);
+  for (unsigned by = 0; by < grid.y; ++by)
+    for (unsigned bx = 0; bx < grid.x; ++bx) {
+      std::fill(smem.begin(), smem.end(), float4{0, 0, 0, 0});
+      for (int p = 0; p < phases; ++p)
+        for (unsigned ty = 0; ty < block.y; ++ty)
+          for (unsigned tx = 0; tx < block.x; ++tx) {
+            blockIdx = dim3(bx, by, 1);
+            threadIdx = dim3(tx, ty, 1);
+            phase(p, smem.data());
+          }
+    }
 }
 template <class T> static T *alloc(size_t n) { return (T *)calloc(n, sizeof(T)); }
 
@@ -144,7 +165,10 @@ extern "C" int host_pm_run(const dpe_problem *p, dpe_pm_out *out) {
   for (int it = 0; it < a.P.max_iterations; ++it) {
     for (int parity = 0; parity < 2; ++parity) {
       if (a.P.use_edge) { memcpy(a.plane_snap, a.plane, L * 16); memcpy(a.cost_snap, a.cost, L * 4); }
-      launch(hg, hb, k_strong_update<DPE_STAGE_FP32, false>, one, it, parity);
+      launch_phased(dim3((W + kCoopPix - 1) / kCoopPix, (H + 1) / 2), dim3(kCoopThreads), coop_smem_bytes(N - 1),
+                    kStrongPhases, [&](int ph, void *sm) {
+                      strong_update_phase<DPE_STAGE_FP32, false>(ph, one, it, parity, sm);
+                    });
     }
     launch(fg, fb, k_ransac_fit_plane, one);
     if (a.P.use_APD)
