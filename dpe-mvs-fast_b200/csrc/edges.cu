@@ -457,6 +457,9 @@ __global__ void __launch_bounds__(kHoughThreads) k_hough_region(const __grid_con
   uint64_t state = ~0ull;  // cv::RNG((uint64)-1), thread 0 only
   const int shift = 16;
   for (int count = s_count; count > 0; --count) {
+    // Every thread has read the previous point's shared values (s_skip, s_idx_*, s_best_*) before
+    // thread 0 overwrites them: the `continue`s below leave an iteration without a later barrier.
+    __syncthreads();
     if (tid == 0) {
       state = (uint64_t)(unsigned)state * 4164903690u + (unsigned)(state >> 32);
       const int idx = (int)((unsigned)state % (unsigned)count);
@@ -547,6 +550,7 @@ __global__ void __launch_bounds__(kHoughThreads) k_hough_region(const __grid_con
     }
     __syncthreads();
   }
+  __syncthreads();
   if (s_nlines > a.line_cap && tid == 0) atomicExch(a.error, 2);
   const int nl = min(s_nlines, a.line_cap);
   for (int q = tid; q < nl; q += kHoughThreads) draw_line8(a.dst, w, lines[q].x, lines[q].y, lines[q].z, lines[q].w);
