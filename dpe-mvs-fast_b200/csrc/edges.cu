@@ -472,17 +472,21 @@ __global__ void __launch_bounds__(kHoughThreads) k_hough_region(const __grid_con
     __syncthreads();
     if (s_skip) continue;  // uniform: already withdrawn by an earlier segment
     const int j = s_idx_x, i = s_idx_y;
-    // vote, and the first angle with the largest count
+    // vote, and the first angle with the largest count.  Counts can be negative: a segment
+    // withdraws the votes of every mask pixel on it, also of pixels that have not voted yet (as
+    // OpenCV does).  The key's high word is the count with its sign bit flipped, so unsigned
+    // order is the counts' signed order; the low word prefers the smaller angle on ties.
     unsigned long long best = 0;
     for (int nn = tid; nn < a.numangle; nn += kHoughThreads) {
       const int r = hough_bin(a, a.tab[nn], j, i);
       const int val = ++acc[(size_t)nn * a.numrho + r];
-      const unsigned long long key = ((unsigned long long)(unsigned)val << 32) | (unsigned)(0x7fffffff - nn);
+      const unsigned long long key =
+          ((unsigned long long)((unsigned)val ^ 0x80000000u) << 32) | (unsigned)(0x7fffffff - nn);
       best = key > best ? key : best;
     }
     best = RedU(ts_r).Reduce(best, cub::Max());
     if (tid == 0) {
-      s_best_v = (int)(best >> 32);
+      s_best_v = (int)((unsigned)(best >> 32) ^ 0x80000000u);
       s_best_n = 0x7fffffff - (int)(best & 0xffffffffu);
     }
     __syncthreads();
