@@ -202,6 +202,8 @@ dim3 half_grid(int W, int H) { return dim3((W + 31) / 32, ((H + 1) / 2 + 3) / 4)
 const dim3 kHalfBlock(32, 4);
 // the cooperative strong update: 16 pixels of one colour per block (kCoopPix), one half-grid row
 dim3 coop_grid(int W, int H) { return dim3((W + kCoopPix - 1) / kCoopPix, (H + 1) / 2); }
+// the cooperative sweeps (DepthToWeak, LocalRefine): 16 pixels of one row per block
+dim3 sweep_grid(int W, int H) { return dim3((W + kCoopPix - 1) / kCoopPix, H); }
 
 // Blocks of 128 threads for a strided work list of up to `items` entries: enough to fill every
 // multiprocessor, no more than the list needs.
@@ -410,9 +412,10 @@ int setup_problem(dpe_ctx *ctx, const dpe_problem *p, int index, ProblemState *p
 // Grids of one kernel sequence: for one problem the 2D pixel grids; for a batch one 1D grid per
 // kind over all problems, with the prefix tables the kernels resolve their problem from.
 struct SequenceGrids {
-  Launch full, half, prep, eval, coop;
-  dim3 fg, hg, cg;
+  Launch full, half, prep, eval, coop, sweep;
+  dim3 fg, hg, cg, sg;
   size_t coop_smem = 0;  // dynamic shared bytes of the strong update (largest source count)
+  size_t lr_smem = 0;    // dynamic shared bytes of LocalRefine (largest source count)
   unsigned gp = 0, ge = 0;
   const dim3 fb = kFullBlock, hb = kHalfBlock;
 };
@@ -504,9 +507,18 @@ int run_sequence(dpe_ctx *ctx, ProblemState *ps, int n, const PMArgs *d_args, co
     DPE_TIMED(ctx, KID_FILTER, s, k_filter_strong<<<g.hg, g.hb, 0, s>>>(g.half, parity));
     PM_LAUNCHED("k_filter_strong", s);
   }
-  DPE_TIMED(ctx, KID_DEPTH_TO_WEAK, s, with_stage(staging, [&](auto st) { k_depth_to_weak<decltype(st)::value><<<g.fg, g.fb, 0, s>>>(g.full); }));
+  DPE_TIMED(ctx, KID_DEPTH_TO_WEAK, s, with_stage(staging, [&](auto st) { k_depth_to_weak<decltype(st)::value><<<g.sg, kCoopThreads, 0, s>>>(g.sweep); }));
   PM_LAUNCHED("k_depth_to_weak", s);
-  DPE_TIMED(ctx, KID_LOCAL_REFINE, s, with_stage(staging, [&](auto st) { k_local_refine<decltype(st)::value><<<g.fg, g.fb, 0, s>>>(g.full); }));
+  {
+    cudaError_t attr = cudaSuccess;
+    with_stage(staging, [&](auto st) {
+      if (g.lr_smem > 48 * 1024)
+        attr = cudaFuncSetAttribute(k_local_refine<decltype(st)::value>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)g.lr_smem);
+    });
+    DPE_TRY(attr);
+  }
+  DPE_TIMED(ctx, KID_LOCAL_REFINE, s, with_stage(staging, [&](auto st) { k_local_refine<decltype(st)::value><<<g.sg, kCoopThreads, g.lr_smem, s>>>(g.sweep); }));
   PM_LAUNCHED("k_local_refine", s);
   return DPE_OK;
 }
@@ -531,7 +543,7 @@ int pm_run_problems(dpe_ctx *ctx, const dpe_problem *const *problems, int n, dpe
   std::vector<ProblemState> ps(n);
   unsigned long long *counters = A.get<unsigned long long>("counters", 2 * KID_COUNT);
   PMArgs *d_args = A.get<PMArgs>("pm_args", n);
-  int *d_start = n > 1 ? A.get<int>("batch_start", 5 * (n + 1)) : nullptr;
+  int *d_start = n > 1 ? A.get<int>("batch_start", 6 * (n + 1)) : nullptr;
   if (!counters || !d_args || (n > 1 && !d_start)) return DPE_ERR_OUT_OF_MEMORY;
   if (ctx->count_evals) DPE_TRY(cudaMemsetAsync(counters, 0, 16 * KID_COUNT, s));
   for (int b = 0; b < n; ++b) {
@@ -565,21 +577,26 @@ int pm_run_problems(dpe_ctx *ctx, const dpe_problem *const *problems, int n, dpe
   if (n == 1) {
     const PMArgs &a = ps[0].a;
     const Launch one{d_args, nullptr, 1};
-    g.full = g.half = g.prep = g.eval = g.coop = one;
+    g.full = g.half = g.prep = g.eval = g.coop = g.sweep = one;
+    g.sg = sweep_grid(a.W, a.H);
     g.fg = full_grid(a.W, a.H);
     g.hg = half_grid(a.W, a.H);
     g.cg = coop_grid(a.W, a.H);
     g.coop_smem = coop_smem_bytes(a.N - 1);
+    g.lr_smem = local_refine_smem_bytes(a.N - 1);
     g.gp = list_grid(ctx, (long long)ps[0].wcap);
     g.ge = list_grid(ctx, (long long)ps[0].wcap * 10 * (a.N - 1));
   } else {
     // the problems' grids laid end to end: prefix tables per grid kind
-    std::vector<int> start(5 * (n + 1), 0);
+    std::vector<int> start(6 * (n + 1), 0);
     for (int b = 0; b < n; ++b) {
       const PMArgs &a = ps[b].a;
       const dim3 f = full_grid(a.W, a.H), h = half_grid(a.W, a.H), cg = coop_grid(a.W, a.H);
       start[4 * (n + 1) + b + 1] = start[4 * (n + 1) + b] + (int)(cg.x * cg.y);
+      const dim3 sg = sweep_grid(a.W, a.H);
+      start[5 * (n + 1) + b + 1] = start[5 * (n + 1) + b] + (int)(sg.x * sg.y);
       g.coop_smem = std::max(g.coop_smem, coop_smem_bytes(a.N - 1));
+      g.lr_smem = std::max(g.lr_smem, local_refine_smem_bytes(a.N - 1));
       start[0 * (n + 1) + b + 1] = start[0 * (n + 1) + b] + (int)(f.x * f.y);
       start[1 * (n + 1) + b + 1] = start[1 * (n + 1) + b] + (int)(h.x * h.y);
       start[2 * (n + 1) + b + 1] = start[2 * (n + 1) + b] + (int)list_grid(ctx, (long long)ps[b].wcap);
@@ -593,6 +610,8 @@ int pm_run_problems(dpe_ctx *ctx, const dpe_problem *const *problems, int n, dpe
     g.eval = Launch{d_args, d_start + 3 * (n + 1), n};
     g.coop = Launch{d_args, d_start + 4 * (n + 1), n};
     g.cg = dim3(start[4 * (n + 1) + n]);
+    g.sweep = Launch{d_args, d_start + 5 * (n + 1), n};
+    g.sg = dim3(start[5 * (n + 1) + n]);
     g.fg = dim3(start[0 * (n + 1) + n]);
     g.hg = dim3(start[1 * (n + 1) + n]);
     g.gp = (unsigned)start[2 * (n + 1) + n];

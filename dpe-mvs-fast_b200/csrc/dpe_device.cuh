@@ -23,13 +23,19 @@ constexpr int kNeighbours = DPE_NEIGHBOUR_NUM;
 constexpr int kMaxWin = 6;  // taps per window side for radius 5 / step 2 (DPE.cu:728-737)
 // Minimum resident blocks per multiprocessor requested for the strong-window cost kernels
 // (__launch_bounds__): bounds their registers, trading spills against occupancy.  Measured on
-// the 10-view 1600x1200 schedule: the strong update runs fastest at 6 blocks (80 registers,
-// 24 warps), the sweep kernels unconstrained.
+// the 10-view 1600x1200 schedule: the cooperative strong update runs fastest at 8 blocks of 128
+// (64 registers; 2 % faster than 6 blocks at 80), the sweep kernels unconstrained.
 #ifndef DPE_COST_MIN_BLOCKS
 #define DPE_COST_MIN_BLOCKS 1
 #endif
 #ifndef DPE_STRONG_MIN_BLOCKS
-#define DPE_STRONG_MIN_BLOCKS 6
+#define DPE_STRONG_MIN_BLOCKS 8
+#endif
+// the same bound for the cooperative DepthToWeak sweep (measured: 8 blocks, 64 registers, 4 %
+// faster than unbounded; the cooperative LocalRefine, with its larger shared-memory block, runs
+// fastest unbounded and uses DPE_COST_MIN_BLOCKS)
+#ifndef DPE_SWEEP_MIN_BLOCKS
+#define DPE_SWEEP_MIN_BLOCKS 8
 #endif
 // Unrolling of a window column's taps (the reference window, radius 5 / step 2, has 6 per column)
 // in the kernels that sweep one plane family over all sources: measured, unrolling by 3 speeds
@@ -39,6 +45,12 @@ constexpr int kMaxWin = 6;  // taps per window side for radius 5 / step 2 (DPE.c
 #define DPE_SWEEP_UNROLL 3
 #endif
 constexpr int kSweepUnroll = DPE_SWEEP_UNROLL;
+// taps of a window column unrolled in the strong update's cost evaluations (0: rolled loop;
+// measured: unrolling by 3 or 6 makes the cooperative strong update 35-40 % slower)
+#ifndef DPE_STRONG_UNROLL
+#define DPE_STRONG_UNROLL 0
+#endif
+constexpr int kStrongUnroll = DPE_STRONG_UNROLL;
 
 // All per-call read-only data (cameras, relative poses, params, buffer pointers).  It lives in a
 // small device buffer written once per call; kernels receive its address.

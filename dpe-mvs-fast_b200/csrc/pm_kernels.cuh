@@ -901,7 +901,7 @@ __device__ __forceinline__ void strong_p2(const CoopCtx &c, int iter) {
     pos = strong_search_edge(a, c.px, c.py, c.center, d, iter);
     if (pos >= 0) {
       flag = true;
-      ncc_all_sources<kStage>(a, c.px, c.py, G(a.plane_snap, pos, L, 205), rw, row);
+      ncc_all_sources<kStage, kStrongUnroll>(a, c.px, c.py, G(a.plane_snap, pos, L, 205), rw, row);
     }
     if (G(a.edge, c.center, L, 203) == 0) {
       const float good_thr = 0.8f * dpe_expf((float)(iter * iter) / (-90.0f));
@@ -922,7 +922,7 @@ __device__ __forceinline__ void strong_p2(const CoopCtx &c, int iter) {
       if (mc < FLT_MAX) {
         flag = true;
         float tca[kMaxSrc];
-        ncc_all_sources<kStage>(a, c.px, c.py, G(a.plane_snap, mp, L, 205), rw, tca);
+        ncc_all_sources<kStage, kStrongUnroll>(a, c.px, c.py, G(a.plane_snap, mp, L, 205), rw, tca);
         int g0 = 0, g1 = 0, b0 = 0, b1 = 0;
         for (int j = 0; j < n; ++j) {
           if (row[j] < good_thr) g0++;
@@ -940,7 +940,7 @@ __device__ __forceinline__ void strong_p2(const CoopCtx &c, int iter) {
     pos = c.P->pos[d];
     if (pos >= 0) {
       flag = true;
-      ncc_all_sources<kStage>(a, c.px, c.py, G(a.plane, pos, L, 210), rw, row);
+      ncc_all_sources<kStage, kStrongUnroll>(a, c.px, c.py, G(a.plane, pos, L, 210), rw, row);
     }
   }
   c.P->flag[d] = flag ? 1 : 0;
@@ -994,7 +994,7 @@ __device__ __forceinline__ void strong_p4(const CoopCtx &c) {
   const int na = c.P->na;
   const float4 pl = c.P->pl_cur;
   for (int q = c.lane; q < na; q += kCoopLanes)
-    c.hc[q] = ncc_strong<kStage>(*c.a, c.px, c.py, c.P->act[q] + 1, pl, rw);
+    c.hc[q] = ncc_strong<kStage, kStrongUnroll>(*c.a, c.px, c.py, c.P->act[q] + 1, pl, rw);
 }
 
 // Phase 5 (lane 0): the current cost, candidate acceptance, and the five refinement planes of
@@ -1052,7 +1052,7 @@ __device__ __forceinline__ void strong_p6(const CoopCtx &c) {
   const int na = c.P->na, n = c.n;
   for (int i = c.lane; i < 5 * na; i += kCoopLanes) {
     const int h = i / na, q = i - h * na;
-    c.hc[(1 + h) * n + q] = ncc_strong<kStage>(*c.a, c.px, c.py, c.P->act[q] + 1, c.P->hyp[h], rw);
+    c.hc[(1 + h) * n + q] = ncc_strong<kStage, kStrongUnroll>(*c.a, c.px, c.py, c.P->act[q] + 1, c.P->hyp[h], rw);
   }
 }
 
@@ -1576,78 +1576,168 @@ __global__ void k_filter_strong(const Launch lc, int parity) {
   a.plane[center].w = (k % 2 == 0) ? (f[m - 1] + f[m]) / 2 : f[m];
 }
 
-// Common prologue of DepthToWeak / LocalRefine (DPE.cu:2619-2660, 2767-2806)
-struct Sweep {
+// ------------------------------------------------------------------ DepthToWeak / LocalRefine
+// Block-cooperative like the strong update: a block holds kCoopPix consecutive pixels of one row
+// and kCoopLanes threads per pixel.  The pixel's reference window and its per-sample costs live
+// in shared memory; the lanes split the depth samples (each sample's sum over the selected
+// sources stays on one lane, in source order), and one lane per pixel takes the decision.
+//   phase 0  window taps (lanes split the taps)
+//   phase 1  window sums and the sweep prologue (DPE.cu:2619-2660, 2767-2806) (lane 0)
+//   phase 2  sample costs (lanes split the samples; LocalRefine also the current plane's sources)
+//   phase 3  the decision (lane 0)
+struct SweepPixel {
+  float2 win[kWinTaps];
+  float rc[kWinTaps];
   float4 pl;
-  float depth, cost_now, base_line, weight_normal;
-  int valid;
-  uint32_t views;
   uint4 vw;
+  float center, inv_wsum, mean_r, var_r;
+  float depth, base_line, weight_normal, disp;
+  int act[kMaxSrc];
+  int na, ok;           // ok: the sweep runs for this pixel
+  float pc[64];         // DepthToWeak: the 61 sample costs
 };
-template <int kStage>
-__device__ __forceinline__ void sweep_setup(const PMArgs &a, int px, int py, const RefWindow &rw, Sweep &s) {
-  const int center = px + py * a.W;
-  s.pl = normal_to_ref(a.cam[0], a.plane[center]);
-  s.depth = s.pl.w;
-  s.cost_now = 0.0f; s.base_line = 0.0f; s.weight_normal = 0.0f; s.valid = 0;
-  s.views = a.views[center];
-  s.vw = a.vweight[center];
-  if (s.depth == 0) return;
+constexpr int kSweepPhases = 4;
+// LocalRefine's shared bytes: the pixels, then per pixel 12 planes (the current one, then the 11
+// samples) x n = N - 1 sources of (NCC, geometric cost).
+__host__ __device__ inline size_t local_refine_smem_bytes(int n) {
+  return sizeof(SweepPixel) * kCoopPix + sizeof(float2) * (size_t)kCoopPix * 12 * n;
+}
+
+struct SweepCtx {
+  const PMArgs *a;
+  int slot, lane, px, py, center;
+  bool live;  // inside the image
+  SweepPixel *P;
+  float2 *items;  // LocalRefine: [12][n] (NCC, geometric cost) of this pixel
+  int kid;
+  __device__ __forceinline__ SmemWindow window() const {
+    return SmemWindow{P->win, P->center, P->inv_wsum, P->mean_r, P->var_r, a->counters ? a->counters + 2 * kid : nullptr};
+  }
+};
+__device__ __forceinline__ SweepCtx sweep_ctx(const Launch &lc, void *smem, int kid) {
+  const Blk B = resolve<kGridFull>(lc);
+  SweepCtx c;
+  c.a = B.a;
+  c.slot = (int)threadIdx.x / kCoopLanes;
+  c.lane = (int)threadIdx.x % kCoopLanes;
+  c.px = B.x * kCoopPix + c.slot;
+  c.py = B.y;
+  c.center = c.py * B.a->W + c.px;
+  c.live = c.px < B.a->W && c.py < B.a->H;
+  c.P = static_cast<SweepPixel *>(smem) + c.slot;
+  c.items = reinterpret_cast<float2 *>(static_cast<SweepPixel *>(smem) + kCoopPix) + (size_t)c.slot * 12 * (B.a->N - 1);
+  c.kid = kid;
+  return c;
+}
+
+// Phase 0: the window taps, split over the lanes (as strong_p0).
+__device__ __forceinline__ void sweep_p0(const SweepCtx &c) {
+  if (!c.live) return;
+  const PMArgs &a = *c.a;
+  const int r = a.P.strong_radius, inc = a.P.strong_increment, side = 2 * r / inc + 1;
+  const float center = texel(a, 0, c.px, c.py);
+  for (int k = c.lane; k < side * side; k += kCoopLanes) {
+    const int i = -r + (k / side) * inc, j = -r + (k % side) * inc;
+    const float rp = texel(a, 0, c.px + i, c.py + j);
+    const float w = bilateral_weight((float)i, (float)j, rp, center, a.P.sigma_spatial, a.P.sigma_color);
+    const float rcv = rp - center;
+    G(c.P->win, k, kWinTaps, 320) = make_float2(w, w * rcv);
+    c.P->rc[k] = rcv;
+  }
+  if (c.lane == 0) c.P->center = center;
+}
+
+// Phase 1 (lane 0): window sums; the prologue's plane, baseline, weights and selected sources.
+// (The reference's DepthToWeak also costs the current plane here and never reads the result; it
+// is not computed.  LocalRefine's current cost is computed by the lanes in phase 2.)
+__device__ __forceinline__ void sweep_p1(const SweepCtx &c) {
+  if (!c.live || c.lane != 0) return;
+  const PMArgs &a = *c.a;
+  SweepPixel &P = *c.P;
+  const int r = a.P.strong_radius, inc = a.P.strong_increment, side = 2 * r / inc + 1;
+  float sw = 0.f, swr = 0.f, swrr = 0.f;
+  for (int k = 0; k < side * side; ++k) {
+    const float2 t = P.win[k];
+    sw += t.x; swr += t.y; swrr += t.y * P.rc[k];
+  }
+  P.inv_wsum = 1.0f / sw;
+  P.mean_r = swr * P.inv_wsum;
+  P.var_r = swrr * P.inv_wsum - P.mean_r * P.mean_r;
+  P.pl = normal_to_ref(a.cam[0], a.plane[c.center]);
+  P.depth = P.pl.w;
+  const uint32_t views = a.views[c.center];
+  P.vw = a.vweight[c.center];
+  float base_line = 0.0f, weight_normal = 0.0f;
+  int valid = 0, na = 0;
   for (int si = 1; si < a.N; ++si) {
     const int vi = si - 1;
-    if (!isSet(s.views, vi)) continue;
-    float4 t = s.pl;
-    t.w = dist_to_origin(a.cam[0], px, py, s.depth, t);
-    float tc = ncc_strong<kStage, kSweepUnroll>(a, px, py, si, t, rw);
-    if (a.P.geom_consistency) tc += a.P.geom_factor * geom_cost(a, px, py, si, t);
-    const int w = vweight_at(s.vw, vi);
-    s.cost_now += tc * w;
-    s.weight_normal += w;
+    if (!isSet(views, vi)) continue;
+    weight_normal += vweight_at(P.vw, vi);
     const float d0 = a.cam[0].c[0] - a.cam[si].c[0], d1 = a.cam[0].c[1] - a.cam[si].c[1], d2 = a.cam[0].c[2] - a.cam[si].c[2];
     const double tv = d0 * d0 + d1 * d1 + d2 * d2;
-    s.base_line += sqrtf((float)tv);
-    s.valid++;
+    base_line += sqrtf((float)tv);
+    valid++;
+    P.act[na++] = vi;
+  }
+  P.na = na;
+  P.ok = P.depth != 0 && valid != 0;
+  P.weight_normal = weight_normal;
+  if (P.ok) {
+    P.base_line = base_line / valid;
+    P.disp = a.cam[0].K[0] * P.base_line / P.depth;
   }
 }
 
-// DepthToWeak (DPE.cu:2597-2751)
-template <int kStage>
-__global__ void __launch_bounds__(128, DPE_COST_MIN_BLOCKS) k_depth_to_weak(const Launch lc) {
-  const Blk B = resolve<kGridFull>(lc);
-  const PMArgs &a = *B.a;
-  int px, py;
-  if (!full_pixel(a, B, &px, &py)) return;
-  const int W = a.W, H = a.H, center = px + py * W, margin = 6;
-  if (px < margin || py < margin || px >= W - margin || py >= H - margin) { a.weak[center] = DPE_UNKNOWN; return; }
-  const dpe_camera &rc = a.cam[0];
-  DPE_REF_WINDOW(rw);
-  build_ref_window(a, px, py, rw, KID_DEPTH_TO_WEAK);
-  Sweep s;
-  sweep_setup<kStage>(a, px, py, rw, s);
-  if (s.depth == 0 || s.valid == 0) { a.weak[center] = DPE_UNKNOWN; return; }
-  s.cost_now /= s.weight_normal;
-  s.base_line /= s.valid;
-  const float disp = rc.K[0] * s.base_line / s.depth;
-  int act[kMaxSrc];  // selected sources, ascending
-  int na = 0;
-  for (int vi = 0; vi < a.N - 1; ++vi)
-    if (isSet(s.views, vi)) act[na++] = vi;
-  constexpr int R = 30, NS = 61;
-  float pc[NS];
-  for (int pd = -R; pd <= R; ++pd) {
-    const float pdep = rc.K[0] * s.base_line / (disp + pd);
-    if (pdep < a.P.depth_min || pdep > a.P.depth_max) { pc[pd + R] = 2.0f; continue; }
-    float4 t = s.pl;
-    t.w = dist_to_origin(rc, px, py, pdep, t);
-    float cost = 0.0f;
-    for (int q = 0; q < na; ++q) {
-      float tc = ncc_strong<kStage, kSweepUnroll>(a, px, py, act[q] + 1, t, rw);
-      if (a.P.geom_consistency) tc += a.P.geom_factor * geom_cost(a, px, py, act[q] + 1, t);
-      cost += tc * vweight_at(s.vw, act[q]);
+// Cost of the plane of depth pdep: the weighted sum over the selected sources (DPE.cu:2676-2700,
+// 2815-2828), summed in source order.  kLocal: LocalRefine's association (each term weighted).
+template <int kStage, bool kLocal>
+__device__ __forceinline__ float sweep_sample(const SweepCtx &c, const SmemWindow &rw, float pdep) {
+  const PMArgs &a = *c.a;
+  const SweepPixel &P = *c.P;
+  float4 t = P.pl;
+  t.w = dist_to_origin(a.cam[0], c.px, c.py, pdep, t);
+  float cost = 0.0f;
+  for (int q = 0; q < P.na; ++q) {
+    const int vi = P.act[q];
+    const int w = vweight_at(P.vw, vi);
+    if (kLocal) {
+      cost += ncc_strong<kStage, kSweepUnroll>(a, c.px, c.py, vi + 1, t, rw) * w;
+      if (a.P.geom_consistency) cost += a.P.geom_factor * geom_cost(a, c.px, c.py, vi + 1, t) * w;
+    } else {
+      float tc = ncc_strong<kStage, kSweepUnroll>(a, c.px, c.py, vi + 1, t, rw);
+      if (a.P.geom_consistency) tc += a.P.geom_factor * geom_cost(a, c.px, c.py, vi + 1, t);
+      cost += tc * w;
     }
-    cost /= s.weight_normal;
-    pc[pd + R] = cvmin(2.0f, cost);
   }
+  return cost;
+}
+
+// DepthToWeak (DPE.cu:2597-2751), phases 2 and 3.
+template <int kStage>
+__device__ __forceinline__ void d2w_p2(const SweepCtx &c) {
+  if (!c.live || !c.P->ok) return;
+  const PMArgs &a = *c.a;
+  const SmemWindow rw = c.window();
+  constexpr int R = 30, NS = 61;
+  for (int s = c.lane; s < NS; s += kCoopLanes) {
+    const int pd = s - R;
+    const float pdep = a.cam[0].K[0] * c.P->base_line / (c.P->disp + pd);
+    float v = 2.0f;
+    if (!(pdep < a.P.depth_min || pdep > a.P.depth_max))
+      v = cvmin(2.0f, sweep_sample<kStage, false>(c, rw, pdep) / c.P->weight_normal);
+    c.P->pc[s] = v;
+  }
+}
+__device__ __forceinline__ void d2w_p3(const SweepCtx &c) {
+  if (!c.live || c.lane != 0) return;
+  const PMArgs &a = *c.a;
+  const int W = a.W, H = a.H, margin = 6;
+  const float *pc = c.P->pc;
+  if (c.px < margin || c.py < margin || c.px >= W - margin || c.py >= H - margin || !c.P->ok) {
+    a.weak[c.center] = DPE_UNKNOWN;
+    return;
+  }
+  constexpr int R = 30, NS = 61;
   int peaks = 0, min_peak = 0;
   float min_cost = 2.0f;
   uint64_t peak_mask = 0;
@@ -1667,48 +1757,128 @@ __global__ void __launch_bounds__(128, DPE_COST_MIN_BLOCKS) k_depth_to_weak(cons
     var /= (peaks - 1);
     res = var > 0.2f ? DPE_STRONG : DPE_WEAK;
   }
-  a.weak[center] = res;
+  a.weak[c.center] = res;
+}
+// The margin pixels take no window or sweep: phase 0 and 1 skip them through `live` as well.
+__device__ __forceinline__ SweepCtx d2w_ctx(const Launch &lc, void *smem) {
+  SweepCtx c = sweep_ctx(lc, smem, KID_DEPTH_TO_WEAK);
+  const int margin = 6;
+  if (c.live && (c.px < margin || c.py < margin || c.px >= c.a->W - margin || c.py >= c.a->H - margin)) {
+    if (c.lane == 0) c.a->weak[c.center] = DPE_UNKNOWN;
+    c.live = false;
+  }
+  return c;
 }
 
-// LocalRefine (DPE.cu:2753-2839)
+// LocalRefine (DPE.cu:2753-2839), phases 2 and 3.  Phase 2 evaluates every (plane, selected
+// source) pair as one item, split over the lanes: plane 0 is the current one (the prologue's
+// cost), planes 1..11 the disparity samples -5..5; items of samples out of the depth range are
+// not evaluated.  Phase 3 sums them in the reference's order.
+__device__ __forceinline__ float lr_sample_depth(const PMArgs &a, const SweepPixel &P, int pd) {
+  return a.cam[0].K[0] * P.base_line / (P.disp + pd);
+}
 template <int kStage>
-__global__ void __launch_bounds__(128, DPE_COST_MIN_BLOCKS) k_local_refine(const Launch lc) {
-  const Blk B = resolve<kGridFull>(lc);
-  const PMArgs &a = *B.a;
-  int px, py;
-  if (!full_pixel(a, B, &px, &py)) return;
-  const int center = px + py * a.W;
-  const dpe_camera &rc = a.cam[0];
-  DPE_REF_WINDOW(rw);
-  build_ref_window(a, px, py, rw, KID_LOCAL_REFINE);
-  Sweep s;
-  sweep_setup<kStage>(a, px, py, rw, s);
-  if (s.depth == 0) return;
-  if (s.weight_normal == 0 || s.valid == 0) return;
-  s.cost_now /= s.weight_normal;
-  s.base_line /= s.valid;
-  const float disp = rc.K[0] * s.base_line / s.depth;
-  int act[kMaxSrc];  // selected sources, ascending
-  int na = 0;
-  for (int vi = 0; vi < a.N - 1; ++vi)
-    if (isSet(s.views, vi)) act[na++] = vi;
-  float min_cost = 2.0f, best = s.depth;
+__device__ __forceinline__ void lr_p2(const SweepCtx &c) {
+  if (!c.live || !c.P->ok) return;
+  const PMArgs &a = *c.a;
+  const SweepPixel &P = *c.P;
+  const SmemWindow rw = c.window();
+  const int na = P.na, n = a.N - 1;
+  const bool geom = a.P.geom_consistency != 0;
+  for (int i = c.lane; i < 12 * na; i += kCoopLanes) {
+    const int h = i / na, q = i - h * na;
+    float pdep = P.depth;
+    if (h > 0) {
+      pdep = lr_sample_depth(a, P, h - 6);
+      if (pdep < a.P.depth_min || pdep > a.P.depth_max) continue;
+    }
+    float4 t = P.pl;
+    t.w = dist_to_origin(a.cam[0], c.px, c.py, pdep, t);
+    const int si = P.act[q] + 1;
+    const float ncc = ncc_strong<kStage, kSweepUnroll>(a, c.px, c.py, si, t, rw);
+    c.items[h * n + q] = make_float2(ncc, geom ? geom_cost(a, c.px, c.py, si, t) : 0.0f);
+  }
+}
+__device__ __forceinline__ void lr_p3(const SweepCtx &c) {
+  if (!c.live || c.lane != 0 || !c.P->ok) return;
+  const PMArgs &a = *c.a;
+  const SweepPixel &P = *c.P;
+  if (P.weight_normal == 0) return;
+  const int na = P.na, n = a.N - 1;
+  const bool geom = a.P.geom_consistency != 0;
+  float cost_now = 0.0f;
+  for (int q = 0; q < na; ++q) {
+    const float2 e = c.items[q];
+    float tc = e.x;
+    if (geom) tc += a.P.geom_factor * e.y;
+    cost_now += tc * vweight_at(P.vw, P.act[q]);
+  }
+  cost_now /= P.weight_normal;
+  float min_cost = 2.0f, best = P.depth;
   for (int pd = -5; pd <= 5; ++pd) {
-    const float pdep = rc.K[0] * s.base_line / (disp + pd);
+    const float pdep = lr_sample_depth(a, P, pd);
     if (pdep < a.P.depth_min || pdep > a.P.depth_max) continue;
-    float4 t = s.pl;
-    t.w = dist_to_origin(rc, px, py, pdep, t);
+    const float2 *row = c.items + (pd + 6) * n;
     float tc = 0.0f;
     for (int q = 0; q < na; ++q) {
-      const int vi = act[q];
-      const int w = vweight_at(s.vw, vi);
-      tc += ncc_strong<kStage, kSweepUnroll>(a, px, py, vi + 1, t, rw) * w;
-      if (a.P.geom_consistency) tc += a.P.geom_factor * geom_cost(a, px, py, vi + 1, t) * w;
+      const int w = vweight_at(P.vw, P.act[q]);
+      tc += row[q].x * w;
+      if (geom) tc += a.P.geom_factor * row[q].y * w;
     }
-    tc /= s.weight_normal;
+    tc /= P.weight_normal;
     if (tc < min_cost) { min_cost = tc; best = pdep; }
   }
-  if ((double)(s.cost_now - min_cost) > 0.1) a.plane[center].w = best;
+  if ((double)(cost_now - min_cost) > 0.1) a.plane[c.center].w = best;
+}
+
+// One phase for one thread (host builds run the phases in lock-step over a block).
+template <int kStage>
+__device__ __forceinline__ void depth_to_weak_phase(int phase, const Launch &lc, void *smem) {
+  const SweepCtx c = d2w_ctx(lc, smem);
+  switch (phase) {
+    case 0: sweep_p0(c); break;
+    case 1: sweep_p1(c); break;
+    case 2: d2w_p2<kStage>(c); break;
+    default: d2w_p3(c); break;
+  }
+}
+template <int kStage>
+__device__ __forceinline__ void local_refine_phase(int phase, const Launch &lc, void *smem) {
+  const SweepCtx c = sweep_ctx(lc, smem, KID_LOCAL_REFINE);
+  switch (phase) {
+    case 0: sweep_p0(c); break;
+    case 1: sweep_p1(c); break;
+    case 2: lr_p2<kStage>(c); break;
+    default: lr_p3(c); break;
+  }
+}
+
+// Grid: ((W + 15) / 16, H) blocks of kCoopThreads.
+template <int kStage>
+__global__ void __launch_bounds__(kCoopThreads, DPE_SWEEP_MIN_BLOCKS) k_depth_to_weak(const Launch lc) {
+  __shared__ SweepPixel sp[kCoopPix];
+  const SweepCtx c = d2w_ctx(lc, sp);
+  sweep_p0(c);
+  __syncthreads();
+  sweep_p1(c);
+  __syncthreads();
+  d2w_p2<kStage>(c);
+  __syncthreads();
+  d2w_p3(c);
+}
+// LocalRefine: the same grid, local_refine_smem_bytes(N - 1) dynamic shared bytes.
+template <int kStage>
+__global__ void __launch_bounds__(kCoopThreads, DPE_COST_MIN_BLOCKS) k_local_refine(const Launch lc) {
+  extern __shared__ float4 lr_smem[];
+  const SweepCtx c = sweep_ctx(lc, lr_smem, KID_LOCAL_REFINE);
+  sweep_p0(c);
+  __syncthreads();
+  sweep_p1(c);
+  __syncthreads();
+  lr_p2<kStage>(c);
+  __syncthreads();
+  lr_p3(c);
 }
 
 }  // namespace dpe
+

@@ -182,8 +182,11 @@ extern "C" int host_pm_run(const dpe_problem *p, dpe_pm_out *out) {
   }
   launch(fg, fb, k_get_depth_normal, one);
   for (int parity = 0; parity < 2; ++parity) launch(hg, hb, k_filter_strong, one, parity);
-  launch(fg, fb, k_depth_to_weak<DPE_STAGE_FP32>, one);
-  launch(fg, fb, k_local_refine<DPE_STAGE_FP32>, one);
+  const dim3 sg((W + kCoopPix - 1) / kCoopPix, H);
+  launch_phased(sg, dim3(kCoopThreads), sizeof(SweepPixel) * kCoopPix, kSweepPhases,
+                [&](int ph, void *sm) { depth_to_weak_phase<DPE_STAGE_FP32>(ph, one, sm); });
+  launch_phased(sg, dim3(kCoopThreads), local_refine_smem_bytes(N - 1), kSweepPhases,
+                [&](int ph, void *sm) { local_refine_phase<DPE_STAGE_FP32>(ph, one, sm); });
   memcpy(out->plane, a.plane, L * 16);
   memcpy(out->weak, a.weak, L);
   memcpy(out->selected_views, a.views, L * 4);
