@@ -120,15 +120,20 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+# DRAM bytes per launch of the cost kernels on this workload: ncu dram__bytes_read.sum +
+# dram__bytes_write.sum over every launch of one complete schedule (a 1-pass capture of
+# `dpe-mvs-fast_b200/profile_case.py --scene c2 --levels 3 --repeat 1`), averaged over the launches
+# the way `roofline.achieved` averages FLOP over them.  Measured, not modelled: re-captured when a
+# kernel changes.
+DRAM_BYTES_PER_LAUNCH = {
+    "k_strong_update": 130.1e6,
+    "k_depth_to_weak": 162.6e6,
+}
+
+
 def _traffic_for(kernel: str):
-    path = os.path.join(ROOT, "profiles", "dram_traffic.json")
-    if not os.path.exists(path):
-        return None
-    try:
-        data = json.load(open(path))
-        return data.get("kernels", {}).get(kernel, {}).get("bytes_per_launch_full_workload")
-    except Exception:
-        return None
+    v = DRAM_BYTES_PER_LAUNCH.get(kernel)
+    return int(v) if v is not None else None
 
 
 def cpu_sample(threads: int = 0):
