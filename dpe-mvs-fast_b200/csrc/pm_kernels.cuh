@@ -696,22 +696,46 @@ __device__ __forceinline__ void gn_hypothesis(const PMArgs &a, int px, int py, c
 // the random draws and the order of each weighted sum are those of one thread doing it all.
 //
 // Phases, separated by block barriers:
-//   0  window taps (lanes split the taps)           4  current plane's costs (lanes split sources)
-//   1  window sums (lane 0); candidate search       5  candidate acceptance, refinement planes (lane 0)
-//   2  candidate costs (lane d: candidate d)        6  refinement costs (lanes split plane x source)
-//   3  view sampling, best candidate (lane 0)       7  refinement decisions, outputs (lane 0)
+//   0  window taps (lanes split the taps)
+//   1  window sums (lane 0); candidate search (lane d: direction d)
+//   2  candidate costs (lane d: candidate d)
+//   3  view-selection probabilities per source and the 15 uniform draws (lanes split them)
+//   4  view sampling from the draws, in order (lane 0)
+//   5  candidates' weighted costs (lane d) and the current plane's costs (lanes split sources)
+//   6  best candidate, acceptance, refinement planes (lane 0)
+//   7  refinement costs (lanes split plane x source)
+//   8  refinement decisions, outputs (lane 0)
 constexpr int kCoopPix = 16, kCoopLanes = 8, kCoopThreads = kCoopPix * kCoopLanes;
+
+// The strong NCC as the cooperative strong update calls it, inlined at each call site (measured:
+// one shared out-of-line copy, which would ease the instruction cache, is 10 % slower).
+template <int kStage>
+__device__ __forceinline__ float coop_ncc(const PMArgs &a, int px, int py, int s, float4 pl, const SmemWindow &rw) {
+  return ncc_strong<kStage, kStrongUnroll>(a, px, py, s, pl, rw);
+}
+template <int kStage>
+__device__ __forceinline__ void coop_ncc_all(const PMArgs &a, int px, int py, float4 pl, const SmemWindow &rw, float *out) {
+  for (int j = 0; j < a.N - 1; ++j) out[j] = coop_ncc<kStage>(a, px, py, j + 1, pl, rw);
+}
 
 // Decision state of one pixel, in shared memory.
 struct CoopPixel {
   float2 win[kWinTaps];  // (w, w * (r - c)) per tap
-  float rc[kWinTaps];    // r - c per tap
-  float4 pl_cur, pl_now, hyp[5];
+  union {
+    float rc[kWinTaps];     // phases 0-1: r - c per tap
+    float probs[kMaxSrc];   // phases 3-4: view-selection probability per source
+  };
+  union {
+    float4 hyp[5];          // phases 6-8: the refinement planes
+    float u[16];            // phases 3-4: the 15 uniform draws of the view sampling
+    float fc[8];            // phases 5-6: the candidates' weighted costs
+  };
+  float4 pl_cur, pl_now;
   float center, inv_wsum, mean_r, var_r;
-  float wn, cost_now, cost_written, depth_now, fcost_mi;
+  float wn, cost_now, cost_written, depth_now;
   int pos[8];
   int act[kMaxSrc];
-  int na, mi;
+  int na;
   uint32_t views_new, temp_sel, rng_ctr;
   uint8_t flag[8];
   uint8_t vw[32];
@@ -901,7 +925,7 @@ __device__ __forceinline__ void strong_p2(const CoopCtx &c, int iter) {
     pos = strong_search_edge(a, c.px, c.py, c.center, d, iter);
     if (pos >= 0) {
       flag = true;
-      ncc_all_sources<kStage, kStrongUnroll>(a, c.px, c.py, G(a.plane_snap, pos, L, 205), rw, row);
+      coop_ncc_all<kStage>(a, c.px, c.py, G(a.plane_snap, pos, L, 205), rw, row);
     }
     if (G(a.edge, c.center, L, 203) == 0) {
       const float good_thr = 0.8f * dpe_expf((float)(iter * iter) / (-90.0f));
@@ -922,7 +946,7 @@ __device__ __forceinline__ void strong_p2(const CoopCtx &c, int iter) {
       if (mc < FLT_MAX) {
         flag = true;
         float tca[kMaxSrc];
-        ncc_all_sources<kStage, kStrongUnroll>(a, c.px, c.py, G(a.plane_snap, mp, L, 205), rw, tca);
+        coop_ncc_all<kStage>(a, c.px, c.py, G(a.plane_snap, mp, L, 205), rw, tca);
         int g0 = 0, g1 = 0, b0 = 0, b1 = 0;
         for (int j = 0; j < n; ++j) {
           if (row[j] < good_thr) g0++;
@@ -940,66 +964,105 @@ __device__ __forceinline__ void strong_p2(const CoopCtx &c, int iter) {
     pos = c.P->pos[d];
     if (pos >= 0) {
       flag = true;
-      ncc_all_sources<kStage, kStrongUnroll>(a, c.px, c.py, G(a.plane, pos, L, 210), rw, row);
+      coop_ncc_all<kStage>(a, c.px, c.py, G(a.plane, pos, L, 210), rw, row);
     }
   }
   c.P->flag[d] = flag ? 1 : 0;
   c.P->pos[d] = pos;
 }
 
-// Phase 3 (lane 0): view-selection priors and sampling, the best candidate, the sampled sources.
+// Phase 3: the view-selection probability of each source (sample_views' first loop, with the
+// priors of DPE.cu:1551-1563), lane j taking sources j, j + 8, ...; and the 15 uniform draws of
+// the sampling (counter-based, so draw s is the pixel's counter + s), split over the lanes.
 __device__ __forceinline__ void strong_p3(const CoopCtx &c, int iter) {
-  if (!c.live || c.lane != 0) return;
+  if (!c.live) return;
   const PMArgs &a = *c.a;
   const int W = a.W, n = c.n, center = c.center;
-  [[maybe_unused]] const long long L = (long long)W * a.H;
+  const long long L = (long long)W * a.H;
   CoopPixel &P = *c.P;
-  float priors[kMaxSrc], probs[kMaxSrc];
-  for (int j = 0; j < n; ++j) priors[j] = 0.0f;
+  const uint32_t ctr0 = G(a.rng_ctr, center, L, 106);
+  for (int s = c.lane; s < 15; s += kCoopLanes) {
+    Rng r{a.key[0], a.key[1], (uint32_t)center, ctr0 + (uint32_t)s};
+    P.u[s] = r.uniform();
+  }
   const long total = (long)W * a.H;
   const long nbr[4] = {(long)center - W, (long)center + W, (long)center - 1, (long)center + 1};
+  uint32_t sv[4];
   for (int i = 0; i < 4; ++i)
-    if (P.flag[2 * i]) {
-      const uint32_t sv = (nbr[i] >= 0 && nbr[i] < total) ? G(a.views, nbr[i], L, 211) : 0u;
-      for (int j = 0; j < n; ++j) priors[j] += isSet(sv, j) == 1 ? 0.9f : 0.1f;
+    sv[i] = (P.flag[2 * i] && nbr[i] >= 0 && nbr[i] < total) ? G(a.views, nbr[i], L, 211) : 0u;
+  const float thr = (float)(0.8 * (double)dpe_expf((float)(iter * iter) / (-90.0f)));
+  const float base = dpe_expf(thr * thr / (-0.32f));
+  for (int j = c.lane; j < n; j += kCoopLanes) {
+    float prior = 0.0f;
+    for (int i = 0; i < 4; ++i)
+      if (P.flag[2 * i]) prior += isSet(sv[i], j) == 1 ? 0.9f : 0.1f;
+    float count = 0;
+    int count_false = 0;
+    float tmpw = 0;
+    for (int d = 0; d < 8; ++d) {
+      const float v = c.cost[d * n + j];
+      if (v < thr) { tmpw += dpe_expf(v * v / (-0.18f)); count++; }
+      if (v > 1.2f) count_false++;
     }
-  Rng rng = make_rng(a, center);
-  uint32_t temp_sel = 0;
-  const float wn = sample_views(a, rng, iter, c.cost, n, priors, P.vw, &temp_sel, probs);
-  float final_costs[8];
-  for (int i = 0; i < 8; ++i) {
-    float fc = 0.0f;
-    for (int j = 0; j < n; ++j)
-      if (P.vw[j] > 0) fc += P.vw[j] * c.cost[i * n + j];
-    final_costs[i] = fc / wn;
+    float p = 0.0f;
+    if (count > 2 && count_false < 3) p = tmpw / count;
+    else if (count_false < 3) p = base;
+    P.probs[j] = p * prior;
   }
-  const int mi = find_min_cost_index(final_costs, 8);
+  if (c.lane == 0) {
+    P.rng_ctr = ctr0 + 15;
+    P.pl_cur = G(a.plane, center, L, 212);
+  }
+}
+
+// Phase 4 (lane 0): the rest of sample_views (normalised cumulative probabilities, the 15
+// samples, the selection mask and weight sum) and the list of sampled sources.
+__device__ __forceinline__ void strong_p4(const CoopCtx &c) {
+  if (!c.live || c.lane != 0) return;
+  const int n = c.n;
+  CoopPixel &P = *c.P;
+  for (int i = 0; i < 32; ++i) P.vw[i] = 0;
+  float sum = 0.0f;
+  for (int i = 0; i < n; ++i) sum += P.probs[i];
+  const float inv = 1.0f / sum;
+  float cum = 0.0f;
+  for (int i = 0; i < n; ++i) { cum += P.probs[i] * inv; P.probs[i] = cum; }
+  for (int s = 0; s < 15; ++s) {
+    const float r = P.u[s] - FLT_EPSILON;
+    for (int id = 0; id < n; ++id)
+      if (P.probs[id] > r) { P.vw[id] += 1; break; }
+  }
+  uint32_t sel = 0;
+  float wn = 0;
   int na = 0;
   for (int i = 0; i < n; ++i)
-    if (P.vw[i] > 0) P.act[na++] = i;
+    if (P.vw[i] > 0) { setBit(&sel, i); wn += P.vw[i]; P.act[na++] = i; }
   P.na = na;
-  P.mi = mi;
-  P.fcost_mi = final_costs[mi];
   P.wn = wn;
-  P.temp_sel = temp_sel;
-  P.rng_ctr = rng.ctr;
-  P.pl_cur = G(a.plane, center, L, 212);
+  P.temp_sel = sel;
 }
 
-// Phase 4: the current plane's cost against each sampled source (lanes split the sources).
+// Phase 5: candidate d's cost weighted by the samples (lane d), then the current plane's cost
+// against each sampled source (lanes split the sources).
 template <int kStage>
-__device__ __forceinline__ void strong_p4(const CoopCtx &c) {
+__device__ __forceinline__ void strong_p5(const CoopCtx &c) {
   if (!c.live) return;
+  CoopPixel &P = *c.P;
+  const int n = c.n, d = c.lane;
+  float fc = 0.0f;
+  for (int j = 0; j < n; ++j)
+    if (P.vw[j] > 0) fc += P.vw[j] * c.cost[d * n + j];
+  P.fc[d] = fc / P.wn;
   const SmemWindow rw = c.window();
-  const int na = c.P->na;
-  const float4 pl = c.P->pl_cur;
+  const int na = P.na;
+  const float4 pl = P.pl_cur;
   for (int q = c.lane; q < na; q += kCoopLanes)
-    c.hc[q] = ncc_strong<kStage, kStrongUnroll>(*c.a, c.px, c.py, c.P->act[q] + 1, pl, rw);
+    c.hc[q] = coop_ncc<kStage>(*c.a, c.px, c.py, P.act[q] + 1, pl, rw);
 }
 
-// Phase 5 (lane 0): the current cost, candidate acceptance, and the five refinement planes of
-// PlaneHypothesisRefinementStrong (DPE.cu:1069-1122) with their random draws.
-__device__ __forceinline__ void strong_p5(const CoopCtx &c) {
+// Phase 6 (lane 0): the current cost, the best candidate and its acceptance, and the five
+// refinement planes of PlaneHypothesisRefinementStrong (DPE.cu:1069-1122) with their draws.
+__device__ __forceinline__ void strong_p6(const CoopCtx &c) {
   if (!c.live || c.lane != 0) return;
   const PMArgs &a = *c.a;
   const dpe_camera &rc = a.cam[0];
@@ -1014,12 +1077,13 @@ __device__ __forceinline__ void strong_p5(const CoopCtx &c) {
   float depth_now = depth_from_plane(rc, pl_cur, c.px, c.py);
   float4 pl_now = pl_cur;
   uint32_t views_new = G(a.views, c.center, L, 213);
-  const int mi = P.mi;
+  const int mi = find_min_cost_index(P.fc, 8);
+  const float fcost_mi = P.fc[mi];
   if (P.flag[mi]) {
     const float4 cand = G(a.P.use_edge ? a.plane_snap : a.plane, P.pos[mi], L, 214);
     const float db = depth_from_plane(rc, cand, c.px, c.py);
-    if (db >= a.P.depth_min && db <= a.P.depth_max && P.fcost_mi < cost_now) {
-      depth_now = db; pl_now = cand; cost_now = P.fcost_mi;
+    if (db >= a.P.depth_min && db <= a.P.depth_max && fcost_mi < cost_now) {
+      depth_now = db; pl_now = cand; cost_now = fcost_mi;
       views_new = P.temp_sel;
     }
   }
@@ -1044,21 +1108,21 @@ __device__ __forceinline__ void strong_p5(const CoopCtx &c) {
   P.rng_ctr = rng.ctr;
 }
 
-// Phase 6: the refinement planes' costs, (plane, sampled source) pairs split over the lanes.
+// Phase 7: the refinement planes' costs, (plane, sampled source) pairs split over the lanes.
 template <int kStage>
-__device__ __forceinline__ void strong_p6(const CoopCtx &c) {
+__device__ __forceinline__ void strong_p7(const CoopCtx &c) {
   if (!c.live) return;
   const SmemWindow rw = c.window();
   const int na = c.P->na, n = c.n;
   for (int i = c.lane; i < 5 * na; i += kCoopLanes) {
     const int h = i / na, q = i - h * na;
-    c.hc[(1 + h) * n + q] = ncc_strong<kStage, kStrongUnroll>(*c.a, c.px, c.py, c.P->act[q] + 1, c.P->hyp[h], rw);
+    c.hc[(1 + h) * n + q] = coop_ncc<kStage>(*c.a, c.px, c.py, c.P->act[q] + 1, c.P->hyp[h], rw);
   }
 }
 
-// Phase 7 (lane 0): the refinement decisions in order, the optional Gauss-Newton plane, outputs.
+// Phase 8 (lane 0): the refinement decisions in order, the optional Gauss-Newton plane, outputs.
 template <int kStage, bool kGN>
-__device__ __forceinline__ void strong_p7(const CoopCtx &c) {
+__device__ __forceinline__ void strong_p8(const CoopCtx &c) {
   if (!c.live || c.lane != 0) return;
   const PMArgs &a = *c.a;
   const dpe_camera &rc = a.cam[0];
@@ -1100,13 +1164,14 @@ __device__ __forceinline__ void strong_update_phase(int phase, const Launch &lc,
     case 1: strong_p1(c); break;
     case 2: strong_p2<kStage>(c, iter); break;
     case 3: strong_p3(c, iter); break;
-    case 4: strong_p4<kStage>(c); break;
-    case 5: strong_p5(c); break;
-    case 6: strong_p6<kStage>(c); break;
-    default: strong_p7<kStage, kGN>(c); break;
+    case 4: strong_p4(c); break;
+    case 5: strong_p5<kStage>(c); break;
+    case 6: strong_p6(c); break;
+    case 7: strong_p7<kStage>(c); break;
+    default: strong_p8<kStage, kGN>(c); break;
   }
 }
-constexpr int kStrongPhases = 8;
+constexpr int kStrongPhases = 9;
 
 // Grid: ((W + 15) / 16, (H + 1) / 2) blocks of kCoopThreads; coop_smem_bytes(N - 1) dynamic shared
 // bytes (the largest N of a batch).
@@ -1122,13 +1187,15 @@ __global__ void __launch_bounds__(kCoopThreads, DPE_STRONG_MIN_BLOCKS) k_strong_
   __syncthreads();
   strong_p3(c, iter);
   __syncthreads();
-  strong_p4<kStage>(c);
+  strong_p4(c);
   __syncthreads();
-  strong_p5(c);
+  strong_p5<kStage>(c);
   __syncthreads();
-  strong_p6<kStage>(c);
+  strong_p6(c);
   __syncthreads();
-  strong_p7<kStage, kGN>(c);
+  strong_p7<kStage>(c);
+  __syncthreads();
+  strong_p8<kStage, kGN>(c);
 }
 
 
