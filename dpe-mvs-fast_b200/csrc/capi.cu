@@ -247,6 +247,7 @@ namespace {
 // names suffixed with its index, so problems never share state.
 struct ProblemState {
   PMArgs a;
+  int staging = DPE_STAGE_FP32;  // the storage the cost kernels sample this problem's sources from
   const float4 *plane_in = nullptr;
   const uint32_t *views_in = nullptr;
   const uint8_t *weak_in = nullptr;
@@ -280,15 +281,12 @@ int setup_problem(dpe_ctx *ctx, const dpe_problem *p, int index, ProblemState *p
   for (int i = 1; i < N; ++i) relative_pose(a.cam[0], a.cam[i], a.Rrel[i], a.trel[i]);
   a.key[0] = (uint32_t)p->seed;
   a.key[1] = (uint32_t)(p->seed >> 32);
-  a.stage = ctx->opt.staging;
   a.gn = ctx->opt.gn_refine;
   ps->L = L;
   ps->wcap = (L + 1) / 2;  // pixels of one colour
 
   // ---- device buffers
   float *img_pad = get((float *)0, "img_pad", PL * N);
-  const int staging = ctx->opt.staging;
-  uint32_t *img_pairs = staging != DPE_STAGE_FP32 ? get((uint32_t *)0, "img_pairs", PL * N) : nullptr;
   float *stage = host ? get((float *)0, "img_stage", L * N) : nullptr;
   a.plane = get((float4 *)0, "plane", L);
   a.plane_snap = get((float4 *)0, "plane_snap", L);
@@ -397,7 +395,29 @@ int setup_problem(dpe_ctx *ctx, const dpe_problem *p, int index, ProblemState *p
     a.img[i] = img_pad + PL * i;
     k_pad_image<<<dim3((W + 2 + 31) / 32, (H + 2 + 7) / 8), dim3(32, 8), 0, s>>>(src, img_pad + PL * i, W, H);
     PM_LAUNCHED("k_pad_image", s);
-    if (i > 0 && staging != DPE_STAGE_FP32) {
+  }
+  // FP32 staging: when every source texel is exact in BF16 (8-bit images, the finest pyramid
+  // level), the cost kernels sample BF16 pairs instead: the same values, half the gather bytes.
+  int staging = ctx->opt.staging;
+  if (staging == DPE_STAGE_FP32 && N > 1) {
+    unsigned *flag = get((unsigned *)0, "bf16_flag", 1);
+    if (!flag) return DPE_ERR_OUT_OF_MEMORY;
+    DPE_TRY(cudaMemsetAsync(flag, 0, sizeof(unsigned), s));
+    const long long n = (long long)PL * (N - 1);
+    const unsigned blocks = (unsigned)std::max(1LL, std::min((n + 255) / 256, (long long)ctx->sms * 8));
+    k_bf16_exact<<<blocks, 256, 0, s>>>(img_pad + PL, n, flag);
+    PM_LAUNCHED("k_bf16_exact", s);
+    unsigned inexact = 1;
+    DPE_TRY(cudaMemcpyAsync(&inexact, flag, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    DPE_TRY(cudaStreamSynchronize(s));
+    if (!inexact) staging = DPE_STAGE_BF16;
+  }
+  ps->staging = staging;
+  a.stage = staging;
+  uint32_t *img_pairs = staging != DPE_STAGE_FP32 ? get((uint32_t *)0, "img_pairs", PL * N) : nullptr;
+  if (staging != DPE_STAGE_FP32 && !img_pairs) return DPE_ERR_OUT_OF_MEMORY;
+  for (int i = 1; i < N; ++i) {
+    if (staging != DPE_STAGE_FP32) {
       a.pair[i] = img_pairs + PL * i;
       if (staging == DPE_STAGE_BF16)
         k_stage_pairs<true><<<(unsigned)((PL + 255) / 256), 256, 0, s>>>(img_pad + PL * i, img_pairs + PL * i, (long long)PL);
@@ -426,7 +446,10 @@ int run_sequence(dpe_ctx *ctx, ProblemState *ps, int n, const PMArgs *d_args, co
   cudaStream_t s = ctx->stream;
   Arena &A = ctx->arena;
   const dpe_params &P = ps[0].a.P;
-  const int staging = ctx->opt.staging;
+  // one staging for the sequence: BF16 pairs only when every problem has them
+  int staging = ps[0].staging;
+  for (int b = 1; b < n; ++b)
+    if (ps[b].staging != staging) staging = ctx->opt.staging;
   const bool gn = ctx->opt.gn_refine != 0;
   DPE_TIMED(ctx, KID_INIT_STATE, s, for (int b = 0; b < n; ++b) {
     // k_init_state takes per-problem inputs: one launch per problem

@@ -95,6 +95,15 @@ __global__ void k_stage_pairs(const float *__restrict__ pad, uint32_t *__restric
   out[o] = a | (b << 16);
 }
 
+// Sets *flag when any of the n floats is not exact in BF16 (a float is exact when its low 16
+// bits are zero: 8-bit images are).  One atomic per block.
+__global__ void k_bf16_exact(const float *__restrict__ p, long long n, unsigned *flag) {
+  unsigned bits = 0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    bits |= __float_as_uint(p[i]) & 0xFFFFu;
+  if (__syncthreads_or(bits != 0) && threadIdx.x == 0) atomicOr(flag, 1u);
+}
+
 __global__ void k_init_state(const Launch lc, const float4 *plane_in, const uint32_t *views_in,
                              const uint8_t *weak_in, int *weak_flag) {
   const Blk B = resolve<kGridFull>(lc);

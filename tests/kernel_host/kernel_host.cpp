@@ -36,6 +36,8 @@ template <class T> static inline T __ldg(const T *p) { return *p; }
 // Kernels with block barriers run here only through launch_phased (their phases in lock-step); a
 // sequential launch of one would ignore its barriers, so the stand-in refuses to run.
 static inline void __syncthreads() { std::abort(); }
+static inline int __syncthreads_or(int) { std::abort(); }
+static inline unsigned atomicOr(unsigned *, unsigned) { std::abort(); }
 // the device's correctly rounded, never-contracted arithmetic intrinsics
 static inline float __fmul_rn(float a, float b) { volatile float r = a * b; return r; }
 static inline float __fadd_rn(float a, float b) { volatile float r = a + b; return r; }
