@@ -126,8 +126,9 @@ class ClockSampler:
 # the way `roofline.achieved` averages FLOP over them.  Measured, not modelled: re-captured when a
 # kernel changes.
 DRAM_BYTES_PER_LAUNCH = {
-    "k_strong_update": 130.1e6,
-    "k_depth_to_weak": 162.6e6,
+    "k_strong_update": 121.3e6,
+    "k_depth_to_weak": 73.7e6,
+    "k_local_refine": 72.1e6,
 }
 
 
