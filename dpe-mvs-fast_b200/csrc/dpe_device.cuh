@@ -704,9 +704,9 @@ __device__ __forceinline__ void ncc_all_sources(const PMArgs &a, int px, int py,
   for (int j = 0; j < a.N - 1; ++j) out[j] = ncc_strong<kStage, kUnroll>(a, px, py, j + 1, pl, rw);
 }
 // Sum over the listed sources act[0..na) (ascending) of vw[j] * cost(j), in list order.
-template <int kStage, class RW>
+template <int kStage, class RW, class A>
 __device__ __forceinline__ float weighted_ncc(const PMArgs &a, int px, int py, float4 pl, const RW &rw,
-                                             const int *act, int na, const uint8_t *vw) {
+                                             const A *act, int na, const uint8_t *vw) {
   float tc = 0.0f;
   for (int q = 0; q < na; ++q) tc += vw[act[q]] * ncc_strong<kStage>(a, px, py, act[q] + 1, pl, rw);
   return tc;

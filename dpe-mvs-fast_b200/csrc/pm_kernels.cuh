@@ -641,8 +641,8 @@ __device__ __forceinline__ int find_min_cost_index(const float *c, int n) {
 // equations  (J^T V J + lambda diag(J^T V J)) theta = -J^T V c  (V = the sample counts).  The
 // resulting plane is a hypothesis like the random ones: kept only when its cost is lower and its
 // depth lies in range.  It draws no random numbers, so the rest of the update is unchanged.
-template <int kStage, class RW>
-__device__ __forceinline__ void gn_hypothesis(const PMArgs &a, int px, int py, const RW &rw, const int *act,
+template <int kStage, class RW, class A>
+__device__ __forceinline__ void gn_hypothesis(const PMArgs &a, int px, int py, const RW &rw, const A *act,
                                               int na, const uint8_t *vw, float wn, float4 *pl_now, float *depth_now,
                                               float *cost_now) {
   const dpe_camera &rc = a.cam[0];
@@ -743,7 +743,7 @@ struct CoopPixel {
   float center, inv_wsum, mean_r, var_r;
   float wn, cost_now, cost_written, depth_now;
   int pos[8];
-  int act[kMaxSrc];
+  uint8_t act[32];  // the sampled sources (source index - 1), ascending
   int na;
   uint32_t views_new, temp_sel, rng_ctr;
   uint8_t flag[8];
