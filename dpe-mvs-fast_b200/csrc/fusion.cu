@@ -33,7 +33,11 @@ struct FuseView {
   const uint8_t *block;
   uint8_t *mask;
   int *acc_min;  // per pixel: smallest accepted contender of the current reference view
-  int *und_min;  // per pixel: smallest undecided contender in the current wave
+  // per pixel: smallest undecided contender of the current wave, as (stamp << 32 | pixel) with
+  // stamp = 0xFFFFFFFF - wave number (counted over the whole call): a wave's keys are smaller
+  // than every earlier wave's, so no reset between waves is needed, and an entry belongs to the
+  // current wave exactly when its stamp is the current one.
+  unsigned long long *und_min;
   dpe_camera cam;
 };
 
@@ -146,15 +150,19 @@ __global__ void k_entries(const __grid_constant__ FuseArgs f) {
   f.status[pix] = st;
 }
 
-__global__ void k_mark_undecided(const __grid_constant__ FuseArgs f, int npix) {
+// One wave, first half: every undecided pixel stamps itself on the source pixels it would use.
+// Also clears the wave's count of undecided pixels (k_decide, next in the stream, counts them).
+__global__ void k_mark_undecided(const __grid_constant__ FuseArgs f, int npix, unsigned stamp) {
   const int pix = blockIdx.x * blockDim.x + threadIdx.x;
+  if (pix == 0) *f.remaining = 0;
   if (pix >= npix || f.status[pix] != 0) return;
   const int *eq = f.entry_q + (size_t)pix * f.ns;
+  const unsigned long long key = ((unsigned long long)stamp << 32) | (unsigned)pix;
   for (int j = 0; j < f.ns; ++j)
-    if (eq[j] >= 0) atomicMin(&f.views[f.src[j]].und_min[eq[j]], pix);
+    if (eq[j] >= 0) atomicMin(&f.views[f.src[j]].und_min[eq[j]], key);
 }
 
-__global__ void k_decide(const __grid_constant__ FuseArgs f, int npix) {
+__global__ void k_decide(const __grid_constant__ FuseArgs f, int npix, unsigned stamp) {
   const FuseView &V = f.views[f.ref];
   const int pix = blockIdx.x * blockDim.x + threadIdx.x;
   if (pix >= npix || f.status[pix] != 0) return;
@@ -167,7 +175,11 @@ __global__ void k_decide(const __grid_constant__ FuseArgs f, int npix) {
     if (eq[j] < 0) continue;
     const FuseView &S = f.views[f.src[j]];
     if (S.acc_min[eq[j]] < pix) continue;  // masked by an earlier accepted pixel of this view
-    if (S.und_min[eq[j]] < pix) { atomicAdd(f.remaining, 1); return; }  // an earlier contender is undecided
+    const unsigned long long u = S.und_min[eq[j]];
+    if ((unsigned)(u >> 32) == stamp && (int)(unsigned)u < pix) {  // an earlier contender is undecided
+      atomicAdd(f.remaining, 1);
+      return;
+    }
     n++;
     dyn_d += es[j];
     dyn_f += (float)es[j];
@@ -431,6 +443,7 @@ __global__ void k_tat_emit(const __grid_constant__ TatArgs t, const int *offsets
 // per-view decision and scan buffers, and the point output.
 struct FuseBuffers {
   std::vector<FuseView> hv;
+  unsigned wave = 0;  // waves run in this call (the undecided markers' stamps)
   FuseView *d_views = nullptr;
   size_t max_pix = 0, total_pix = 0;
   int max_ns = 1;
@@ -475,7 +488,9 @@ static int fuse_prepare(dpe_ctx *ctx, const dpe_fusion_in *in, const dpe_fusion_
   B.hv.resize(nv);
   uint8_t *masks = A.get<uint8_t>("f_mask", total_pix);
   int *acc = A.get<int>("f_acc", total_pix);
-  int *und = A.get<int>("f_und", total_pix);
+  unsigned long long *und = A.get<unsigned long long>("f_und", total_pix);
+  // all ones: the stamp of wave 0, older than every wave of this call
+  if (und) DPE_TRY(cudaMemsetAsync(und, 0xFF, total_pix * sizeof(unsigned long long), ctx->stream));
   float *d_depth = host ? A.get<float>("f_depth", total_pix) : nullptr;
   float *d_normal = host ? A.get<float>("f_normal", total_pix * 3) : nullptr;
   uint8_t *d_weak = host && need_weak ? A.get<uint8_t>("f_weak", total_pix) : nullptr;
@@ -606,17 +621,18 @@ extern "C" int dpe_fuse(dpe_ctx *ctx, const dpe_fusion_in *in, dpe_fusion_out *o
     if (v.num_src > 0) {
       DPE_TIMED(ctx, KID_FUSE_ENTRIES, s, k_entries<<<blocks, 256, 0, s>>>(f));
       DPE_LAUNCHED("k_entries", s);
-      // waves until every candidate pixel is decided; each wave decides at least the first one
-      for (int wave = 0; wave < npix + 1; ++wave) {
-        for (int j = 0; j < v.num_src; ++j) {
-          const FuseView &S = B.hv[v.src_views[j]];
-          DPE_TRY(cudaMemsetAsync(S.und_min, 0x7F, (size_t)S.W * S.H * 4, s));
+      // waves until every candidate pixel is decided; each wave decides at least the first one.
+      // The count of the last wave is read every kWaveBatch waves: waves after the last decision
+      // find no undecided pixel and change nothing.
+      constexpr int kWaveBatch = 8;
+      for (int wave = 0; wave < npix + 1; wave += kWaveBatch) {
+        for (int k = 0; k < kWaveBatch; ++k) {
+          const unsigned stamp = 0xFFFFFFFFu - (unsigned)(++B.wave);
+          DPE_TIMED(ctx, KID_FUSE_WAVES, s, k_mark_undecided<<<blocks, 256, 0, s>>>(f, npix, stamp));
+          DPE_LAUNCHED("k_mark_undecided", s);
+          DPE_TIMED(ctx, KID_FUSE_WAVES, s, k_decide<<<blocks, 256, 0, s>>>(f, npix, stamp));
+          DPE_LAUNCHED("k_decide", s);
         }
-        DPE_TRY(cudaMemsetAsync(remaining, 0, 4, s));
-        DPE_TIMED(ctx, KID_FUSE_WAVES, s, k_mark_undecided<<<blocks, 256, 0, s>>>(f, npix));
-        DPE_LAUNCHED("k_mark_undecided", s);
-        DPE_TIMED(ctx, KID_FUSE_WAVES, s, k_decide<<<blocks, 256, 0, s>>>(f, npix));
-        DPE_LAUNCHED("k_decide", s);
         int rem = 0;
         DPE_TRY(cudaMemcpyAsync(&rem, remaining, 4, cudaMemcpyDeviceToHost, s));
         DPE_TRY(cudaStreamSynchronize(s));
