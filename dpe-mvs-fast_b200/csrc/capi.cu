@@ -900,6 +900,15 @@ std::mutex g_static_mu;
 unsigned char *g_static_addr[kMaxDevices] = {};
 
 size_t round256(size_t b) { return (b + 255) & ~size_t(255); }
+
+// Writes the call's argument block into the static scratch.  The block travels as a kernel
+// parameter (captured by value at launch), so no host buffer has to outlive the call.
+__global__ void k_store_args(const __grid_constant__ PMArgs a, PMArgs *dst) {
+  static_assert(sizeof(PMArgs) % 4 == 0, "argument block is copied as 32-bit words");
+  const uint32_t *s = reinterpret_cast<const uint32_t *>(&a);
+  uint32_t *d = reinterpret_cast<uint32_t *>(dst);
+  for (int i = threadIdx.x; i < (int)(sizeof(PMArgs) / 4); i += blockDim.x) d[i] = s[i];
+}
 }  // namespace
 
 extern "C" int dpe_ncc_eval_noalloc(const dpe_ncc_query *q, float *costs_out, void *stream) {
@@ -947,7 +956,8 @@ extern "C" int dpe_ncc_eval_noalloc(const dpe_ncc_query *q, float *costs_out, vo
   unsigned char *img_base = base + round256(sizeof(PMArgs));
   for (int i = 0; i < N; ++i) a.img[i] = reinterpret_cast<const float *>(img_base + (size_t)i * img_bytes);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  DPE_TRY(cudaMemcpyAsync(base, &a, sizeof(PMArgs), cudaMemcpyHostToDevice, s));
+  k_store_args<<<1, 256, 0, s>>>(a, reinterpret_cast<PMArgs *>(base));
+  DPE_LAUNCHED("k_store_args", s);
   for (int i = 0; i < N; ++i) {
     k_pad_image<<<dim3((W + 2 + 31) / 32, (H + 2 + 7) / 8), dim3(32, 8), 0, s>>>(
         q->images[i], reinterpret_cast<float *>(img_base + (size_t)i * img_bytes), W, H);

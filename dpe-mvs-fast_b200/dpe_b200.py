@@ -523,20 +523,36 @@ def ncc_eval_noalloc(images, cameras, params: Params, px, py, src, planes, costs
     import torch
 
     lib = lib or load_library()
+    if not 2 <= len(images) <= MAX_IMAGES or len(cameras) != len(images):
+        raise ValueError(f"need 2..{MAX_IMAGES} images and one camera per image")
+    if images[0].dim() != 2:
+        raise ValueError("images must be 2-D (H, W) tensors")
+    shape, device = tuple(images[0].shape), images[0].device
     q = NCCQuery()
-    q.height, q.width = int(images[0].shape[0]), int(images[0].shape[1])
+    q.height, q.width = int(shape[0]), int(shape[1])
     q.num_images = len(images)
     for i, im in enumerate(images):
         if not (im.is_cuda and im.dtype == torch.float32 and im.is_contiguous()):
             raise ValueError("images must be contiguous float32 CUDA tensors")
+        if tuple(im.shape) != shape or im.device != device:
+            raise ValueError(f"image {i} has shape {tuple(im.shape)} on {im.device}; every image must be "
+                             f"{shape} on {device}")
         q.images[i] = im.data_ptr()
         q.cameras[i] = make_camera(cameras[i])
     q.params = params
-    for t, dt in ((px, torch.int32), (py, torch.int32), (src, torch.int32), (planes, torch.float32),
-                  (costs_out, torch.float32)):
+    n = int(px.numel())
+    for name, t, dt, want in (("px", px, torch.int32, (n,)), ("py", py, torch.int32, (n,)),
+                              ("src", src, torch.int32, (n,)), ("planes", planes, torch.float32, (n, 4)),
+                              ("costs_out", costs_out, torch.float32, (n,))):
         if not (t.is_cuda and t.dtype == dt and t.is_contiguous()):
             raise ValueError("queries and output must be contiguous CUDA tensors of the documented types")
-    q.count = int(px.numel())
+        if tuple(t.shape) != want:
+            raise ValueError(f"{name} has shape {tuple(t.shape)}, expected {want}")
+        if t.device != device:
+            raise ValueError(f"{name} is on {t.device}, the images on {device}")
+    if device != torch.device("cuda", torch.cuda.current_device()):
+        raise ValueError(f"the tensors are on {device}, the current device is cuda:{torch.cuda.current_device()}")
+    q.count = n
     q.px, q.py, q.src, q.plane = px.data_ptr(), py.data_ptr(), src.data_ptr(), planes.data_ptr()
     s = (stream or torch.cuda.current_stream()).cuda_stream
     st = lib.dpe_ncc_eval_noalloc(C.byref(q), C.c_void_p(costs_out.data_ptr()), C.c_void_p(s))

@@ -154,12 +154,14 @@ typedef struct dpe_fusion_out {
   float gpu_ms;
 } dpe_fusion_out;
 
-/* ---- NCC evaluation at explicit (pixel, plane, source) queries ---- */
+/* ---- NCC evaluation at explicit (pixel, plane, source) queries ----
+ * The memory space of every pointer below is set by the entry point that takes the query:
+ * host memory for dpe_ncc_eval and dpe_ncc_grad, device memory for dpe_ncc_eval_noalloc. */
 typedef struct dpe_ncc_query {
   int width;
   int height;
   int num_images;
-  const float *images[DPE_MAX_IMAGES];  /* host memory */
+  const float *images[DPE_MAX_IMAGES];  /* W*H float images; memory space: see above */
   dpe_camera cameras[DPE_MAX_IMAGES];
   dpe_params params;                    /* strong_radius/increment, sigmas */
   int64_t count;
@@ -328,10 +330,12 @@ int dpe_edge_labels(dpe_ctx *ctx, const uint8_t *gray, int width, int height, in
 int dpe_scene_run(dpe_ctx *ctx, const dpe_scene *scene, const dpe_schedule *schedule, dpe_scene_out *out);
 
 /* Strong bilateral NCC (ComputeBilateralNCCOld, DPE.cu:696-782) at explicit queries; test and
- * measurement entry point. */
+ * measurement entry point.  Every pointer of `q` and `costs_out` is HOST memory; the call copies
+ * the inputs to the context's device and returns after the costs are back on the host. */
 int dpe_ncc_eval(dpe_ctx *ctx, const dpe_ncc_query *q, float *costs_out);
 
-/* Adjoint of dpe_ncc_eval: the strong NCC and its gradient at explicit queries (host buffers).
+/* Adjoint of dpe_ncc_eval: the strong NCC and its gradient at explicit queries.  Every pointer
+ * of `q` and every output buffer is HOST memory, as for dpe_ncc_eval.
  * The reference has no gradient; this is the differentiable form of ComputeBilateralNCCOld
  * (DPE.cu:696-782) for plane refinement and autograd harnesses.
  *   grad_plane_out        [count][4] dC/d(nx, ny, nz, w) of the query's plane (n, w) in

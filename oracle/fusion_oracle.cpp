@@ -3,10 +3,10 @@
 // (DPE.cpp:1720-1867).
 //
 // TEST INFRASTRUCTURE ONLY: the checker for the fusion kernels.
-// PARITY UNPINNED: the reference ships no tests or known-answer vectors for this path, and its
-// sources need the OpenCV and Boost C++ libraries, which are not available to build it, so
-// this restatement is checked against its own FP64 mode and the committed golden fixtures, not
-// against outputs of the reference itself.
+// PARITY PINNED to the reference itself: the float mode gives the same points, coordinates and
+// colours bit for bit as the reference's own RunFusion compiled for the CPU (oracle/_ref, driven
+// by oracle/ref_harness.cpp; tests/test_ref_oracle.py).  The TAT variants are checked against an
+// independent numpy restatement (tests/test_fusion_tat.py) and their golden fixtures.
 // The loop order is the
 // reference's: views in pair.txt order, pixels in raster order, sources in list order, with the
 // consumed-pixel masks updated as points are accepted, so the result depends on that order

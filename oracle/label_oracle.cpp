@@ -22,8 +22,8 @@
 //   - line (thickness 1, 8-connected): the Bresenham iterator from the left end.
 // PINNED against the dependency itself: tests/test_labels.py compares every part and the whole
 // map with the host preprocessing, which calls cv2 as the reference calls OpenCV, bit for bit.
-// The reference's own code is not built here (it needs OpenCV to build), so the Roberts and
-// Connect restatements are PARITY UNPINNED beyond a line-by-line Python restatement.
+// Roberts and Connect are the reference's own functions: tests/test_ref_oracle.py pins this
+// Connect and the host preprocessing's Roberts to them, compiled for the CPU (oracle/_ref).
 #include <cmath>
 #include <cstdint>
 #include <vector>

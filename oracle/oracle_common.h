@@ -3,9 +3,9 @@
 // The oracle is the checker for the CUDA path: only tests/, __graft_entry__.smoke() and the
 // cpu_baseline leg of bench.py may load it.  It is never part of the product path.
 //
-// Parity status: no golden vectors exist in the reference (it has no tests); the oracle is a
-// restatement of the reference algorithm (DPE.cu, DPE.cpp) and is pinned against the
-// reference's own kernels only where those were run on a B200 (see oracle/ref_harness).
+// Parity status: the reference has no tests or golden vectors; the oracle restates its algorithm
+// (DPE.cu, DPE.cpp) and is pinned bit for bit to the reference's own code compiled for the CPU
+// (oracle/_ref, oracle/ref_harness.cpp, tests/test_ref_oracle.py).
 #ifndef DPE_ORACLE_COMMON_H_
 #define DPE_ORACLE_COMMON_H_
 

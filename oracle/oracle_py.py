@@ -45,6 +45,8 @@ def load() -> C.CDLL:
                                          C.c_void_p]
     lib.oracle_edge_labels.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int]
     lib.oracle_set_raw_moments.argtypes = [C.c_int]
+    lib.oracle_set_ref_addressing.argtypes = [C.c_int]
+    lib.oracle_set_serial_race.argtypes = [C.c_int]
     lib.oracle_ncc_strong_grad.argtypes = [C.POINTER(D.NCCQuery), C.c_void_p, C.c_void_p, C.c_void_p]
     _lib = lib
     return lib
@@ -53,6 +55,25 @@ def load() -> C.CDLL:
 def set_raw_moments(on: bool) -> None:
     """Select the reference's raw-moment NCC arithmetic (default: compensated, shifted moments)."""
     load().oracle_set_raw_moments(1 if on else 0)
+
+
+def set_ref_addressing(on: bool) -> None:
+    """Sample positions pass through the reference's tex2D(x + 0.5, y + 0.5) rounding (default: sampled
+    at x, the CUDA kernels' addressing)."""
+    load().oracle_set_ref_addressing(1 if on else 0)
+
+
+def set_serial_race(on: bool) -> None:
+    """Resolve the edge-aware update's same-colour read race (Q1) as a serial raster-order run does
+    (default: a snapshot taken before each colour pass, the CUDA kernels' resolution)."""
+    load().oracle_set_serial_race(1 if on else 0)
+
+
+def reference_arithmetic(on: bool) -> None:
+    """Raw moments and the reference's texture addressing together: the arithmetic of the reference's
+    own DPE.cu, for bit-for-bit comparison with its host build (oracle/ref_py.py)."""
+    set_raw_moments(on)
+    set_ref_addressing(on)
 
 
 def philox(ctr, key) -> np.ndarray:

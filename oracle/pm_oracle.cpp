@@ -1,19 +1,23 @@
 // pm_oracle.cpp -- CPU restatement of the reference's per-view PatchMatch (DPE.cu:1-3262).
 //
 // TEST INFRASTRUCTURE ONLY: the checker for the CUDA kernels in dpe-mvs-fast_b200/csrc.
-// PARITY UNPINNED: the reference ships no tests or known-answer vectors for this path, and its
-// sources need the OpenCV and Boost C++ libraries, which are not available to build it, so
-// this restatement is checked against published vectors (Philox), its own FP64 evaluation and
-// the committed golden fixtures, not against outputs of the reference itself.
+// PARITY PINNED to the reference itself: the reference's own DPE.cu and DPE.cpp compiled for the
+// CPU (oracle/_ref, built by oracle/Makefile behind the stand-ins of oracle/refshim) produce the
+// same bits as this restatement on the first-init, weak-texture and geometric paths when the
+// switches below select the reference's arithmetic (oracle_set_raw_moments,
+// oracle_set_ref_addressing, oracle_set_serial_race); tests/test_ref_oracle.py holds that.
 // Each function cites the reference lines it restates.  Semantics are FP32 without fast-math
 // (the reference build uses --use_fast_math, CMakeLists.txt:26; that rounding is not restated).
 // Red/black passes run in the reference's colour order; pixels of one colour are independent and
 // run in parallel with OpenMP.  Deviations from the reference, all documented:
 //   * random streams: Philox4x32-10 per pixel instead of clock64()-seeded XORWOW (DPE.cu:1036);
 //   * the same-colour read race of the edge-aware strong update (direction 4, DPE.cu:1279/1316)
-//     reads a snapshot of costs/planes taken before the colour pass;
-//   * texture reads are exact bilinear with clamp-to-edge addressing (the hardware path uses
-//     8-bit interpolation weights);
+//     reads a snapshot of costs/planes taken before the colour pass (oracle_set_serial_race
+//     selects the serial raster-order reading instead);
+//   * NCC moments are shifted by the window centre (oracle_set_raw_moments selects the raw ones);
+//   * texture reads are exact bilinear with clamp-to-edge addressing at x itself (the hardware
+//     path uses 8-bit interpolation weights; oracle_set_ref_addressing adds the rounding of the
+//     reference's tex2D(x + 0.5, y + 0.5) coordinate);
 //   * radius_cuda starts at strong_radius (the reference may read it uninitialised,
 //     DPE.cu:2950-2953 vs :624);
 //   * out-of-image linear indices read 0 (the reference reads outside its buffers in
@@ -30,6 +34,20 @@ namespace oracle {
 
 static const float kPi = 3.14159265358979323846f;
 
+// Texture addressing of the reference: its kernels sample tex2D(x + 0.5f, y + 0.5f) and the
+// texture unit blends around (u - 0.5, v - 0.5), so a sample position passes through one float
+// rounding of x + 0.5 (inexact when x + 0.5 changes binade or x has bits below its ulp).  The
+// default samples at x itself (the CUDA kernels' addressing); oracle_set_ref_addressing(1) adds
+// the round trip, for bit-for-bit comparisons with the reference's own code compiled for the CPU.
+static bool g_ref_addressing = false;
+
+// The same-colour read race of the edge-aware strong update (quirk Q1, DPE.cu:1279/1316): by
+// default the edge branch reads a snapshot taken before each colour pass (the CUDA kernels'
+// resolution).  oracle_set_serial_race(1) resolves it as a one-thread run in raster order does
+// instead -- the up-left same-colour candidate has already been updated when it is read -- which
+// is how the reference's own kernels behave when compiled for the CPU and run one thread at a time.
+static bool g_serial_race = false;
+
 struct Image {
   const float *data = nullptr;
   int w = 0, h = 0;
@@ -40,6 +58,11 @@ struct Image {
   }
   // tex2D(x + 0.5, y + 0.5) with linear filtering and clamp addressing, exact weights.
   float bilinear(float x, float y) const {
+    if (g_ref_addressing) {
+      volatile float u = x + 0.5f, v = y + 0.5f;
+      x = u - 0.5f;
+      y = v - 0.5f;
+    }
     const float xc = std::fmin(std::fmax(x, -1.0f), (float)(w - 1));
     const float yc = std::fmin(std::fmax(y, -1.0f), (float)(h - 1));
     const float fx = std::floor(xc), fy = std::floor(yc);
@@ -578,9 +601,11 @@ static void strong_update(Ctx &c, int px, int py, int iter) {
   bool flag[8] = {false};
   int positions[8] = {0};
   // candidate planes are read from `src_plane`/`src_cost`: the live arrays (non-edge branch, only
-  // opposite-colour pixels) or the pre-pass snapshot (edge branch, see header).
-  const std::vector<f4> &cand_plane = c.P.use_edge ? c.plane_snap : c.plane;
-  const std::vector<float> &cand_cost = c.P.use_edge ? c.cost_snap : c.cost;
+  // opposite-colour pixels) or the pre-pass snapshot (edge branch, see header).  With
+  // g_serial_race the edge branch reads the live arrays too, in a serial raster-order pass.
+  const bool snap = c.P.use_edge && !g_serial_race;
+  const std::vector<f4> &cand_plane = snap ? c.plane_snap : c.plane;
+  const std::vector<float> &cand_cost = snap ? c.cost_snap : c.cost;
 
   if (c.P.use_edge) {
     const s2 *en = &c.edge_neigh[(size_t)center * 8];
@@ -1506,6 +1531,10 @@ void oracle_philox(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]
 
 void oracle_set_raw_moments(int on) { g_raw_moments = on != 0; }
 
+void oracle_set_ref_addressing(int on) { g_ref_addressing = on != 0; }
+
+void oracle_set_serial_race(int on) { g_serial_race = on != 0; }
+
 // Strong NCC at explicit queries.  fp64 != 0 evaluates the cost in double precision end to end
 // (homography from the float cameras, exact bilinear, double exp/sqrt).
 void oracle_ncc_strong(const dpe_ncc_query *q, int fp64, double *out) {
@@ -1770,10 +1799,10 @@ int oracle_pm_run(const dpe_problem *pr, dpe_pm_out *out, int threads) {
   for_all(c, [&](int x, int y) { random_initialization(c, x, y); }, threads);
   for (int it = 0; it < c.P.max_iterations; ++it) {
     for (int colour = 0; colour < 2; ++colour) {
-      if (c.P.use_edge) { c.plane_snap = c.plane; c.cost_snap = c.cost; }
+      if (c.P.use_edge && !g_serial_race) { c.plane_snap = c.plane; c.cost_snap = c.cost; }
       for_colour(c, colour, [&](int x, int y) {
         if (c.weak[x + y * c.W] != DPE_WEAK) strong_update(c, x, y, it);
-      }, threads);
+      }, c.P.use_edge && g_serial_race ? 1 : threads);
     }
     for_all(c, [&](int x, int y) { ransac_fit_plane(c, x, y); }, threads);
     for (int colour = 0; colour < 2; ++colour)

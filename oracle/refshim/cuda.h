@@ -1,0 +1,2 @@
+// cuda.h -- host stand-in (TEST INFRASTRUCTURE): everything lives in cuda_runtime.h.
+#include "cuda_runtime.h"

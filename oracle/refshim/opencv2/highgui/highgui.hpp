@@ -1,0 +1,2 @@
+// opencv2/highgui/highgui.hpp -- host stand-in (TEST INFRASTRUCTURE): everything lives in opencv2/opencv.hpp.
+#include "../opencv.hpp"
