@@ -176,6 +176,19 @@ def default_params(lib: Optional[C.CDLL] = None) -> Params:
     return p
 
 
+def reference_default_params() -> Params:
+    """PatchMatchParams' member defaults (main.h:81-109) without loading the library (what
+    dpe_params_default returns; a CPU test holds the two equal)."""
+    p = Params()
+    for k, v in dict(max_iterations=3, num_images=5, sigma_spatial=5.0, sigma_color=3.0, top_k=4, depth_min=0.0,
+                     depth_max=1.0, geom_consistency=0, strong_radius=5, strong_increment=2, weak_radius=5,
+                     weak_increment=5, use_APD=1, use_edge=1, use_limit=1, use_label=1, use_radius=1, high_res_img=1,
+                     max_scale_size=1, scale_size=1, weak_peak_radius=2, rotate_time=4, ransac_threshold=0.005,
+                     geom_factor=0.2, state=FIRST_INIT).items():
+        setattr(p, k, v)
+    return p
+
+
 def make_camera(d: Dict) -> Camera:
     cam = Camera()
     for name in ("K", "R", "t", "c"):
@@ -427,7 +440,7 @@ class Context:
     def scene_run(self, gray, bgr, cameras, srcs, edges=None, labels=None, *, num_levels=0, refine_calls=3,
                   max_iterations=3, fuse_mode=FUSE_FP64, min_consistent=1, seed=1, memory=MEM_HOST,
                   want_maps=True, point_capacity=None, batch_views=False, device_edges=False,
-                  device_labels=False) -> Dict:
+                  device_labels=False, want_consistency=False) -> Dict:
         """The reference's full schedule over all views (dpe_scene_run).  gray[v]: (H, W) uint8,
         bgr[v]: (H, W, 3) uint8, cameras[v]: full-resolution camera dicts, srcs[v]: source view
         indices, edges[v][level] / labels[v][level]: per-level maps (level 0 = coarsest).
@@ -475,12 +488,16 @@ class Context:
         rgb = np.zeros((max(cap, 1), 3), np.uint8)
         so.fusion.capacity = cap
         so.fusion.xyz, so.fusion.bgr = _ptr(xyz), _ptr(rgb)
+        ncons = np.zeros(max(cap, 1), np.uint8) if want_consistency else None
+        so.fusion.num_consistent = _ptr(ncons)
         st = self.lib.dpe_scene_run(self.handle, C.byref(sc), C.byref(sch), C.byref(so))
         if st != OK:
             raise DPEError(st, "dpe_scene_run")
         n = int(so.fusion.count)
         res.update(points=n, xyz=xyz[:n], bgr=rgb[:n], gpu_ms=so.gpu_ms, fusion_ms=so.fusion_ms,
                    num_levels=so.num_levels, calls=so.calls)
+        if want_consistency:
+            res["num_consistent"] = ncons[:n]
         return res
 
     # ------------------------------------------------------------------ NCC queries

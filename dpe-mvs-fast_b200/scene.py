@@ -71,6 +71,9 @@ def preset(name: str) -> SceneSpec:
     if name == "c2_small":  # the c2 scene layout at 400x300 (coarse pyramid level)
         return SceneSpec(width=400, height=300, n_views=10, fx=328.125, fy=328.125, cx=200.0, cy=150.0,
                          n_planes=6, n_spheres=2, weak_sigma=3.0, tex_freq=15.0, supersample=1)
+    if name == "c2_200":  # the c2 scene layout at 200x150 (the CPU reference's timing sample)
+        return SceneSpec(width=200, height=150, n_views=10, fx=164.0625, fy=164.0625, cx=100.0, cy=75.0,
+                         n_planes=6, n_spheres=2, weak_sigma=3.0, tex_freq=7.5, supersample=1)
     raise ValueError(f"unknown scene preset {name!r}")
 
 

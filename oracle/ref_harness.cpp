@@ -167,9 +167,12 @@ const char *ref_last_error() { return g_error.c_str(); }
 // must be 1 (the images are given at the level's size).  With edges, pr->params.max_scale_size
 // names the low-resolution map's level when high_res_img is set.  radius_init 1 starts radius
 // at strong_radius (the oracle's deviation from the reference's uninitialised read); 0 leaves
-// the freshly allocated (zero) buffer.  Outputs: plane (float4 per pixel), weak, views, costs,
+// the freshly allocated (zero) buffer.  serial_race 1 runs the two edge-aware strong-update
+// kernels one thread at a time (a deterministic result, the one a serial run gives); 0 runs
+// every kernel's blocks in parallel, as for timing.  Outputs: plane (float4 per pixel), weak, views, costs,
 // and the cameras / params the reference used.  Returns 0, or 1 with ref_last_error().
-int ref_pm_call(const dpe_problem *pr, const char *work_dir, int threads, int radius_init, float *plane_out,
+int ref_pm_call(const dpe_problem *pr, const char *work_dir, int threads, int radius_init, int serial_race,
+                float *plane_out,
                 uint8_t *weak_out, uint32_t *views_out, float *costs_out, dpe_camera *cams_out,
                 dpe_params *params_out, long long *guard_writes) {
   try {
@@ -252,7 +255,10 @@ int ref_pm_call(const dpe_problem *pr, const char *work_dir, int threads, int ra
     // In the edge-aware branch a strong-update thread reads the cost and plane of an up-left
     // same-colour pixel that another thread of the launch may be writing (quirk Q1): those two
     // kernels run one thread at a time, so the result is the one of a serial run.
-    ref_set_serial_kernels({(const void *)&BlackPixelUpdateStrong, (const void *)&RedPixelUpdateStrong});
+    if (serial_race)
+      ref_set_serial_kernels({(const void *)&BlackPixelUpdateStrong, (const void *)&RedPixelUpdateStrong});
+    else
+      ref_set_serial_kernels({});
     ref_rng_configure(W, pr->seed);
     SceneCache cache(problem.dense_folder);
     DPE dpe(problem, &cache, &store, nullptr);

@@ -50,8 +50,8 @@ def load() -> C.CDLL:
         build()
     lib = C.CDLL(LIB_PATH)
     lib.ref_last_error.restype = C.c_char_p
-    lib.ref_pm_call.argtypes = [C.POINTER(D.Problem), C.c_char_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
-                                C.c_void_p, C.POINTER(D.Camera), C.POINTER(D.Params), C.POINTER(C.c_longlong)]
+    lib.ref_pm_call.argtypes = [C.POINTER(D.Problem), C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
+                                C.c_void_p, C.c_void_p, C.POINTER(D.Camera), C.POINTER(D.Params), C.POINTER(C.c_longlong)]
     lib.ref_fuse.argtypes = [C.POINTER(D.FusionIn), C.c_int, C.c_char_p, C.c_void_p, C.c_void_p, C.c_int64,
                              C.POINTER(C.c_int64)]
     lib.ref_set_texture_8bit_weights.argtypes = [C.c_int]
@@ -68,11 +68,13 @@ def set_texture_8bit_weights(on: bool) -> None:
 
 
 def pm_call(images, cameras, params, *, seed: int, threads: int = 0, radius_init: bool = True,
-            work_dir: str | None = None, **kw) -> Dict:
+            serial_race: bool = True, work_dir: str | None = None, **kw) -> Dict:
     """One per-view call of the reference (images: float32 arrays of integer grey levels; cameras:
     dicts with the cam-file depth range; params.scale_size 1).  Returns plane / weak / views /
     costs, the cameras and params the reference derived (`cameras`, `params`, ctypes structs), and
-    `guard_writes` (bytes the reference wrote just outside its buffers; 0 expected)."""
+    `guard_writes` (bytes the reference wrote just outside its buffers; 0 expected).
+    serial_race False runs the edge-aware strong update's blocks in parallel too (timing runs:
+    its same-colour read race then resolves by thread timing, as on a GPU)."""
     lib = load()
     pr = D.build_problem(images, cameras, params, seed=seed, **kw)
     H, W, N = pr.height, pr.width, pr.num_images
@@ -83,7 +85,8 @@ def pm_call(images, cameras, params, *, seed: int, threads: int = 0, radius_init
     guard = C.c_longlong(0)
     nthreads = threads if threads > 0 else (os.cpu_count() or 1)
     with tempfile.TemporaryDirectory(prefix="dpe_ref_", dir=work_dir) as tmp:
-        st = lib.ref_pm_call(C.byref(pr), tmp.encode(), nthreads, 1 if radius_init else 0, out["plane"].ctypes.data,
+        st = lib.ref_pm_call(C.byref(pr), tmp.encode(), nthreads, 1 if radius_init else 0, 1 if serial_race else 0,
+                             out["plane"].ctypes.data,
                              out["weak"].ctypes.data, out["views"].ctypes.data, out["costs"].ctypes.data, cams,
                              C.byref(used), C.byref(guard))
     if st != 0:

@@ -61,7 +61,10 @@ enum cudaMemcpyKind {
 };
 enum cudaChannelFormatKind { cudaChannelFormatKindSigned = 0, cudaChannelFormatKindUnsigned = 1, cudaChannelFormatKindFloat = 2 };
 struct cudaChannelFormatDesc { int x, y, z, w; enum cudaChannelFormatKind f; };
-struct cudaArray;  // a W x H float image (ref_runtime.cpp)
+struct cudaArray {  // a W x H float image
+  int w, h;
+  float *data;
+};
 typedef struct cudaArray *cudaArray_t;
 enum cudaResourceType { cudaResourceTypeArray = 0, cudaResourceTypeMipmappedArray = 1, cudaResourceTypeLinear = 2, cudaResourceTypePitch2D = 3 };
 struct cudaResourceDesc {
@@ -114,10 +117,43 @@ cudaError_t cudaPeekAtLastError();
 cudaError_t cudaGetLastError();
 const char *cudaGetErrorString(cudaError_t e);
 
-// Linear filtering of a 32-bit float texture with unnormalised coordinates: texel centres at
-// i + 0.5; coordinates outside the image address the edge texel (unnormalised coordinates do not
-// wrap).  Implemented in ref_runtime.cpp.
-float ref_tex2D_float(cudaTextureObject_t tex, float x, float y);
+// A texture object: the array, its filter mode and whether coordinates are normalised.
+struct RefTexture {
+  const cudaArray *arr;
+  enum cudaTextureFilterMode filter;
+  int normalized;
+};
+extern int g_ref_tex_8bit;  // 1: bilinear weights rounded to 8 fractional bits (the texture unit's)
+
+// Sampling with unnormalised coordinates (the reference's textures, DPE.cpp:1078-1097): the
+// sample at (u, v) blends the texels around (u - 0.5, v - 0.5); addresses beyond the image take
+// the edge texel (unnormalised coordinates do not wrap), which for linear filtering is the clamp
+// of the coordinate to [-1, size - 1] before the blend.  Weights are exact floats unless
+// g_ref_tex_8bit.
+inline float ref_texel(const cudaArray *a, int x, int y) {
+  x = x < 0 ? 0 : (x >= a->w ? a->w - 1 : x);
+  y = y < 0 ? 0 : (y >= a->h ? a->h - 1 : y);
+  return a->data[(size_t)y * a->w + x];
+}
+inline float ref_floorf(float v) { return __builtin_floorf(v); }
+inline float ref_tex2D_float(cudaTextureObject_t tex, float u, float v) {
+  const RefTexture *t = reinterpret_cast<const RefTexture *>((uintptr_t)tex);
+  const cudaArray *a = t->arr;
+  if (t->normalized) { u *= (float)a->w; v *= (float)a->h; }
+  if (t->filter == cudaFilterModePoint) return ref_texel(a, (int)ref_floorf(u), (int)ref_floorf(v));
+  const float x = u - 0.5f, y = v - 0.5f;
+  const float xc = __builtin_fminf(__builtin_fmaxf(x, -1.0f), (float)(a->w - 1));
+  const float yc = __builtin_fminf(__builtin_fmaxf(y, -1.0f), (float)(a->h - 1));
+  const float fx = ref_floorf(xc), fy = ref_floorf(yc);
+  const int x0 = (int)fx, y0 = (int)fy;
+  float ax = xc - fx, ay = yc - fy;
+  if (g_ref_tex_8bit) { ax = ref_floorf(ax * 256.0f + 0.5f) / 256.0f; ay = ref_floorf(ay * 256.0f + 0.5f) / 256.0f; }
+  const float v00 = ref_texel(a, x0, y0), v10 = ref_texel(a, x0 + 1, y0);
+  const float v01 = ref_texel(a, x0, y0 + 1), v11 = ref_texel(a, x0 + 1, y0 + 1);
+  const float top = (1.0f - ax) * v00 + ax * v10;
+  const float bot = (1.0f - ax) * v01 + ax * v11;
+  return (1.0f - ay) * top + ay * bot;
+}
 template <class T> T tex2D(cudaTextureObject_t tex, float x, float y);
 template <> inline float tex2D<float>(cudaTextureObject_t tex, float x, float y) { return ref_tex2D_float(tex, x, y); }
 

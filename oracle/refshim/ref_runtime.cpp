@@ -25,7 +25,7 @@ long long clock64() { return 0; }
 
 // ------------------------------------------------------------------ launches, textures, RNG
 static int g_launch_threads = 1;
-static int g_tex_8bit = 0;
+int g_ref_tex_8bit = 0;
 static int g_rng_width = 0;
 static uint32_t g_rng_key[2] = {0, 0};
 static std::vector<const void *> g_serial_kernels;
@@ -40,7 +40,7 @@ bool ref_launch_serial(const void *kernel) {
 void ref_set_serial_kernels(const std::vector<const void *> &kernels) { g_serial_kernels = kernels; }
 
 extern "C" void ref_set_launch_threads(int n) { g_launch_threads = n > 0 ? n : 1; }
-extern "C" void ref_set_texture_8bit_weights(int on) { g_tex_8bit = on != 0; }
+extern "C" void ref_set_texture_8bit_weights(int on) { g_ref_tex_8bit = on != 0; }
 
 void ref_rng_configure(int width, unsigned long long seed) {
   g_rng_width = width;
@@ -112,18 +112,6 @@ cudaError_t cudaMemset(void *dst, int value, size_t bytes) {
 }
 
 // ------------------------------------------------------------------ arrays and textures
-struct cudaArray {
-  int w = 0, h = 0;
-  std::vector<float> data;
-};
-namespace {
-struct Texture {
-  const cudaArray *arr;
-  cudaTextureFilterMode filter;
-  int normalized;
-};
-}  // namespace
-
 cudaChannelFormatDesc cudaCreateChannelDesc(int x, int y, int z, int w, enum cudaChannelFormatKind f) {
   cudaChannelFormatDesc d;
   d.x = x; d.y = y; d.z = z; d.w = w; d.f = f;
@@ -136,11 +124,12 @@ cudaError_t cudaMallocArray(cudaArray_t *array, const cudaChannelFormatDesc *des
   cudaArray *a = new cudaArray;
   a->w = (int)width;
   a->h = (int)(height ? height : 1);
-  a->data.assign((size_t)a->w * a->h, 0.0f);
+  a->data = new float[(size_t)a->w * a->h]();
   *array = a;
   return cudaSuccess;
 }
 cudaError_t cudaFreeArray(cudaArray_t array) {
+  if (array) delete[] array->data;
   delete array;
   return cudaSuccess;
 }
@@ -155,41 +144,13 @@ cudaError_t cudaMemcpy2DToArray(cudaArray_t dst, size_t w_offset, size_t h_offse
 cudaError_t cudaCreateTextureObject(cudaTextureObject_t *tex, const cudaResourceDesc *res, const cudaTextureDesc *desc,
                                     const cudaResourceViewDesc *) {
   if (res->resType != cudaResourceTypeArray) return cudaErrorInvalidValue;
-  Texture *t = new Texture{res->res.array.array, desc->filterMode, desc->normalizedCoords};
+  RefTexture *t = new RefTexture{res->res.array.array, desc->filterMode, desc->normalizedCoords};
   *tex = (cudaTextureObject_t)(uintptr_t)t;
   return cudaSuccess;
 }
 cudaError_t cudaDestroyTextureObject(cudaTextureObject_t tex) {
-  delete reinterpret_cast<Texture *>((uintptr_t)tex);
+  delete reinterpret_cast<RefTexture *>((uintptr_t)tex);
   return cudaSuccess;
-}
-
-// Unnormalised coordinates (the reference's textures, DPE.cpp:1078-1097): the sample at (u, v)
-// blends the texels around (u - 0.5, v - 0.5); addresses beyond the image take the edge texel,
-// which for linear filtering is the clamp of the coordinate to [-1, size - 1] before the blend.
-// Weights are exact floats, or (ref_set_texture_8bit_weights) rounded to 8 fractional bits.
-float ref_tex2D_float(cudaTextureObject_t tex, float u, float v) {
-  const Texture *t = reinterpret_cast<const Texture *>((uintptr_t)tex);
-  const cudaArray *a = t->arr;
-  auto texel = [a](int x, int y) {
-    x = x < 0 ? 0 : (x >= a->w ? a->w - 1 : x);
-    y = y < 0 ? 0 : (y >= a->h ? a->h - 1 : y);
-    return a->data[(size_t)y * a->w + x];
-  };
-  if (t->normalized) { u *= (float)a->w; v *= (float)a->h; }
-  if (t->filter == cudaFilterModePoint) return texel((int)std::floor(u), (int)std::floor(v));
-  const float x = u - 0.5f, y = v - 0.5f;
-  const float xc = std::fmin(std::fmax(x, -1.0f), (float)(a->w - 1));
-  const float yc = std::fmin(std::fmax(y, -1.0f), (float)(a->h - 1));
-  const float fx = std::floor(xc), fy = std::floor(yc);
-  const int x0 = (int)fx, y0 = (int)fy;
-  float ax = xc - fx, ay = yc - fy;
-  if (g_tex_8bit) { ax = std::floor(ax * 256.0f + 0.5f) / 256.0f; ay = std::floor(ay * 256.0f + 0.5f) / 256.0f; }
-  const float v00 = texel(x0, y0), v10 = texel(x0 + 1, y0);
-  const float v01 = texel(x0, y0 + 1), v11 = texel(x0 + 1, y0 + 1);
-  const float top = (1.0f - ax) * v00 + ax * v10;
-  const float bot = (1.0f - ax) * v01 + ax * v11;
-  return (1.0f - ay) * top + ay * bot;
 }
 
 // ------------------------------------------------------------------ events, errors

@@ -78,3 +78,11 @@ int main(void) {
                                            D.FusionOut, D.NCCQuery)]
     assert sizes[0] == 112  # reference Camera, main.h:53-62
     assert offs == [D.Problem.params.offset, D.Problem.seed.offset, D.FusionView.camera.offset]
+
+
+def test_python_reference_defaults_match_library():
+    """dpe_b200.reference_default_params (no library) equals dpe_params_default field for field."""
+    lib = D.load_library()
+    a, b = D.default_params(lib), D.reference_default_params()
+    for name, _ in D.Params._fields_:
+        assert getattr(a, name) == getattr(b, name), name
