@@ -1,9 +1,9 @@
 """Build the sm_100a shared library libdpe_sm100.so in-tree (nvcc, no torch extension machinery).
 
-Usage: python dpe-mvs-fast_b200/build.py [--force] [--checked] [--variant NAME -DMACRO=V ...]
+Usage: python dpe-mvs-fast_b200/build.py [--force] [--checked]
 
---variant builds libdpe_sm100_NAME.so with the given preprocessor definitions (kernel-shape
-experiments selected at run time with DPE_LIBRARY=libdpe_sm100_NAME.so).
+Builds the default library and the exact build (libdpe_sm100_exact.so: no multiply-add
+contraction, IEEE division); --checked builds the bounds-checked debug library instead.
 """
 from __future__ import annotations
 
@@ -47,7 +47,7 @@ def build(force: bool = False, verbose: bool = False, checked: bool = False, var
           defines: tuple = ()) -> str:
     """Compile csrc/*.cu for sm_100a and link libdpe_sm100.so (checked=True: the bounds-checked
     debug variant libdpe_sm100_checked.so, built with -DDPE_CHECKED; variant: a named build with
-    extra -D definitions)."""
+    extra flags, here the exact build)."""
     os.makedirs(OBJ, exist_ok=True)
     lib = LIB_CHECKED if checked else LIB
     if variant:
@@ -84,11 +84,7 @@ def build_all(force: bool = False, verbose: bool = False) -> list:
 
 if __name__ == "__main__":
     args = sys.argv[1:]
-    if "--variant" in args:
-        name = args[args.index("--variant") + 1]
-        flags = tuple(a for a in args if a.startswith("-D") or a.startswith("-f"))
-        print(build(force="--force" in args, verbose=True, variant=name, defines=flags))
-    elif "--checked" in args:
+    if "--checked" in args:
         print(build(force="--force" in args, verbose=True, checked=True))
     else:
         print("\n".join(build_all(force="--force" in args, verbose=True)))

@@ -61,6 +61,41 @@ def load() -> C.CDLL:
     return lib
 
 
+class _Quiet:
+    """The reference prints its progress to stdout (std::cout); while it runs, file descriptor 1 goes
+    to /dev/null so a caller's own output (a bench line) stays the only output."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.libc = C.CDLL(None)
+        self.libc.fflush(None)
+        self.saved = os.dup(1)
+        self.null = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(self.null, 1)
+        return self
+
+    def __exit__(self, *exc):
+        self.libc.fflush(None)
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+        os.close(self.null)
+
+
+QUIET = os.environ.get("DPE_REFERENCE_VERBOSE", "0") != "1"
+
+
+def _maybe_quiet():
+    return _Quiet() if QUIET else _NoOp()
+
+
+class _NoOp:
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        return False
+
+
 def set_texture_8bit_weights(on: bool) -> None:
     """Bilinear weights rounded to 8 fractional bits, as the texture unit interpolates (default:
     exact float weights, the CUDA kernels' and the oracle's interpolation)."""
@@ -84,7 +119,7 @@ def pm_call(images, cameras, params, *, seed: int, threads: int = 0, radius_init
     used = D.Params()
     guard = C.c_longlong(0)
     nthreads = threads if threads > 0 else (os.cpu_count() or 1)
-    with tempfile.TemporaryDirectory(prefix="dpe_ref_", dir=work_dir) as tmp:
+    with tempfile.TemporaryDirectory(prefix="dpe_ref_", dir=work_dir) as tmp, _maybe_quiet():
         st = lib.ref_pm_call(C.byref(pr), tmp.encode(), nthreads, 1 if radius_init else 0, 1 if serial_race else 0,
                              out["plane"].ctypes.data,
                              out["weak"].ctypes.data, out["views"].ctypes.data, out["costs"].ctypes.data, cams,
@@ -113,7 +148,7 @@ def fuse(views: List[Dict], variant: int = 0, work_dir: str | None = None) -> Di
     xyz = np.zeros((max(cap, 1), 3), np.float32)
     bgr = np.zeros((max(cap, 1), 3), np.uint8)
     n = C.c_int64(0)
-    with tempfile.TemporaryDirectory(prefix="dpe_ref_fuse_", dir=work_dir) as tmp:
+    with tempfile.TemporaryDirectory(prefix="dpe_ref_fuse_", dir=work_dir) as tmp, _maybe_quiet():
         st = lib.ref_fuse(C.byref(fin), variant, tmp.encode(), xyz.ctypes.data, bgr.ctypes.data, cap, C.byref(n))
     if st != 0:
         raise RuntimeError(lib.ref_last_error().decode())
