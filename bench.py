@@ -542,7 +542,7 @@ def run_ours(args):
         # the same first-init sample call on this GPU: depth agreement with the reference's own result
         p0, kw0, r0 = sampler.first_init_inputs
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
-        g0 = ctx.pm_run(sampler.images, sampler.R.camera_dicts(r0["cameras"]), r0["params"], seed=kw0["seed"])
+        g0 = ctx.pm_run(sampler.images, sampler.R.camera_dicts(r0["cameras"]), r0["params"], **kw0)
         da, db = g0["plane"][..., 3].astype(np.float64), r0["plane"][..., 3].astype(np.float64)
         agree = float((np.abs(da - db) <= 1e-3 * np.abs(db)).mean())
         cpu = dict(value=round(cvalue, 6), unit=UNIT, cores=threads, kind="reference", sample=desc,

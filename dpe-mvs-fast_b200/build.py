@@ -28,6 +28,7 @@ UNITS = {
     "scene.cu": [],
     "fusion.cu": ["-fmad=false"],
     "edges.cu": [],
+    "views.cu": ["-fmad=false"],
 }
 
 

@@ -773,25 +773,37 @@ int upload_queries(dpe_ctx *ctx, const dpe_ncc_query *q, QueryUpload *u) {
 
 // Cost and gradients of each query (the adjoint of k_ncc_queries).  gdn: dC/d(depth, nx, ny, nz)
 // with the depth at the pixel held instead of the plane offset w = -depth * (n . ray).
+// kChecked: queries come from device memory the host has not read, so a pixel or source outside
+// the problem gives NaN outputs instead of an access outside the images.
+template <bool kChecked>
 __global__ void k_ncc_grad(const PMArgs *__restrict__ pa, int64_t n, const int32_t *px, const int32_t *py,
-                           const int32_t *src, const float4 *pl, float *cost, float4 *gplane, float4 *gdn,
-                           float *gimg) {
+                           const int32_t *src, const float4 *pl, const float *upstream, float *cost, float4 *gplane,
+                           float4 *gdn, float *gimg) {
   const PMArgs &a = *pa;
   const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
+  if (kChecked && (src[k] < 1 || src[k] >= a.N || px[k] < 0 || px[k] >= a.W || py[k] < 0 || py[k] >= a.H)) {
+    const float nan = __int_as_float(0x7fc00000);
+    cost[k] = nan;
+    if (gplane) gplane[k] = make_float4(nan, nan, nan, nan);
+    if (gdn) gdn[k] = make_float4(nan, nan, nan, nan);
+    return;
+  }
   DPE_REF_WINDOW(rw);
   build_ref_window(a, px[k], py[k], rw, KID_NCC_QUERY);
   float g[4];
   const int s = src[k];
   const float4 p = pl[k];
-  cost[k] = ncc_strong_adjoint(a, px[k], py[k], s, p, rw, g, gimg ? gimg + (size_t)(s - 1) * a.W * a.H : nullptr);
+  cost[k] = ncc_strong_adjoint(a, px[k], py[k], s, p, rw, g, gimg ? gimg + (size_t)(s - 1) * a.W * a.H : nullptr,
+                               upstream ? upstream[k] : 1.0f);
+  if (!gplane) return;
   gplane[k] = make_float4(g[0], g[1], g[2], g[3]);
   // w = -depth * (n . ray), ray = Kr^-1 (x, y, 1): dC/ddepth = g_w * -(n . ray); dC/dn|depth = g_n + g_w * -depth * ray
   const dpe_camera &c = a.cam[0];
   const float ray[3] = {((float)px[k] - c.K[2]) / c.K[0], ((float)py[k] - c.K[5]) / c.K[4], 1.0f};
   const float nr = p.x * ray[0] + p.y * ray[1] + p.z * ray[2];
   const float depth = nr != 0.0f ? -p.w / nr : 0.0f;
-  gdn[k] = make_float4(-g[3] * nr, g[0] - g[3] * depth * ray[0], g[1] - g[3] * depth * ray[1], g[2] - g[3] * depth * ray[2]);
+  if (gdn) gdn[k] = make_float4(-g[3] * nr, g[0] - g[3] * depth * ray[0], g[1] - g[3] * depth * ray[1], g[2] - g[3] * depth * ray[2]);
 }
 }  // namespace
 
@@ -833,7 +845,7 @@ extern "C" int dpe_ncc_grad(dpe_ctx *ctx, const dpe_ncc_query *q, float *costs_o
   float *dgimg = grad_images_out ? A.get<float>("q_gimg", L * (q->num_images - 1)) : nullptr;
   if (!A.ok()) return DPE_ERR_OUT_OF_MEMORY;
   if (dgimg) DPE_TRY(cudaMemsetAsync(dgimg, 0, L * (q->num_images - 1) * 4, s));
-  DPE_TIMED(ctx, KID_NCC_QUERY, s, k_ncc_grad<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(u.d_args, n, u.px, u.py, u.src, u.plane, dcost, dgp, dgd, dgimg));
+  DPE_TIMED(ctx, KID_NCC_QUERY, s, k_ncc_grad<false><<<(unsigned)((n + 127) / 128), 128, 0, s>>>(u.d_args, n, u.px, u.py, u.src, u.plane, nullptr, dcost, dgp, dgd, dgimg));
   PM_LAUNCHED("k_ncc_grad", s);
   DPE_TRY(cudaMemcpyAsync(costs_out, dcost, n * 4, cudaMemcpyDeviceToHost, s));
   DPE_TRY(cudaMemcpyAsync(grad_plane_out, dgp, n * 16, cudaMemcpyDeviceToHost, s));
@@ -844,6 +856,52 @@ extern "C" int dpe_ncc_grad(dpe_ctx *ctx, const dpe_ncc_query *q, float *costs_o
         DPE_TRY(cudaMemcpyAsync(grad_images_out[i], dgimg + L * (i - 1), L * 4, cudaMemcpyDeviceToHost, s));
   DPE_TRY(cudaStreamSynchronize(s));
   ctx->collect();
+  return DPE_OK;
+}
+
+extern "C" int dpe_ncc_grad_device(dpe_ctx *ctx, const dpe_ncc_query *q, const float *upstream, float *costs_out,
+                                   float *grad_plane_out, float *grad_depth_normal_out, float *grad_images_out,
+                                   void *stream) {
+  if (!ctx || !q || !costs_out || q->count < 0) return DPE_ERR_INVALID_ARGUMENT;
+  if (q->num_images < 2 || q->num_images > DPE_MAX_IMAGES || q->width < 16 || q->height < 16) return DPE_ERR_INVALID_ARGUMENT;
+  if (q->params.strong_increment <= 0 || q->params.strong_radius < 0 ||
+      (2 * q->params.strong_radius) / q->params.strong_increment + 1 > kMaxWin)
+    return DPE_ERR_INVALID_ARGUMENT;
+  for (int i = 0; i < q->num_images; ++i)
+    if (!q->images[i]) return DPE_ERR_INVALID_ARGUMENT;
+  if (q->count > 0 && (!q->px || !q->py || !q->src || !q->plane)) return DPE_ERR_INVALID_ARGUMENT;
+  if (q->count == 0) return DPE_OK;
+  DPE_TRY(cudaSetDevice(ctx->device));
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const int W = q->width, H = q->height, N = q->num_images;
+  const size_t L = (size_t)W * H, PL = (size_t)(W + 2) * (H + 2);
+  Arena &A = ctx->arena;
+  PMArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.W = W; a.H = H; a.N = N; a.pad_w = W + 2;
+  a.P = q->params;
+  a.P.num_images = N;
+  for (int i = 0; i < N; ++i) a.cam[i] = q->cameras[i];
+  for (int i = 1; i < N; ++i) relative_pose(a.cam[0], a.cam[i], a.Rrel[i], a.trel[i]);
+  float *img_pad = A.get<float>("gd_img_pad", PL * N);
+  PMArgs *d_args = A.get<PMArgs>("gd_args", 1);
+  if (!A.ok()) return DPE_ERR_OUT_OF_MEMORY;
+  for (int i = 0; i < N; ++i) {
+    a.img[i] = img_pad + PL * i;
+    k_pad_image<<<dim3((W + 2 + 31) / 32, (H + 2 + 7) / 8), dim3(32, 8), 0, s>>>(q->images[i], img_pad + PL * i, W, H);
+    PM_LAUNCHED("k_pad_image", s);
+  }
+  DPE_TRY(cudaMemcpyAsync(d_args, &a, sizeof(PMArgs), cudaMemcpyHostToDevice, s));
+  if (grad_images_out) DPE_TRY(cudaMemsetAsync(grad_images_out, 0, L * (N - 1) * 4, s));
+  const int64_t n = q->count;
+  k_ncc_grad<true><<<(unsigned)((n + 127) / 128), 128, 0, s>>>(d_args, n, q->px, q->py, q->src,
+                                                               reinterpret_cast<const float4 *>(q->plane), upstream,
+                                                               costs_out, reinterpret_cast<float4 *>(grad_plane_out),
+                                                               reinterpret_cast<float4 *>(grad_depth_normal_out),
+                                                               grad_images_out);
+  PM_LAUNCHED("k_ncc_grad", s);
+  // the argument block is read by the kernels above: keep the host copy alive until they ran
+  DPE_TRY(cudaStreamSynchronize(s));
   return DPE_OK;
 }
 

@@ -582,7 +582,8 @@ __device__ __forceinline__ float ncc_strong(const PMArgs &a, int px, int py, int
 
 // ------------------------------------------------------------------ strong NCC adjoint
 // Cost and gradient of the strong NCC with respect to the plane (nx, ny, nz, w), and optionally
-// with respect to the source image's pixels (accumulated into gimg, W*H, with atomics).  Two passes
+// with respect to the source image's pixels (accumulated into gimg, W*H, with atomics, each
+// query's contribution times gscale: the upstream weight of its cost).  Two passes
 // over the window, the second recomputing the projections instead of storing the patch:
 //   pass 1: the moments and the cost, exactly as ncc_strong;
 //   pass 2: per tap, dC/ds (s = bilinear sample) from the moments, through the bilinear slope to
@@ -591,7 +592,7 @@ __device__ __forceinline__ float ncc_strong(const PMArgs &a, int px, int py, int
 // constant 2 (centre outside the source, flat window) or clamped to [0, 2], the gradient is zero.
 template <class RW>
 __device__ __forceinline__ float ncc_strong_adjoint(const PMArgs &a, int px, int py, int s, float4 pl,
-                                                    const RW &rw, float g[4], float *gimg) {
+                                                    const RW &rw, float g[4], float *gimg, float gscale = 1.0f) {
   g[0] = g[1] = g[2] = g[3] = 0.0f;
   float H[9];
   homography(a, s, pl, H);
@@ -655,13 +656,14 @@ __device__ __forceinline__ float ncc_strong_adjoint(const PMArgs &a, int px, int
       const float gz = -(gu * u + gv * v);
       gH[6] += gz * x; gH[7] += gz * y; gH[8] += gz;
       if (gimg) {
+        const float dcs = dc * gscale;  // the upstream weight of this query's cost
         const int x0 = (int)fx, y0 = (int)fy;
         const int xa = min(max(x0, 0), W - 1), xb = min(max(x0 + 1, 0), W - 1);
         const int ya = min(max(y0, 0), Hh - 1), yb = min(max(y0 + 1, 0), Hh - 1);
-        atomicAdd(&gimg[(size_t)ya * W + xa], dc * (1.0f - ax) * (1.0f - ay));
-        atomicAdd(&gimg[(size_t)ya * W + xb], dc * ax * (1.0f - ay));
-        atomicAdd(&gimg[(size_t)yb * W + xa], dc * (1.0f - ax) * ay);
-        atomicAdd(&gimg[(size_t)yb * W + xb], dc * ax * ay);
+        atomicAdd(&gimg[(size_t)ya * W + xa], dcs * (1.0f - ax) * (1.0f - ay));
+        atomicAdd(&gimg[(size_t)ya * W + xb], dcs * ax * (1.0f - ay));
+        atomicAdd(&gimg[(size_t)yb * W + xa], dcs * (1.0f - ax) * ay);
+        atomicAdd(&gimg[(size_t)yb * W + xb], dcs * ax * ay);
       }
       ++k;
     }

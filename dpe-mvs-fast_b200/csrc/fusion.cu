@@ -3,13 +3,22 @@
 //
 // The reference walks views in pair.txt order and pixels in raster order; an accepted pixel
 // masks the source pixels it used, and a masked source pixel is skipped by every later pixel.
-// Equivalently, for one reference view: a (source, pixel) entry of pixel p is masked iff an
-// earlier pixel of the same view that lists the same entry was accepted (or a previous view
-// masked it).  The kernels below compute every pixel's consistency entries in parallel, then
-// decide pixels in "waves": a pixel is decided once every earlier contender for each of its
-// entries is decided.  The globally first undecided pixel is always decidable, so the waves end;
-// in practice contention is sparse and a handful of waves suffice.  Decisions, counts, point
-// order and colours are those of the sequential loop.
+// Views run one after another here as well (a view's own pixels are masked only by earlier
+// views).  Within one reference view, a (source, pixel) entry of pixel p is live iff no earlier
+// pixel of the view that is ACCEPTED tests the same source pixel consistent; p's acceptance
+// depends on which of its entries are live.  The kernels compute every pixel's consistency
+// entries in parallel, then find the decisions as the fixed point of a Jacobi iteration:
+//   * start from every pixel's decision with all its entries live;
+//   * a round stamps each currently accepted pixel on the source pixels it tests consistent
+//     (atomicMin, the first accepted claimant wins) and re-decides every candidate from those
+//     claims;
+//   * stop after a round that changes no decision.
+// The decisions of the sequential loop satisfy every round (each depends only on earlier
+// pixels), and they are the only assignment that does: induction over raster order.  After k
+// rounds every pixel whose chain of earlier dependencies is k long is final, so the rounds end;
+// on the 10-view 1600x1200 scene they end after 5-10 rounds per view, because a changed decision
+// rarely changes a later one.  Decisions, counts, point order and colours are those of the
+// sequential loop.
 //
 // This file is compiled with -fmad=false so that its float and double arithmetic rounds like the
 // CPU restatement of the same loop.
@@ -32,12 +41,11 @@ struct FuseView {
   const uint8_t *bgr;
   const uint8_t *block;
   uint8_t *mask;
-  int *acc_min;  // per pixel: smallest accepted contender of the current reference view
-  // per pixel: smallest undecided contender of the current wave, as (stamp << 32 | pixel) with
-  // stamp = 0xFFFFFFFF - wave number (counted over the whole call): a wave's keys are smaller
-  // than every earlier wave's, so no reset between waves is needed, and an entry belongs to the
-  // current wave exactly when its stamp is the current one.
-  unsigned long long *und_min;
+  // per pixel: the first accepted claimant of the current round, as (stamp << 32 | pixel) with
+  // stamp = 0xFFFFFFFF - round number (counted over the whole call): a round's keys are smaller
+  // than every earlier round's, so no reset between rounds is needed, and a key belongs to the
+  // current round exactly when its stamp is the current one.
+  unsigned long long *claim;
   dpe_camera cam;
 };
 
@@ -52,9 +60,18 @@ struct FuseArgs {
   const FuseView *views;  // device array
   int *entry_q;           // W*H*ns: source pixel index, -1 when the entry is not consistent
   double *entry_score;    // W*H*ns: exp(-(e + 200 dd + 10 angle)) of a consistent entry
-  uint8_t *status;        // W*H: 0 undecided, 1 accepted, 2 rejected / not a candidate
-  int *remaining;
+  uint8_t *status;        // W*H: 1 accepted, 3 rejected (this round), 2 not a candidate
+  int *changes;           // decisions a round changed
 };
+
+// RunFusion's acceptance rule (DPE.cpp:1517-1520) over the live entries of one pixel, summed in
+// source order; min_consistent > 1 raises the reference's n >= 1.
+__device__ __forceinline__ bool fuse_accept(const FuseArgs &f, const FuseView &V, int pix, int n, double dyn_d,
+                                            float dyn_f) {
+  const float factor = V.weak[pix] == DPE_WEAK ? 0.45f : 0.3f;
+  const int need = f.min_consistent > 1 ? f.min_consistent : 1;
+  return f.mode == DPE_FUSE_FP64 ? (n >= need && dyn_d > (double)factor * n) : (n >= need && dyn_f > factor * n);
+}
 
 template <class T> __device__ __forceinline__ void world_point(T x, T y, T depth, const dpe_camera &c, T out[3]) {
   const T px = depth * (x - (T)c.K[2]) / (T)c.K[0];
@@ -95,6 +112,8 @@ __global__ void k_entries(const __grid_constant__ FuseArgs f) {
     world_point<double>((double)c, (double)r, (double)ref_depth, V.cam, Xd);
     world_point<float>((float)c, (float)r, ref_depth, V.cam, Xf);
     int n_pass = 0;
+    double dyn_d = 0.0;
+    float dyn_f = 0.0f;
     for (int j = 0; j < f.ns; ++j) {
       const FuseView &S = f.views[f.src[j]];
       int sr, sc;
@@ -144,28 +163,36 @@ __global__ void k_entries(const __grid_constant__ FuseArgs f) {
       eq[j] = sp;
       es[j] = score;
       n_pass++;
+      dyn_d += score;
+      dyn_f += (float)score;
     }
-    if (n_pass > 0) st = 0;
+    // the starting point of the rounds: the decision with every entry live
+    if (n_pass > 0) st = fuse_accept(f, V, pix, n_pass, dyn_d, dyn_f) ? 1 : 3;
   }
   f.status[pix] = st;
 }
 
-// One wave, first half: every undecided pixel stamps itself on the source pixels it would use.
-// Also clears the wave's count of undecided pixels (k_decide, next in the stream, counts them).
-__global__ void k_mark_undecided(const __grid_constant__ FuseArgs f, int npix, unsigned stamp) {
+// One round, first half: every accepted pixel stamps itself on the source pixels it tests
+// consistent; the smallest key of the round on a source pixel is its first accepted claimant.
+// Also clears the round's change count (k_redecide, next in the stream, counts).
+__global__ void k_claim(const __grid_constant__ FuseArgs f, int npix, unsigned stamp) {
   const int pix = blockIdx.x * blockDim.x + threadIdx.x;
-  if (pix == 0) *f.remaining = 0;
-  if (pix >= npix || f.status[pix] != 0) return;
+  if (pix == 0) *f.changes = 0;
+  if (pix >= npix || f.status[pix] != 1) return;
   const int *eq = f.entry_q + (size_t)pix * f.ns;
   const unsigned long long key = ((unsigned long long)stamp << 32) | (unsigned)pix;
   for (int j = 0; j < f.ns; ++j)
-    if (eq[j] >= 0) atomicMin(&f.views[f.src[j]].und_min[eq[j]], key);
+    if (eq[j] >= 0) atomicMin(&f.views[f.src[j]].claim[eq[j]], key);
 }
 
-__global__ void k_decide(const __grid_constant__ FuseArgs f, int npix, unsigned stamp) {
+// One round, second half: every candidate's decision from the round's claims.  An entry is live
+// unless an earlier accepted pixel claims its source pixel.
+__global__ void k_redecide(const __grid_constant__ FuseArgs f, int npix, unsigned stamp) {
   const FuseView &V = f.views[f.ref];
   const int pix = blockIdx.x * blockDim.x + threadIdx.x;
-  if (pix >= npix || f.status[pix] != 0) return;
+  if (pix >= npix) return;
+  const uint8_t st = f.status[pix];
+  if (st != 1 && st != 3) return;
   const int *eq = f.entry_q + (size_t)pix * f.ns;
   const double *es = f.entry_score + (size_t)pix * f.ns;
   int n = 0;
@@ -173,24 +200,17 @@ __global__ void k_decide(const __grid_constant__ FuseArgs f, int npix, unsigned 
   float dyn_f = 0.0f;
   for (int j = 0; j < f.ns; ++j) {
     if (eq[j] < 0) continue;
-    const FuseView &S = f.views[f.src[j]];
-    if (S.acc_min[eq[j]] < pix) continue;  // masked by an earlier accepted pixel of this view
-    const unsigned long long u = S.und_min[eq[j]];
-    if ((unsigned)(u >> 32) == stamp && (int)(unsigned)u < pix) {  // an earlier contender is undecided
-      atomicAdd(f.remaining, 1);
-      return;
-    }
+    const unsigned long long u = f.views[f.src[j]].claim[eq[j]];
+    if ((unsigned)(u >> 32) == stamp && (int)(unsigned)u < pix) continue;  // claimed earlier
     n++;
     dyn_d += es[j];
     dyn_f += (float)es[j];
   }
-  const float factor = V.weak[pix] == DPE_WEAK ? 0.45f : 0.3f;
-  const int need = f.min_consistent > 1 ? f.min_consistent : 1;
-  const bool accept = f.mode == DPE_FUSE_FP64 ? (n >= need && dyn_d > (double)factor * n) : (n >= need && dyn_f > factor * n);
-  f.status[pix] = accept ? 1 : 2;
-  if (accept)
-    for (int j = 0; j < f.ns; ++j)
-      if (eq[j] >= 0) atomicMin(&f.views[f.src[j]].acc_min[eq[j]], pix);
+  const uint8_t now = fuse_accept(f, V, pix, n, dyn_d, dyn_f) ? 1 : 3;
+  if (now != st) {
+    f.status[pix] = now;
+    atomicAdd(f.changes, 1);
+  }
 }
 
 __global__ void k_accept_flags(const uint8_t *status, int *flags, int npix) {
@@ -200,7 +220,7 @@ __global__ void k_accept_flags(const uint8_t *status, int *flags, int npix) {
 
 // Emit accepted points in raster order and mask the source pixels they used (DPE.cpp:1519-1541).
 __global__ void k_emit(const __grid_constant__ FuseArgs f, const int *offsets, long long *base, long long capacity,
-                       float *xyz, uint8_t *bgr, int32_t *origin, uint8_t *ncons, int view_index) {
+                       float *xyz, uint8_t *bgr, int32_t *origin, uint8_t *ncons, int view_index, unsigned stamp) {
   const FuseView &V = f.views[f.ref];
   const int npix = V.W * V.H;
   const int pix = blockIdx.x * blockDim.x + threadIdx.x;
@@ -212,7 +232,8 @@ __global__ void k_emit(const __grid_constant__ FuseArgs f, const int *offsets, l
   for (int j = 0; j < f.ns; ++j) {
     if (eq[j] < 0) continue;
     const FuseView &S = f.views[f.src[j]];
-    if (S.acc_min[eq[j]] != pix) continue;  // masked by an earlier accepted pixel
+    const unsigned long long u = S.claim[eq[j]];
+    if ((unsigned)(u >> 32) != stamp || (int)(unsigned)u != pix) continue;  // claimed by an earlier pixel
     S.mask[eq[j]] = 1;
     col0 += S.bgr[3 * eq[j]]; col1 += S.bgr[3 * eq[j] + 1]; col2 += S.bgr[3 * eq[j] + 2];
     n++;
@@ -443,7 +464,8 @@ __global__ void k_tat_emit(const __grid_constant__ TatArgs t, const int *offsets
 // per-view decision and scan buffers, and the point output.
 struct FuseBuffers {
   std::vector<FuseView> hv;
-  unsigned wave = 0;  // waves run in this call (the undecided markers' stamps)
+  unsigned round = 0;  // rounds run in this call (the claim keys' stamps)
+  long long rounds = 0;
   FuseView *d_views = nullptr;
   size_t max_pix = 0, total_pix = 0;
   int max_ns = 1;
@@ -487,10 +509,9 @@ static int fuse_prepare(dpe_ctx *ctx, const dpe_fusion_in *in, const dpe_fusion_
 
   B.hv.resize(nv);
   uint8_t *masks = A.get<uint8_t>("f_mask", total_pix);
-  int *acc = A.get<int>("f_acc", total_pix);
-  unsigned long long *und = A.get<unsigned long long>("f_und", total_pix);
-  // all ones: the stamp of wave 0, older than every wave of this call
-  if (und) DPE_TRY(cudaMemsetAsync(und, 0xFF, total_pix * sizeof(unsigned long long), ctx->stream));
+  unsigned long long *claim = A.get<unsigned long long>("f_claim", total_pix);
+  // all ones: the stamp of round 0, older than every round of this call
+  if (claim) DPE_TRY(cudaMemsetAsync(claim, 0xFF, total_pix * sizeof(unsigned long long), ctx->stream));
   float *d_depth = host ? A.get<float>("f_depth", total_pix) : nullptr;
   float *d_normal = host ? A.get<float>("f_normal", total_pix * 3) : nullptr;
   uint8_t *d_weak = host && need_weak ? A.get<uint8_t>("f_weak", total_pix) : nullptr;
@@ -516,7 +537,7 @@ static int fuse_prepare(dpe_ctx *ctx, const dpe_fusion_in *in, const dpe_fusion_
     const size_t n = (size_t)v.width * v.height;
     FuseView &f = B.hv[i];
     f.W = v.width; f.H = v.height; f.cam = v.camera;
-    f.mask = masks + off; f.acc_min = acc + off; f.und_min = und + off;
+    f.mask = masks + off; f.claim = claim + off;
     if (host) {
       DPE_TRY(cudaMemcpyAsync(d_depth + off, v.depth, n * 4, cudaMemcpyHostToDevice, s));
       DPE_TRY(cudaMemcpyAsync(d_normal + 3 * off, v.normal, n * 12, cudaMemcpyHostToDevice, s));
@@ -595,7 +616,7 @@ extern "C" int dpe_fuse(dpe_ctx *ctx, const dpe_fusion_in *in, dpe_fusion_out *o
   Arena &A = ctx->arena;
   int *entry_q = A.get<int>("f_eq", B.max_pix * B.max_ns);
   double *entry_s = A.get<double>("f_es", B.max_pix * B.max_ns);
-  int *remaining = A.get<int>("f_remaining", 1);
+  int *changes = A.get<int>("f_changes", 1);
   if (!A.ok()) return DPE_ERR_OUT_OF_MEMORY;
 
   FuseArgs f;
@@ -606,7 +627,7 @@ extern "C" int dpe_fuse(dpe_ctx *ctx, const dpe_fusion_in *in, dpe_fusion_out *o
   f.entry_q = entry_q;
   f.entry_score = entry_s;
   f.status = B.status;
-  f.remaining = remaining;
+  f.changes = changes;
   for (int i = 0; i < in->num_views; ++i) {
     const dpe_fusion_view &v = in->views[i];
     const int npix = v.width * v.height;
@@ -614,36 +635,31 @@ extern "C" int dpe_fuse(dpe_ctx *ctx, const dpe_fusion_in *in, dpe_fusion_out *o
     f.ref = i;
     f.ns = v.num_src;
     for (int j = 0; j < v.num_src; ++j) f.src[j] = v.src_views[j];
-    for (int j = 0; j < v.num_src; ++j) {
-      const FuseView &S = B.hv[v.src_views[j]];
-      DPE_TRY(cudaMemsetAsync(S.acc_min, 0x7F, (size_t)S.W * S.H * 4, s));
-    }
+    unsigned stamp = 0xFFFFFFFFu;
     if (v.num_src > 0) {
       DPE_TIMED(ctx, KID_FUSE_ENTRIES, s, k_entries<<<blocks, 256, 0, s>>>(f));
       DPE_LAUNCHED("k_entries", s);
-      // waves until every candidate pixel is decided; each wave decides at least the first one.
-      // The count of the last wave is read every kWaveBatch waves: waves after the last decision
-      // find no undecided pixel and change nothing.
-      constexpr int kWaveBatch = 8;
-      for (int wave = 0; wave < npix + 1; wave += kWaveBatch) {
-        for (int k = 0; k < kWaveBatch; ++k) {
-          const unsigned stamp = 0xFFFFFFFFu - (unsigned)(++B.wave);
-          DPE_TIMED(ctx, KID_FUSE_WAVES, s, k_mark_undecided<<<blocks, 256, 0, s>>>(f, npix, stamp));
-          DPE_LAUNCHED("k_mark_undecided", s);
-          DPE_TIMED(ctx, KID_FUSE_WAVES, s, k_decide<<<blocks, 256, 0, s>>>(f, npix, stamp));
-          DPE_LAUNCHED("k_decide", s);
-        }
-        int rem = 0;
-        DPE_TRY(cudaMemcpyAsync(&rem, remaining, 4, cudaMemcpyDeviceToHost, s));
+      // Jacobi rounds until one changes nothing.  Each round makes at least the first undecided
+      // pixel of the dependency order final, so npix + 1 rounds always suffice.
+      for (int round = 0; round < npix + 1; ++round) {
+        stamp = 0xFFFFFFFFu - (unsigned)(++B.round);
+        DPE_TIMED(ctx, KID_FUSE_ROUNDS, s, k_claim<<<blocks, 256, 0, s>>>(f, npix, stamp));
+        DPE_LAUNCHED("k_claim", s);
+        DPE_TIMED(ctx, KID_FUSE_ROUNDS, s, k_redecide<<<blocks, 256, 0, s>>>(f, npix, stamp));
+        DPE_LAUNCHED("k_redecide", s);
+        int changed = 0;
+        DPE_TRY(cudaMemcpyAsync(&changed, changes, 4, cudaMemcpyDeviceToHost, s));
         DPE_TRY(cudaStreamSynchronize(s));
-        if (rem == 0) break;
+        B.rounds++;
+        if (changed == 0) break;
       }
     } else {
       DPE_TRY(cudaMemsetAsync(B.status, 2, npix, s));
     }
     if ((st = fuse_offsets(ctx, B, npix)) != DPE_OK) return st;
     DPE_TIMED(ctx, KID_FUSE_EMIT, s,
-              k_emit<<<blocks, 256, 0, s>>>(f, B.offsets, B.base, B.cap_dev, B.xyz, B.rgb, B.origin, B.ncons, i));
+              k_emit<<<blocks, 256, 0, s>>>(f, B.offsets, B.base, B.cap_dev, B.xyz, B.rgb, B.origin, B.ncons, i,
+                                            stamp));
     DPE_LAUNCHED("k_emit", s);
     if ((st = fuse_advance(ctx, B, npix)) != DPE_OK) return st;
   }

@@ -21,7 +21,7 @@ enum KernelId {
   KID_PAD_IMAGE,
   KID_NCC_QUERY,
   KID_FUSE_ENTRIES,
-  KID_FUSE_WAVES,
+  KID_FUSE_ROUNDS,
   KID_FUSE_EMIT,
   KID_FUSE_TAT,
   KID_EDGE_MAP,
@@ -35,5 +35,5 @@ static const char *const kKernelNames[KID_COUNT] = {
     "k_random_init",   "k_strong_update",   "k_ransac_fit_plane",    "k_weak_prepare",   "k_weak_eval",
     "k_weak_decide",   "k_weak_finish",     "k_get_depth_normal",
     "k_filter_strong", "k_depth_to_weak",   "k_local_refine",        "k_pad_image",      "k_ncc_queries",
-    "k_fuse_entries",  "k_fuse_waves",      "k_fuse_emit",           "k_fuse_tat",       "k_edge_map",
+    "k_fuse_entries",  "k_fuse_rounds",      "k_fuse_emit",           "k_fuse_tat",       "k_edge_map",
     "k_edge_labels",   "k_scene_misc"};

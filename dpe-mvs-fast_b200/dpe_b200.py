@@ -107,6 +107,11 @@ class SceneOut(C.Structure):
                 ("gpu_ms", C.c_float), ("fusion_ms", C.c_float), ("num_levels", C.c_int), ("calls", C.c_int)]
 
 
+class SparseModel(C.Structure):
+    _fields_ = [("num_images", C.c_int), ("centers", C.c_void_p), ("obs_offsets", C.c_void_p),
+                ("obs_point", C.c_void_p), ("num_points", C.c_int64), ("points", C.c_void_p)]
+
+
 class Options(C.Structure):
     _fields_ = [("staging", C.c_int), ("gn_refine", C.c_int)]
 
@@ -118,7 +123,8 @@ class Limits(C.Structure):
 EXPORTED = ["dpe_status_string", "dpe_last_error", "dpe_params_default", "dpe_ctx_create", "dpe_ctx_destroy", "dpe_pm_run",
             "dpe_fuse", "dpe_ncc_eval", "dpe_ctx_set_eval_counting", "dpe_scene_run", "dpe_ctx_set_profiling",
             "dpe_ctx_reset_kernel_stats", "dpe_ctx_get_kernel_stats", "dpe_launch_count", "dpe_fp32_peak",
-            "dpe_ncc_eval_noalloc", "dpe_ncc_grad", "dpe_ctx_set_options", "dpe_pm_run_batch", "dpe_fuse_tat", "dpe_edge_map", "dpe_edge_labels"]
+            "dpe_ncc_eval_noalloc", "dpe_ncc_grad", "dpe_ctx_set_options", "dpe_pm_run_batch", "dpe_fuse_tat", "dpe_edge_map", "dpe_edge_labels",
+            "dpe_view_scores", "dpe_ncc_grad_device"]
 
 _lib = None
 
@@ -154,6 +160,9 @@ def load_library(path: Optional[str] = None) -> C.CDLL:
     lib.dpe_launch_count.argtypes = []
     lib.dpe_fp32_peak.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
     lib.dpe_ncc_eval_noalloc.argtypes = [C.POINTER(NCCQuery), C.c_void_p, C.c_void_p]
+    lib.dpe_view_scores.argtypes = [C.c_void_p, C.POINTER(SparseModel), C.c_void_p]
+    lib.dpe_ncc_grad_device.argtypes = [C.c_void_p, C.POINTER(NCCQuery), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                        C.c_void_p, C.c_void_p]
     lib.dpe_ctx_set_options.argtypes = [C.c_void_p, C.POINTER(Options)]
     lib.dpe_pm_run_batch.argtypes = [C.c_void_p, C.POINTER(Problem), C.c_int, C.POINTER(PMOut)]
     lib.dpe_ncc_grad.argtypes = [C.c_void_p, C.POINTER(NCCQuery), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
@@ -499,6 +508,22 @@ class Context:
         if want_consistency:
             res["num_consistent"] = ncons[:n]
         return res
+
+    # ------------------------------------------------------------------ view selection
+    def view_scores(self, centers, obs_offsets, obs_point, points) -> np.ndarray:
+        """dpe_view_scores: the pair score matrix (N, N) of calc_score (colmap2mvsnet.py:280-302)."""
+        centers = np.ascontiguousarray(centers, np.float64).reshape(-1, 3)
+        obs_offsets = np.ascontiguousarray(obs_offsets, np.int64)
+        obs_point = np.ascontiguousarray(obs_point, np.int32)
+        points = np.ascontiguousarray(points, np.float64).reshape(-1, 3)
+        n = centers.shape[0]
+        m = SparseModel(n, _ptr(centers), _ptr(obs_offsets), _ptr(obs_point) if obs_point.size else None,
+                        points.shape[0], _ptr(points) if points.size else None)
+        out = np.zeros((n, n), np.float64)
+        st = self.lib.dpe_view_scores(self.handle, C.byref(m), _ptr(out))
+        if st != OK:
+            raise DPEError(st, "dpe_view_scores")
+        return out
 
     # ------------------------------------------------------------------ NCC queries
     def set_options(self, staging: int = STAGE_FP32, gn_refine: int = 0) -> None:

@@ -156,7 +156,8 @@ typedef struct dpe_fusion_out {
 
 /* ---- NCC evaluation at explicit (pixel, plane, source) queries ----
  * The memory space of every pointer below is set by the entry point that takes the query:
- * host memory for dpe_ncc_eval and dpe_ncc_grad, device memory for dpe_ncc_eval_noalloc. */
+ * host memory for dpe_ncc_eval and dpe_ncc_grad, device memory for dpe_ncc_grad_device and
+ * dpe_ncc_eval_noalloc. */
 typedef struct dpe_ncc_query {
   int width;
   int height;
@@ -269,7 +270,11 @@ int dpe_pm_run(dpe_ctx *ctx, const dpe_problem *problem, dpe_pm_out *out);
  * must agree on the schedule flags (params.state, use_APD, use_edge, geom_consistency,
  * max_iterations); other parameters may differ.  Each problem's result equals its dpe_pm_run
  * result.  outs[b].gpu_ms and the evaluation counts are the batch's totals.  count <=
- * DPE_MAX_BATCH. */
+ * DPE_MAX_BATCH.
+ * It takes no dpe_schedule: it is one call of the schedule for many views, and each problem
+ * already carries that call's parameters.  The schedule across calls and pyramid levels (levels,
+ * refine calls, iterations, fusion) is dpe_scene_run's dpe_schedule, whose batch_views = 1 runs
+ * every call through this entry point. */
 #define DPE_MAX_BATCH 256
 int dpe_pm_run_batch(dpe_ctx *ctx, const dpe_problem *problems, int count, dpe_pm_out *outs);
 
@@ -350,6 +355,21 @@ int dpe_ncc_eval(dpe_ctx *ctx, const dpe_ncc_query *q, float *costs_out);
 int dpe_ncc_grad(dpe_ctx *ctx, const dpe_ncc_query *q, float *costs_out, float *grad_plane_out,
                  float *grad_depth_normal_out, float *const *grad_images_out);
 
+/* dpe_ncc_grad on device memory, for autograd callers whose tensors stay on the GPU (no
+ * reference counterpart).  Every pointer of `q`, `upstream` and the outputs is DEVICE memory of the
+ * context's device; the work runs on `stream` (a cudaStream_t; NULL: the default stream) and the
+ * call returns when it has completed.
+ *   upstream              NULL, or count weights: each query's contribution to grad_images_out is
+ *                         scaled by its weight (the gradient of sum_k upstream[k] * C_k), so a
+ *                         backward pass gives the image gradient in one call;
+ *   grad_plane_out        NULL, or [count][4] dC/d(nx, ny, nz, w) (unweighted, as dpe_ncc_grad);
+ *   grad_depth_normal_out NULL, or [count][4] dC/d(depth, nx, ny, nz);
+ *   grad_images_out       NULL, or (num_images - 1) consecutive width x height float planes, one per
+ *                         source image (image 1 first); zeroed by the call before accumulating.
+ * Queries whose pixel or source index lies outside the problem get NaN outputs. */
+int dpe_ncc_grad_device(dpe_ctx *ctx, const dpe_ncc_query *q, const float *upstream, float *costs_out,
+                        float *grad_plane_out, float *grad_depth_normal_out, float *grad_images_out, void *stream);
+
 /* Allocation-free variant of dpe_ncc_eval for callers that cannot allocate device memory: code
  * hosted by a framework that owns and budgets all device memory through its own allocator (a
  * private cudaMalloc there would bypass its accounting), and real-time paths that must not pay
@@ -372,6 +392,26 @@ int dpe_ncc_grad(dpe_ctx *ctx, const dpe_ncc_query *q, float *costs_out, float *
  * it keeps the previous call's contents, so calls that overlap on the GPU (different streams or
  * host threads without ordering between them) race and corrupt each other's results. */
 int dpe_ncc_eval_noalloc(const dpe_ncc_query *q, float *costs_out, void *stream);
+
+/* ---- view selection: the pair scores behind pair.txt ----
+ * The reference's view selection (colmap2mvsnet.py:280-302 calc_score, 405-419 in
+ * processing_single_scene) scores every image pair (i, j), i < j, by the 2D observations of
+ * image i whose 3D point image j also observes (an observation listed twice counts twice), and
+ * sets the score to 0 when the 75th percentile (element int(0.75 n) of the sorted list) of those
+ * observations' triangulation angles is below 1 degree.  Points are given densely indexed (the
+ * caller maps COLMAP's point ids to 0..num_points-1; -1 is an observation without a point). */
+typedef struct dpe_sparse_model {
+  int num_images;
+  const double *centers;        /* num_images*3 camera centres -R^T t (host memory)         */
+  const int64_t *obs_offsets;   /* num_images+1: image i's observations are
+                                   obs_point[obs_offsets[i] .. obs_offsets[i+1])             */
+  const int32_t *obs_point;     /* dense point index per observation, or -1                  */
+  int64_t num_points;
+  const double *points;         /* num_points*3 xyz                                          */
+} dpe_sparse_model;
+/* scores_out: num_images x num_images doubles (host memory), symmetric, 0 on the diagonal: the
+ * matrix `score` that processing_single_scene ranks for each view's sources. */
+int dpe_view_scores(dpe_ctx *ctx, const dpe_sparse_model *m, double *scores_out);
 
 /* ---- options: the precision and differentiation forms of the path (no reference counterpart) */
 enum { DPE_STAGE_FP32 = 0, DPE_STAGE_FP16 = 1, DPE_STAGE_BF16 = 2 };

@@ -37,6 +37,7 @@ typedef signed char schar;
 #define CV_32SC1 CV_MAKETYPE(CV_32S, 1)
 #define CV_32FC1 CV_MAKETYPE(CV_32F, 1)
 #define CV_32FC3 CV_MAKETYPE(CV_32F, 3)
+#define CV_32FC4 CV_MAKETYPE(CV_32F, 4)
 #define CV_PI 3.1415926535897932384626433832795
 #ifndef MIN
 #define MIN(a, b) ((a) > (b) ? (b) : (a))
@@ -72,6 +73,7 @@ template <class T, int n, class S> Vec<T, n> operator*(const Vec<T, n> &v, S s) 
 typedef Vec<float, 3> Vec3f;
 typedef Vec<uchar, 3> Vec3b;
 typedef Vec<int, 4> Vec4i;
+typedef Vec<float, 4> Vec4f;
 
 template <class T> struct Size_ {
   T width = 0, height = 0;

@@ -99,21 +99,82 @@ def test_image_gradient_matches_fp64(ctx, grad_inputs):
     assert rel <= 1e-3
 
 
+def _cuda_inputs(images, px, py, src, planes, n):
+    import torch
+
+    return (torch.from_numpy(np.stack(images)).cuda(), torch.from_numpy(np.ascontiguousarray(px[:n], np.int32)).cuda(),
+            torch.from_numpy(np.ascontiguousarray(py[:n], np.int32)).cuda(),
+            torch.from_numpy(np.ascontiguousarray(src[:n], np.int32)).cuda(),
+            torch.from_numpy(np.ascontiguousarray(planes[:n], np.float32)).cuda())
+
+
+def _image_rel(gi, gi64):
+    return np.sqrt(sum(np.sum((gi[i] - gi64[i]) ** 2) for i in range(1, len(gi64))) /
+                   sum(np.sum(gi64[i] ** 2) for i in range(1, len(gi64))))
+
+
 def test_autograd_function(grad_inputs):
+    """NCCCost on CUDA tensors (no host round trip): plane and image gradients of the summed cost
+    against the FP64 oracle."""
     import torch
     import ncc_autograd as AG
 
     images, cams, p, (px, py, src, planes) = grad_inputs
     n = 500
-    pl = torch.from_numpy(planes[:n].copy()).requires_grad_(True)
-    imgs = torch.from_numpy(np.stack(images)).requires_grad_(True)
-    cost = AG.NCCCost.apply(pl, imgs, cams, p, px[:n], py[:n], src[:n])
+    imgs, tpx, tpy, tsrc, tpl = _cuda_inputs(images, px, py, src, planes, n)
+    pl = tpl.clone().requires_grad_(True)
+    imgs = imgs.requires_grad_(True)
+    cost = AG.NCCCost.apply(pl, imgs, cams, p, tpx, tpy, tsrc)
+    assert cost.is_cuda
     cost.sum().backward()
+    assert pl.grad.is_cuda and imgs.grad.is_cuda
     c64, g64, gi64 = O.ncc_strong_grad(images, cams, p, px[:n], py[:n], src[:n], planes[:n], want_images=True)
     live = (c64 > 0.01) & (c64 < 1.99)
-    assert (_rel(pl.grad.numpy()[live].astype(np.float64), g64[live]) <= 1e-3).mean() >= 0.99
+    assert (_rel(pl.grad.cpu().numpy()[live].astype(np.float64), g64[live]) <= 1e-3).mean() >= 0.99
     assert float(imgs.grad[0].abs().max()) == 0.0  # the reference image carries no gradient
-    gi = imgs.grad.numpy()
-    rel = np.sqrt(sum(np.sum((gi[i] - gi64[i]) ** 2) for i in range(1, len(images))) /
-                  sum(np.sum(gi64[i] ** 2) for i in range(1, len(images))))
+    assert _image_rel(imgs.grad.cpu().numpy(), gi64) <= 1e-3
+
+
+def test_autograd_weighted_image_gradient(grad_inputs):
+    """Per-query upstream weights: the image gradient of sum_k w_k C_k (two query groups weighted 1
+    and -2.5) against the FP64 oracle's gradients of the two groups' sums."""
+    import torch
+    import ncc_autograd as AG
+
+    images, cams, p, (px, py, src, planes) = grad_inputs
+    n = 600
+    imgs, tpx, tpy, tsrc, tpl = _cuda_inputs(images, px, py, src, planes, n)
+    imgs = imgs.requires_grad_(True)
+    w = np.where(np.arange(n) < n // 2, 1.0, -2.5).astype(np.float32)
+    cost = AG.NCCCost.apply(tpl, imgs, cams, p, tpx, tpy, tsrc)
+    (cost * torch.from_numpy(w).cuda()).sum().backward()
+    h = n // 2
+    _, _, ga = O.ncc_strong_grad(images, cams, p, px[:h], py[:h], src[:h], planes[:h], want_images=True)
+    _, _, gb = O.ncc_strong_grad(images, cams, p, px[h:n], py[h:n], src[h:n], planes[h:n], want_images=True)
+    want = [None] + [ga[i] - 2.5 * gb[i] for i in range(1, len(images))]
+    rel = _image_rel(imgs.grad.cpu().numpy(), want)
+    print(f"weighted image gradient vs FP64: relative L2 {rel:.2e}")
     assert rel <= 1e-3
+
+
+def test_autograd_depth_normal(ctx, grad_inputs):
+    """d(NCC)/d(depth, normal) through autograd (planes built from depth and normal with torch ops)
+    equals the kernel's own chain rule (dpe_ncc_grad's grad_depth_normal)."""
+    import torch
+    import ncc_autograd as AG
+
+    images, cams, p, (px, py, src, planes) = grad_inputs
+    n = 400
+    imgs, tpx, tpy, tsrc, tpl = _cuda_inputs(images, px, py, src, planes, n)
+    K = np.asarray(cams[0]["K"], np.float32).reshape(3, 3)
+    ray = np.stack([(px[:n] - K[0, 2]) / K[0, 0], (py[:n] - K[1, 2]) / K[1, 1], np.ones(n)], 1).astype(np.float32)
+    depth = (-planes[:n, 3] / np.sum(planes[:n, :3] * ray, 1)).astype(np.float32)
+    d = torch.from_numpy(depth).cuda().requires_grad_(True)
+    nrm = torch.from_numpy(np.ascontiguousarray(planes[:n, :3])).cuda().requires_grad_(True)
+    AG.ncc_cost_depth_normal(d, nrm, imgs, cams, p, tpx, tpy, tsrc).sum().backward()
+    c, _, gdn, _ = ctx.ncc_grad(images, cams, p, px[:n], py[:n], src[:n], planes[:n])
+    live = (c > 0.01) & (c < 1.99)
+    got = np.concatenate([d.grad.cpu().numpy()[:, None], nrm.grad.cpu().numpy()], 1)
+    ok = (_rel(got[live].astype(np.float64), gdn[live].astype(np.float64)) <= 1e-2).mean()
+    print(f"d/d(depth, normal) through autograd vs the kernel's chain rule: {ok:.4f} within 1e-2")
+    assert ok >= 0.98
