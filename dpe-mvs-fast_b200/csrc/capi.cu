@@ -278,7 +278,7 @@ int setup_problem(dpe_ctx *ctx, const dpe_problem *p, int index, ProblemState *p
   a.P = p->params;
   a.P.num_images = N;
   for (int i = 0; i < N; ++i) a.cam[i] = p->cameras[i];
-  for (int i = 1; i < N; ++i) relative_pose(a.cam[0], a.cam[i], a.Rrel[i], a.trel[i]);
+  set_homography_bases(a);
   a.key[0] = (uint32_t)p->seed;
   a.key[1] = (uint32_t)(p->seed >> 32);
   a.gn = ctx->opt.gn_refine;
@@ -747,7 +747,7 @@ int upload_queries(dpe_ctx *ctx, const dpe_ncc_query *q, QueryUpload *u) {
   a.P = q->params;
   a.P.num_images = N;
   for (int i = 0; i < N; ++i) a.cam[i] = q->cameras[i];
-  for (int i = 1; i < N; ++i) relative_pose(a.cam[0], a.cam[i], a.Rrel[i], a.trel[i]);
+  set_homography_bases(a);
   float *img_pad = A.get<float>("img_pad", PL * N);
   float *stage = A.get<float>("img_stage", L * N);
   const int64_t n = q->count;
@@ -882,7 +882,7 @@ extern "C" int dpe_ncc_grad_device(dpe_ctx *ctx, const dpe_ncc_query *q, const f
   a.P = q->params;
   a.P.num_images = N;
   for (int i = 0; i < N; ++i) a.cam[i] = q->cameras[i];
-  for (int i = 1; i < N; ++i) relative_pose(a.cam[0], a.cam[i], a.Rrel[i], a.trel[i]);
+  set_homography_bases(a);
   float *img_pad = A.get<float>("gd_img_pad", PL * N);
   PMArgs *d_args = A.get<PMArgs>("gd_args", 1);
   if (!A.ok()) return DPE_ERR_OUT_OF_MEMORY;
@@ -1010,7 +1010,7 @@ extern "C" int dpe_ncc_eval_noalloc(const dpe_ncc_query *q, float *costs_out, vo
   a.P = q->params;
   a.P.num_images = N;
   for (int i = 0; i < N; ++i) a.cam[i] = q->cameras[i];
-  for (int i = 1; i < N; ++i) relative_pose(a.cam[0], a.cam[i], a.Rrel[i], a.trel[i]);
+  set_homography_bases(a);
   unsigned char *img_base = base + round256(sizeof(PMArgs));
   for (int i = 0; i < N; ++i) a.img[i] = reinterpret_cast<const float *>(img_base + (size_t)i * img_bytes);
   cudaStream_t s = static_cast<cudaStream_t>(stream);

@@ -58,8 +58,10 @@ struct PMArgs {
   int W, H, N, lowW, lowH, pad_w;  // pad_w = W + 2 (images carry a 1-texel clamp border)
   dpe_params P;
   dpe_camera cam[kMaxImages];
-  float Rrel[kMaxImages][9];  // source rotation relative to the reference (DPE.cu:471-479)
-  float trel[kMaxImages][3];  // source translation relative to the reference (DPE.cu:480-485)
+  // Plane-independent parts of each source's homography H = A - b m^T / w (homography_base):
+  // composed in double (window centres are projected in double), and the same rounded to float.
+  double dA[kMaxImages][9], db[kMaxImages][3], dm[4];
+  float hA[kMaxImages][9], hb[kMaxImages][3], hm[4];
   uint32_t key[2];
   const float *img[kMaxImages];  // padded (W+2)*(H+2) float images
   // Staged source images (dpe_options::staging FP16 / BF16): pair[s][o] holds the padded texels
@@ -107,19 +109,53 @@ struct PMArgs {
   float4 *wstate;     // [slot][2] plane after the candidate and fit-plane steps; (depth, cost, cost0, wn)
 };
 
-// Relative pose of source s with respect to the reference, computed once per call on the host
-// with the float operation order of ComputeHomography (DPE.cu:459-485).
-inline void relative_pose(const dpe_camera &rc, const dpe_camera &sc, float Rrel[9], float trel[3]) {
-  float rC[3], sC[3], Cr[3];
+// Plane-independent parts of the homography of source camera sc with respect to the reference
+// camera rc (DPE.cu:457-517).  H = Ks (Rrel - trel n^T / w) Kr^-1 is written as A - b m^T / w with
+//   A = Ks Rrel Kr^-1,  b = Ks trel,  m = Kr^-T n = (nx / fx, ny / fy, nz - nx cx / fx - ny cy / fy),
+// Rrel = Rs Rr^T, trel = Rs (Cr - Cs) and camera centres C = -R^T t.  A, b and the entries of
+// Kr^-1 (m = (1/fx, 1/fy, -cx/fx, -cy/fy) here) are composed once per call on the host in double.
+// The reference composes the same products in float per hypothesis; the float rounding of the
+// camera products moves the entries of H by a few ulps, which at source coordinates of ~2000 px
+// places a window ~1e-4 px off.
+inline void homography_base(const dpe_camera &rc, const dpe_camera &sc, double A[9], double b[3], double m[4]) {
+  double rC[3], sC[3], Rr[9], Cr[3], tr[3], MK[9];
   for (int k = 0; k < 3; ++k) {
-    rC[k] = -(rc.R[k] * rc.t[0] + rc.R[3 + k] * rc.t[1] + rc.R[6 + k] * rc.t[2]);
-    sC[k] = -(sc.R[k] * sc.t[0] + sc.R[3 + k] * sc.t[1] + sc.R[6 + k] * sc.t[2]);
+    rC[k] = -((double)rc.R[k] * rc.t[0] + (double)rc.R[3 + k] * rc.t[1] + (double)rc.R[6 + k] * rc.t[2]);
+    sC[k] = -((double)sc.R[k] * sc.t[0] + (double)sc.R[3 + k] * sc.t[1] + (double)sc.R[6 + k] * sc.t[2]);
   }
-  for (int a = 0; a < 3; ++a)
-    for (int b = 0; b < 3; ++b)
-      Rrel[3 * a + b] = sc.R[3 * a] * rc.R[3 * b] + sc.R[3 * a + 1] * rc.R[3 * b + 1] + sc.R[3 * a + 2] * rc.R[3 * b + 2];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j)
+      Rr[3 * i + j] = (double)sc.R[3 * i] * rc.R[3 * j] + (double)sc.R[3 * i + 1] * rc.R[3 * j + 1] +
+                      (double)sc.R[3 * i + 2] * rc.R[3 * j + 2];
   for (int k = 0; k < 3; ++k) Cr[k] = rC[k] - sC[k];
-  for (int a = 0; a < 3; ++a) trel[a] = sc.R[3 * a] * Cr[0] + sc.R[3 * a + 1] * Cr[1] + sc.R[3 * a + 2] * Cr[2];
+  for (int i = 0; i < 3; ++i)
+    tr[i] = (double)sc.R[3 * i] * Cr[0] + (double)sc.R[3 * i + 1] * Cr[1] + (double)sc.R[3 * i + 2] * Cr[2];
+  m[0] = 1.0 / rc.K[0];
+  m[1] = 1.0 / rc.K[4];
+  m[2] = -(double)rc.K[2] / rc.K[0];
+  m[3] = -(double)rc.K[5] / rc.K[4];
+  for (int i = 0; i < 3; ++i) {
+    MK[3 * i] = Rr[3 * i] * m[0];
+    MK[3 * i + 1] = Rr[3 * i + 1] * m[1];
+    MK[3 * i + 2] = Rr[3 * i] * m[2] + Rr[3 * i + 1] * m[3] + Rr[3 * i + 2];
+  }
+  for (int j = 0; j < 3; ++j) {
+    A[j] = (double)sc.K[0] * MK[j] + (double)sc.K[2] * MK[6 + j];
+    A[3 + j] = (double)sc.K[4] * MK[3 + j] + (double)sc.K[5] * MK[6 + j];
+    A[6 + j] = (double)sc.K[8] * MK[6 + j];
+  }
+  b[0] = (double)sc.K[0] * tr[0] + (double)sc.K[2] * tr[2];
+  b[1] = (double)sc.K[4] * tr[1] + (double)sc.K[5] * tr[2];
+  b[2] = (double)sc.K[8] * tr[2];
+}
+// Fills the homography bases of every source of a call (cameras already in a.cam).
+inline void set_homography_bases(PMArgs &a) {
+  for (int s = 1; s < a.N; ++s) {
+    homography_base(a.cam[0], a.cam[s], a.dA[s], a.db[s], a.dm);
+    for (int k = 0; k < 9; ++k) a.hA[s][k] = (float)a.dA[s][k];
+    for (int k = 0; k < 3; ++k) a.hb[s][k] = (float)a.db[s][k];
+  }
+  for (int k = 0; k < 4; ++k) a.hm[k] = (float)a.dm[k];
 }
 
 // ------------------------------------------------------------------ checked builds
@@ -390,29 +426,15 @@ __device__ __forceinline__ float4 perturbed_normal(const dpe_camera &c, int x, i
   return r;
 }
 
-// Homography of a reference-camera plane into source `s` (DPE.cu:457-517), using the relative
-// pose precomputed on the host with the reference's float operation order.
+// Homography of a reference-camera plane into source `s` (DPE.cu:457-517) in float, from the
+// per-call bases: H = A - (b / w) m^T with m = (nx / fx, ny / fy, nz - nx cx / fx - ny cy / fy).
 __device__ __forceinline__ void homography(const PMArgs &a, int s, float4 pl, float H[9]) {
-  const dpe_camera &rc = a.cam[0];
-  const dpe_camera &sc = a.cam[s];
-  const float n[3] = {pl.x, pl.y, pl.z};
-  float G[9];
-#pragma unroll
-  for (int i = 0; i < 3; ++i)
-#pragma unroll
-    for (int j = 0; j < 3; ++j) G[3 * i + j] = a.Rrel[s][3 * i + j] - a.trel[s][i] * n[j] / pl.w;
-  float T[9];
+  const float m[3] = {pl.x * a.hm[0], pl.y * a.hm[1], pl.x * a.hm[2] + pl.y * a.hm[3] + pl.z};
 #pragma unroll
   for (int i = 0; i < 3; ++i) {
-    T[3 * i] = G[3 * i] / rc.K[0];
-    T[3 * i + 1] = G[3 * i + 1] / rc.K[4];
-    T[3 * i + 2] = -G[3 * i] * rc.K[2] / rc.K[0] - G[3 * i + 1] * rc.K[5] / rc.K[4] + G[3 * i + 2];
-  }
+    const float bi = a.hb[s][i] / pl.w;
 #pragma unroll
-  for (int j = 0; j < 3; ++j) {
-    H[j] = sc.K[0] * T[j] + sc.K[2] * T[6 + j];
-    H[3 + j] = sc.K[4] * T[3 + j] + sc.K[5] * T[6 + j];
-    H[6 + j] = sc.K[8] * T[6 + j];
+    for (int j = 0; j < 3; ++j) H[3 * i + j] = a.hA[s][3 * i + j] - bi * m[j];
   }
 }
 __device__ __forceinline__ float2 project(const float H[9], int x, int y) {
@@ -511,15 +533,82 @@ __device__ __forceinline__ float tap_rcp(float z) {
   return 1.0f / z;
 #endif
 }
+// Projection of one strong window into source s.  The window centre p0 = (px, py) goes through
+// the homography in double, from the double bases: in float, the rounding of the homography's
+// entries and of the numerators at source coordinates of ~2000 px places the whole window up to
+// ~1e-4 px off, and on low-contrast windows the NCC moves by about as much.  The centre is kept
+// as an integer texel (U0, V0) plus a float fraction, and each tap p0 + (dx, dy) as a float
+// offset from it:
+//   u(p0 + d) - uc = ((H00 - uc H20) dx + (H01 - uc H21) dy) / (Zc + H20 dx + H21 dy),
+// whose terms are small, so float arithmetic places the taps to ~1e-6 px.  The plane enters in
+// double too; the per-tap arithmetic is float.
+struct WinProj {
+  int U0, V0;                // integer part of the projected centre
+  float fu, fv;              // its fraction, in [0, 1]
+  float zc;                  // projective depth of the centre
+  float g0, g1, g3, g4;      // H00 - uc H20, H01 - uc H21, H10 - vc H20, H11 - vc H21
+  float h6, h7;              // H20, H21
+  float lox, hix, loy, hiy;  // the texture clamp [-1, W-1] x [-1, H-1] relative to (U0, V0)
+};
+// Fills wp for plane pl at pixel (px, py) of source s; false when the centre does not project
+// inside the source (the cost is then 2, DPE.cu:709-712).
+__device__ __forceinline__ bool window_projection(const PMArgs &a, int s, float4 pl, int px, int py, WinProj &wp) {
+  const double *A = a.dA[s], *b = a.db[s];
+  const double m0 = (double)pl.x * a.dm[0], m1 = (double)pl.y * a.dm[1];
+  const double m2 = (double)pl.x * a.dm[2] + (double)pl.y * a.dm[3] + (double)pl.z;
+  const double iw = 1.0 / (double)pl.w;
+  const double x = (double)px, y = (double)py;
+  const double q = (m0 * x + m1 * y + m2) * iw;  // m . p0 / w
+  const double X = A[0] * x + A[1] * y + A[2] - b[0] * q;
+  const double Y = A[3] * x + A[4] * y + A[5] - b[1] * q;
+  const double Z = A[6] * x + A[7] * y + A[8] - b[2] * q;
+  const double iz = 1.0 / Z;
+  const double uc = X * iz, vc = Y * iz;
+  const dpe_camera &sc = a.cam[s];
+  if (!(uc >= 0.0 && uc < (double)sc.width && vc >= 0.0 && vc < (double)sc.height)) return false;
+  const double U = floor(uc), V = floor(vc);
+  wp.U0 = (int)U;
+  wp.V0 = (int)V;
+  wp.fu = (float)(uc - U);
+  wp.fv = (float)(vc - V);
+  wp.zc = (float)Z;
+  const double bw0 = b[0] * iw, bw1 = b[1] * iw, bw2 = b[2] * iw;
+  const double h6 = A[6] - bw2 * m0, h7 = A[7] - bw2 * m1;
+  wp.g0 = (float)((A[0] - bw0 * m0) - uc * h6);
+  wp.g1 = (float)((A[1] - bw0 * m1) - uc * h7);
+  wp.g3 = (float)((A[3] - bw1 * m0) - vc * h6);
+  wp.g4 = (float)((A[4] - bw1 * m1) - vc * h7);
+  wp.h6 = (float)h6;
+  wp.h7 = (float)h7;
+  wp.lox = (float)(-1 - wp.U0);
+  wp.hix = (float)(a.W - 1 - wp.U0);
+  wp.loy = (float)(-1 - wp.V0);
+  wp.hiy = (float)(a.H - 1 - wp.V0);
+  return true;
+}
+// bilinear_s at (U0 + x, V0 + y): the clamp to [-1, W-1] x [-1, H-1] and the split into texel and
+// weight are taken on the offsets, which equals them on the absolute coordinates.
+template <class Src, bool kClamp = true>
+__device__ __forceinline__ float bilinear_w(const Src &src, const WinProj &wp, float x, float y) {
+  const float xc = kClamp ? fminf(fmaxf(x, wp.lox), wp.hix) : x;
+  const float yc = kClamp ? fminf(fmaxf(y, wp.loy), wp.hiy) : y;
+  int ix, iy;
+  const float fx = floor_split(xc, &ix), fy = floor_split(yc, &iy);
+  const float ax = xc - fx, ay = yc - fy;
+  const float4 v = src.fetch((wp.V0 + iy + 1) * src.pw + (wp.U0 + ix + 1));
+  const float top = (1.0f - ax) * v.x + ax * v.y;
+  const float bot = (1.0f - ax) * v.z + ax * v.w;
+  return (1.0f - ay) * top + ay * bot;
+}
 // One tap of the strong window: sample the source at the projected tap and accumulate the
-// hypothesis-dependent moments (sums of w*s, w*s^2, w*(r-c)*s over s = sample - c).
+// hypothesis-dependent moments (sums of w*s, w*s^2, w*(r-c)*s over s = sample - c).  (cx, cy, cz)
+// carry the tap column's dx terms.
 template <bool kClamp, class Src, class RW>
-__device__ __forceinline__ void strong_tap(const PMArgs &a, const float H[9], const Src &src, const RW &rw,
-                                           float bx, float by, float bz, float y, int k, float &s_s, float &s_ss,
-                                           float &s_rs) {
-  const float X = H[1] * y + bx, Y = H[4] * y + by, Z = H[7] * y + bz;
+__device__ __forceinline__ void strong_tap(const WinProj &wp, const Src &src, const RW &rw, float cx, float cy,
+                                           float cz, float dy, int k, float &s_s, float &s_ss, float &s_rs) {
+  const float X = wp.g1 * dy + cx, Y = wp.g4 * dy + cy, Z = wp.h7 * dy + cz;
   const float iz = tap_rcp(Z);
-  const float sv = bilinear_s<Src, kClamp>(src, a.W, a.H, X * iz, Y * iz) - rw.center;
+  const float sv = bilinear_w<Src, kClamp>(src, wp, wp.fu + X * iz, wp.fv + Y * iz) - rw.center;
   const float2 t = rw.tap(k);
   const float ws = t.x * sv;
   s_s += ws;
@@ -527,42 +616,39 @@ __device__ __forceinline__ void strong_tap(const PMArgs &a, const float H[9], co
   s_rs += t.y * sv;
 }
 // ComputeBilateralNCCOld (DPE.cu:696-782) with the reference window precomputed; the window loop
-// for one source sampler.
+// for one source sampler, columns dx outer and rows dy inner as the reference window's taps.
 template <bool kClamp, class Src, int kUnroll, class RW>
-__device__ __forceinline__ void strong_window(const PMArgs &a, int px, int py, const float H[9], const Src &src,
-                                              const RW &rw, float &s_s, float &s_ss, float &s_rs) {
+__device__ __forceinline__ void strong_window(const PMArgs &a, const WinProj &wp, const Src &src, const RW &rw,
+                                              float &s_s, float &s_ss, float &s_rs) {
   const int r = a.P.strong_radius, inc = a.P.strong_increment;
-  // Tap coordinates are whole numbers far below 2^24, so stepping them by float adds gives the
-  // same floats as converting each integer, without a conversion per tap.
+  // Tap offsets are small whole numbers, so stepping them by float adds gives the same floats as
+  // converting each integer, without a conversion per tap.
   if (kUnroll > 0 && r == 5 && inc == 2) {
-    const float x0 = (float)(px - 5), y0 = (float)(py - 5);
     for (int ii = 0; ii < 6; ++ii) {
-      const float x = x0 + (float)(2 * ii);
-      const float bx = H[0] * x + H[2], by = H[3] * x + H[5], bz = H[6] * x + H[8];
+      const float dx = (float)(2 * ii - 5);
+      const float cx = wp.g0 * dx, cy = wp.g3 * dx, cz = wp.h6 * dx + wp.zc;
 #pragma unroll(kUnroll > 0 ? kUnroll : 1)
       for (int jj = 0; jj < 6; ++jj)
-        strong_tap<kClamp>(a, H, src, rw, bx, by, bz, y0 + (float)(2 * jj), 6 * ii + jj, s_s, s_ss, s_rs);
+        strong_tap<kClamp>(wp, src, rw, cx, cy, cz, (float)(2 * jj - 5), 6 * ii + jj, s_s, s_ss, s_rs);
     }
   } else {
     int k = 0;
-    const float finc = (float)inc, y0 = (float)(py - r);
-    float x = (float)(px - r);
-    for (int i = -r; i <= r; i += inc, x += finc) {
-      // column x is fixed while y walks the window: the projective numerators are affine in y
-      const float bx = H[0] * x + H[2], by = H[3] * x + H[5], bz = H[6] * x + H[8];
-      float y = y0;
-      for (int j = -r; j <= r; j += inc, y += finc)
-        strong_tap<kClamp>(a, H, src, rw, bx, by, bz, y, k++, s_s, s_ss, s_rs);
+    const float finc = (float)inc, d0 = (float)(-r);
+    float dx = d0;
+    for (int i = -r; i <= r; i += inc, dx += finc) {
+      const float cx = wp.g0 * dx, cy = wp.g3 * dx, cz = wp.h6 * dx + wp.zc;
+      float dy = d0;
+      for (int j = -r; j <= r; j += inc, dy += finc)
+        strong_tap<kClamp>(wp, src, rw, cx, cy, cz, dy, k++, s_s, s_ss, s_rs);
     }
   }
 }
 template <class Src, int kUnroll, class RW>
-__device__ __forceinline__ float ncc_strong_src(const PMArgs &a, int px, int py, const float H[9], const Src &src,
-                                                const RW &rw) {
+__device__ __forceinline__ float ncc_strong_src(const PMArgs &a, const WinProj &wp, const Src &src, const RW &rw) {
   float s_s = 0.f, s_ss = 0.f, s_rs = 0.f;
   // (a clamp-free copy of the loop for windows that project inside the source measured slower:
   // the second copy costs registers under the strong update's occupancy bound)
-  strong_window<true, Src, kUnroll>(a, px, py, H, src, rw, s_s, s_ss, s_rs);
+  strong_window<true, Src, kUnroll>(a, wp, src, rw, s_s, s_ss, s_rs);
   const float m_s = s_s * rw.inv_wsum;
   const float var_s = s_ss * rw.inv_wsum - m_s * m_s;
   if (rw.var_r < 1e-5f || var_s < 1e-5f) return 2.0f;
@@ -571,13 +657,10 @@ __device__ __forceinline__ float ncc_strong_src(const PMArgs &a, int px, int py,
 }
 template <int kStage = DPE_STAGE_FP32, int kUnroll = 0, class RW>
 __device__ __forceinline__ float ncc_strong(const PMArgs &a, int px, int py, int s, float4 pl, const RW &rw) {
-  float H[9];
-  homography(a, s, pl, H);
-  const float2 pt = project(H, px, py);
-  const dpe_camera &sc = a.cam[s];
-  if (pt.x >= sc.width || pt.x < 0.0f || pt.y >= sc.height || pt.y < 0.0f) return 2.0f;
+  WinProj wp;
+  if (!window_projection(a, s, pl, px, py, wp)) return 2.0f;
   if (rw.cnt) atomicAdd(rw.cnt, 1ull);
-  return ncc_strong_src<decltype(SrcOf<kStage>::make(a, s)), kUnroll, RW>(a, px, py, H, SrcOf<kStage>::make(a, s), rw);
+  return ncc_strong_src<decltype(SrcOf<kStage>::make(a, s)), kUnroll, RW>(a, wp, SrcOf<kStage>::make(a, s), rw);
 }
 
 // ------------------------------------------------------------------ strong NCC adjoint
@@ -588,36 +671,18 @@ __device__ __forceinline__ float ncc_strong(const PMArgs &a, int px, int py, int
 //   pass 1: the moments and the cost, exactly as ncc_strong;
 //   pass 2: per tap, dC/ds (s = bilinear sample) from the moments, through the bilinear slope to
 //           the projected point, through the projection to the homography entries.
-// dC/dH then goes through H = K_s (R - t n^T / w) K_r^-1 to the plane.  Where the cost is the
+// dC/dH then goes through H = A - (b / w) m^T (homography_base) to the plane.  Where the cost is the
 // constant 2 (centre outside the source, flat window) or clamped to [0, 2], the gradient is zero.
 template <class RW>
 __device__ __forceinline__ float ncc_strong_adjoint(const PMArgs &a, int px, int py, int s, float4 pl,
                                                     const RW &rw, float g[4], float *gimg, float gscale = 1.0f) {
   g[0] = g[1] = g[2] = g[3] = 0.0f;
-  float H[9];
-  homography(a, s, pl, H);
-  const float2 pt = project(H, px, py);
-  const dpe_camera &sc = a.cam[s];
-  if (pt.x >= sc.width || pt.x < 0.0f || pt.y >= sc.height || pt.y < 0.0f) return 2.0f;
+  WinProj wp;
+  if (!window_projection(a, s, pl, px, py, wp)) return 2.0f;
   const int r = a.P.strong_radius, inc = a.P.strong_increment;
-  const float *__restrict__ img = a.img[s];
+  // pass 1: ncc_strong's own window loop
   float s_s = 0.f, s_ss = 0.f, s_rs = 0.f;
-  int k = 0;
-  for (int i = -r; i <= r; i += inc) {
-    const float x = (float)(px + i);
-    const float bx = H[0] * x + H[2], by = H[3] * x + H[5], bz = H[6] * x + H[8];
-    for (int j = -r; j <= r; j += inc) {
-      const float y = (float)(py + j);
-      const float X = H[1] * y + bx, Y = H[4] * y + by, Z = H[7] * y + bz;
-      const float iz = 1.0f / Z;
-      const float sv = bilinear(img, a.pad_w, a.W, a.H, X * iz, Y * iz) - rw.center;
-      const float ws = rw.w(k) * sv;
-      s_s += ws;
-      s_ss += ws * sv;
-      s_rs += rw.wr(k) * sv;
-      ++k;
-    }
-  }
+  strong_window<true, SrcF32, 0>(a, wp, src_f32(a, s), rw, s_s, s_ss, s_rs);
   const float m_s = s_s * rw.inv_wsum;
   const float var_s = s_ss * rw.inv_wsum - m_s * m_s;
   if (rw.var_r < 1e-5f || var_s < 1e-5f) return 2.0f;
@@ -630,26 +695,31 @@ __device__ __forceinline__ float ncc_strong_adjoint(const PMArgs &a, int px, int
   const float ka = -rw.inv_wsum / sq, kb = rw.inv_wsum * cov / (var_s * sq);
   float gH[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   const int W = a.W, Hh = a.H, pw = a.pad_w;
-  k = 0;
+  const float *__restrict__ img = a.img[s];
+  int k = 0;
   for (int i = -r; i <= r; i += inc) {
-    const float x = (float)(px + i);
-    const float bx = H[0] * x + H[2], by = H[3] * x + H[5], bz = H[6] * x + H[8];
+    const float dx = (float)i, x = (float)(px + i);
+    const float cx = wp.g0 * dx, cy = wp.g3 * dx, cz = wp.h6 * dx + wp.zc;
     for (int j = -r; j <= r; j += inc) {
-      const float y = (float)(py + j);
-      const float X = H[1] * y + bx, Y = H[4] * y + by, Z = H[7] * y + bz;
-      const float iz = 1.0f / Z;
-      const float u = X * iz, v = Y * iz;
-      const float xc = fminf(fmaxf(u, -1.0f), (float)(W - 1)), yc = fminf(fmaxf(v, -1.0f), (float)(Hh - 1));
-      const float fx = floorf(xc), fy = floorf(yc);
+      const float dy = (float)j, y = (float)(py + j);
+      const float X = wp.g1 * dy + cx, Y = wp.g4 * dy + cy, Z = wp.h7 * dy + cz;
+      const float iz = tap_rcp(Z);
+      const float uo = wp.fu + X * iz, vo = wp.fv + Y * iz;  // offsets from (U0, V0)
+      const float xc = fminf(fmaxf(uo, wp.lox), wp.hix), yc = fminf(fmaxf(vo, wp.loy), wp.hiy);
+      int ix, iy;
+      const float fx = floor_split(xc, &ix), fy = floor_split(yc, &iy);
       const float ax = xc - fx, ay = yc - fy;
-      const int o = ((int)fy + 1) * pw + ((int)fx + 1);
+      const int x0 = wp.U0 + ix, y0 = wp.V0 + iy;
+      const int o = (y0 + 1) * pw + (x0 + 1);
       const float v00 = img[o], v10 = img[o + 1], v01 = img[o + pw], v11 = img[o + pw + 1];
       const float sv = (1.0f - ay) * ((1.0f - ax) * v00 + ax * v10) + ay * ((1.0f - ax) * v01 + ax * v11) - rw.center;
       const float rc = texel(a, 0, px + i, py + j) - rw.center;  // r_k - c
       const float dc = rw.w(k) * (ka * (rc - rw.mean_r) + kb * (sv - m_s));
       // slope of the sample; zero along a clamped coordinate
-      const float dsx = (u > -1.0f && u < (float)(W - 1)) ? (1.0f - ay) * (v10 - v00) + ay * (v11 - v01) : 0.0f;
-      const float dsy = (v > -1.0f && v < (float)(Hh - 1)) ? (1.0f - ax) * (v01 - v00) + ax * (v11 - v10) : 0.0f;
+      const float dsx = (uo > wp.lox && uo < wp.hix) ? (1.0f - ay) * (v10 - v00) + ay * (v11 - v01) : 0.0f;
+      const float dsy = (vo > wp.loy && vo < wp.hiy) ? (1.0f - ax) * (v01 - v00) + ax * (v11 - v10) : 0.0f;
+      // u = X' / Z' with X' = H0. p, Z' = H2. p: du/dH0j = p_j / Z', du/dH2j = -u p_j / Z'
+      const float u = (float)wp.U0 + uo, v = (float)wp.V0 + vo;
       const float gu = dc * dsx * iz, gv = dc * dsy * iz;
       gH[0] += gu * x; gH[1] += gu * y; gH[2] += gu;
       gH[3] += gv * x; gH[4] += gv * y; gH[5] += gv;
@@ -657,7 +727,6 @@ __device__ __forceinline__ float ncc_strong_adjoint(const PMArgs &a, int px, int
       gH[6] += gz * x; gH[7] += gz * y; gH[8] += gz;
       if (gimg) {
         const float dcs = dc * gscale;  // the upstream weight of this query's cost
-        const int x0 = (int)fx, y0 = (int)fy;
         const int xa = min(max(x0, 0), W - 1), xb = min(max(x0 + 1, 0), W - 1);
         const int ya = min(max(y0, 0), Hh - 1), yb = min(max(y0 + 1, 0), Hh - 1);
         atomicAdd(&gimg[(size_t)ya * W + xa], dcs * (1.0f - ax) * (1.0f - ay));
@@ -668,34 +737,16 @@ __device__ __forceinline__ float ncc_strong_adjoint(const PMArgs &a, int px, int
       ++k;
     }
   }
-  // H = Ks T, Ks = [[K0 0 K2] [0 K4 K5] [0 0 K8]]: gT = Ks^T gH
-  const dpe_camera &rc0 = a.cam[0];
-  float gT[9];
-  for (int b = 0; b < 3; ++b) {
-    gT[b] = sc.K[0] * gH[b];
-    gT[3 + b] = sc.K[4] * gH[3 + b];
-    gT[6 + b] = sc.K[2] * gH[b] + sc.K[5] * gH[3 + b] + sc.K[8] * gH[6 + b];
-  }
-  // T = M Kr^-1 (rows: T0 = M0 / f, T1 = M1 / fy, T2 = M2 - M0 cx / f - M1 cy / fy): gM
-  float gM[9];
-  for (int ra = 0; ra < 3; ++ra) {
-    gM[3 * ra] = (gT[3 * ra] - gT[3 * ra + 2] * rc0.K[2]) / rc0.K[0];
-    gM[3 * ra + 1] = (gT[3 * ra + 1] - gT[3 * ra + 2] * rc0.K[5]) / rc0.K[4];
-    gM[3 * ra + 2] = gT[3 * ra + 2];
-  }
-  // M = Rrel - t n^T / w
-  const float n3[3] = {pl.x, pl.y, pl.z};
-  const float *t = a.trel[s];
-  float gw = 0.0f;
-  for (int b = 0; b < 3; ++b) {
-    float gn = 0.0f;
-    for (int ra = 0; ra < 3; ++ra) {
-      gn += gM[3 * ra + b] * t[ra];
-      gw += gM[3 * ra + b] * t[ra] * n3[b];
-    }
-    g[b] = -gn / pl.w;
-  }
-  g[3] = gw / (pl.w * pl.w);
+  // H = A - (b / w) m^T, m = (nx / fx, ny / fy, nz - nx cx / fx - ny cy / fy):
+  // dC/dm_j = -sum_i gH_ij b_i / w and dC/dw = -sum_j (dC/dm_j) m_j / w
+  const float m[3] = {pl.x * a.hm[0], pl.y * a.hm[1], pl.x * a.hm[2] + pl.y * a.hm[3] + pl.z};
+  const float *b = a.hb[s];
+  float gm[3];
+  for (int j = 0; j < 3; ++j) gm[j] = -(gH[j] * b[0] + gH[3 + j] * b[1] + gH[6 + j] * b[2]) / pl.w;
+  g[0] = gm[0] * a.hm[0] + gm[2] * a.hm[2];
+  g[1] = gm[1] * a.hm[1] + gm[2] * a.hm[3];
+  g[2] = gm[2];
+  g[3] = -(gm[0] * m[0] + gm[1] * m[1] + gm[2] * m[2]) / pl.w;
   return cost;
 }
 

@@ -638,62 +638,68 @@ __device__ __forceinline__ int find_min_cost_index(const float *c, int n) {
 // Around the current plane (n, depth) it takes the cost of each sampled source j and its gradient
 // (ncc_strong_adjoint) in the local parameters theta = (d depth, d a1, d a2), the normal tilted
 // within its tangent plane (n' = normalize(n + a1 e1 + a2 e2)), and solves the damped normal
-// equations  (J^T V J + lambda diag(J^T V J)) theta = -J^T V c  (V = the sample counts).  The
+// equations  (J^T V J + lambda diag(J^T V J)) theta = -J^T V c  (V = the view weights).  The
 // resulting plane is a hypothesis like the random ones: kept only when its cost is lower and its
 // depth lies in range.  It draws no random numbers, so the rest of the update is unchanged.
-template <int kStage, class RW, class A>
-__device__ __forceinline__ void gn_hypothesis(const PMArgs &a, int px, int py, const RW &rw, const A *act,
-                                              int na, const uint8_t *vw, float wn, float4 *pl_now, float *depth_now,
-                                              float *cost_now) {
-  const dpe_camera &rc = a.cam[0];
-  const float4 p = *pl_now;
-  const float ray0 = ((float)px - rc.K[2]) / rc.K[0], ray1 = ((float)py - rc.K[5]) / rc.K[4];
-  const float nr = p.x * ray0 + p.y * ray1 + p.z;
-  const float d0 = *depth_now;
-  // tangent basis of the normal
-  float e1x, e1y, e1z;
-  if (fabsf(p.x) < 0.9f) { e1x = 0.0f; e1y = p.z; e1z = -p.y; }  // n x (1, 0, 0)
-  else { e1x = -p.z; e1y = 0.0f; e1z = p.x; }                    // n x (0, 1, 0)
-  const float e1n = 1.0f / sqrtf(e1x * e1x + e1y * e1y + e1z * e1z);
-  e1x *= e1n; e1y *= e1n; e1z *= e1n;
-  const float e2x = p.y * e1z - p.z * e1y, e2y = p.z * e1x - p.x * e1z, e2z = p.x * e1y - p.y * e1x;
-  const float e1r = e1x * ray0 + e1y * ray1 + e1z, e2r = e2x * ray0 + e2y * ray1 + e2z;
-  float A00 = 0, A01 = 0, A02 = 0, A11 = 0, A12 = 0, A22 = 0, b0 = 0, b1 = 0, b2 = 0;
-  for (int q = 0; q < na; ++q) {
-    const int j = act[q];
-    float g[4];
-    const float c = ncc_strong_adjoint(a, px, py, j + 1, p, rw, g, nullptr);
-    if (!(c > 0.0f && c < 2.0f)) continue;
-    // w = -depth (n . ray): dC/ddepth = g_w (-(n . ray)); tilting n moves w by -depth (e . ray)
-    const float jd = -g[3] * nr;
-    const float j1 = g[0] * e1x + g[1] * e1y + g[2] * e1z - g[3] * d0 * e1r;
-    const float j2 = g[0] * e2x + g[1] * e2y + g[2] * e2z - g[3] * d0 * e2r;
-    const float v = (float)vw[j];
-    A00 += v * jd * jd; A01 += v * jd * j1; A02 += v * jd * j2;
-    A11 += v * j1 * j1; A12 += v * j1 * j2; A22 += v * j2 * j2;
-    b0 -= v * jd * c; b1 -= v * j1 * c; b2 -= v * j2 * c;
-  }
+struct GnFrame {
+  float ray0, ray1, nr, d0;  // the pixel's ray (z = 1), n . ray, the current depth
+  float e1x, e1y, e1z, e2x, e2y, e2z, e1r, e2r;  // tangent basis of n, e . ray
+};
+__device__ __forceinline__ GnFrame gn_frame(const dpe_camera &rc, int px, int py, float4 p, float d0) {
+  GnFrame f;
+  f.ray0 = ((float)px - rc.K[2]) / rc.K[0];
+  f.ray1 = ((float)py - rc.K[5]) / rc.K[4];
+  f.nr = p.x * f.ray0 + p.y * f.ray1 + p.z;
+  f.d0 = d0;
+  if (fabsf(p.x) < 0.9f) { f.e1x = 0.0f; f.e1y = p.z; f.e1z = -p.y; }  // n x (1, 0, 0)
+  else { f.e1x = -p.z; f.e1y = 0.0f; f.e1z = p.x; }                    // n x (0, 1, 0)
+  const float e1n = 1.0f / sqrtf(f.e1x * f.e1x + f.e1y * f.e1y + f.e1z * f.e1z);
+  f.e1x *= e1n; f.e1y *= e1n; f.e1z *= e1n;
+  f.e2x = p.y * f.e1z - p.z * f.e1y; f.e2y = p.z * f.e1x - p.x * f.e1z; f.e2z = p.x * f.e1y - p.y * f.e1x;
+  f.e1r = f.e1x * f.ray0 + f.e1y * f.ray1 + f.e1z;
+  f.e2r = f.e2x * f.ray0 + f.e2y * f.ray1 + f.e2z;
+  return f;
+}
+// Adds source j's terms (view weight v) to the normal equations m = (A00 A01 A02 A11 A12 A22 b0 b1 b2).
+template <class RW>
+__device__ __forceinline__ void gn_accumulate(const PMArgs &a, int px, int py, const RW &rw, float4 p,
+                                              const GnFrame &f, int j, float v, float m[9]) {
+  float g[4];
+  const float c = ncc_strong_adjoint(a, px, py, j + 1, p, rw, g, nullptr);
+  if (!(c > 0.0f && c < 2.0f)) return;
+  // w = -depth (n . ray): dC/ddepth = g_w (-(n . ray)); tilting n moves w by -depth (e . ray)
+  const float jd = -g[3] * f.nr;
+  const float j1 = g[0] * f.e1x + g[1] * f.e1y + g[2] * f.e1z - g[3] * f.d0 * f.e1r;
+  const float j2 = g[0] * f.e2x + g[1] * f.e2y + g[2] * f.e2z - g[3] * f.d0 * f.e2r;
+  m[0] += v * jd * jd; m[1] += v * jd * j1; m[2] += v * jd * j2;
+  m[3] += v * j1 * j1; m[4] += v * j1 * j2; m[5] += v * j2 * j2;
+  m[6] -= v * jd * c; m[7] -= v * j1 * c; m[8] -= v * j2 * c;
+}
+// Solves the damped normal equations m around plane p; false when singular, when the new plane
+// does not face the camera, or when its depth is out of range.  *t receives the new plane.
+__device__ __forceinline__ bool gn_solve(const PMArgs &a, int px, int py, float4 p, const GnFrame &f,
+                                         const float m[9], float4 *t) {
   const float lambda = 0.1f;
-  A00 *= 1.0f + lambda; A11 *= 1.0f + lambda; A22 *= 1.0f + lambda;
+  const float A00 = m[0] * (1.0f + lambda), A01 = m[1], A02 = m[2];
+  const float A11 = m[3] * (1.0f + lambda), A12 = m[4], A22 = m[5] * (1.0f + lambda);
+  const float b0 = m[6], b1 = m[7], b2 = m[8];
   const float c00 = A11 * A22 - A12 * A12, c01 = A02 * A12 - A01 * A22, c02 = A01 * A12 - A02 * A11;
   const float det = A00 * c00 + A01 * c01 + A02 * c02;
-  if (!(fabsf(det) > 1e-30f) || !isfinite(det)) return;
+  if (!(fabsf(det) > 1e-30f) || !isfinite(det)) return false;
   const float c11 = A00 * A22 - A02 * A02, c12 = A01 * A02 - A00 * A12, c22 = A00 * A11 - A01 * A01;
   const float inv = 1.0f / det;
   const float td = (c00 * b0 + c01 * b1 + c02 * b2) * inv;
   const float t1 = (c01 * b0 + c11 * b1 + c12 * b2) * inv;
   const float t2 = (c02 * b0 + c12 * b1 + c22 * b2) * inv;
-  float nx = p.x + t1 * e1x + t2 * e2x, ny = p.y + t1 * e1y + t2 * e2y, nz = p.z + t1 * e1z + t2 * e2z;
+  float nx = p.x + t1 * f.e1x + t2 * f.e2x, ny = p.y + t1 * f.e1y + t2 * f.e2y, nz = p.z + t1 * f.e1z + t2 * f.e2z;
   const float nn = 1.0f / sqrtf(nx * nx + ny * ny + nz * nz);
   nx *= nn; ny *= nn; nz *= nn;
-  if (!(nx * ray0 + ny * ray1 + nz < 0.0f)) return;  // the plane must face the camera
-  const float dn = d0 + td;
-  if (!(dn >= a.P.depth_min && dn <= a.P.depth_max)) return;
-  float4 t = make_float4(nx, ny, nz, 0.0f);
-  t.w = dist_to_origin(rc, px, py, dn, t);
-  const float tc = weighted_ncc<kStage>(a, px, py, t, rw, act, na, vw) / wn;
-  const float db = depth_from_plane(rc, t, px, py);
-  if (db >= a.P.depth_min && db <= a.P.depth_max && tc < *cost_now) { *depth_now = db; *pl_now = t; *cost_now = tc; }
+  if (!(nx * f.ray0 + ny * f.ray1 + nz < 0.0f)) return false;  // the plane must face the camera
+  const float dn = f.d0 + td;
+  if (!(dn >= a.P.depth_min && dn <= a.P.depth_max)) return false;
+  *t = make_float4(nx, ny, nz, 0.0f);
+  t->w = dist_to_origin(a.cam[0], px, py, dn, *t);
+  return true;
 }
 
 // ------------------------------------------------------------------ strong update (DPE.cu:1218-1670, 1069-1122)
@@ -714,6 +720,8 @@ __device__ __forceinline__ void gn_hypothesis(const PMArgs &a, int px, int py, c
 //   6  best candidate, acceptance, refinement planes (lane 0)
 //   7  refinement costs (lanes split plane x source)
 //   8  refinement decisions, outputs (lane 0)
+//   9-11  with the Gauss-Newton hypothesis only: its normal equations (lanes split the sources,
+//         shuffle sums), its costs (lanes split the sources), its decision and the outputs (lane 0)
 constexpr int kCoopPix = 16, kCoopLanes = 8, kCoopThreads = kCoopPix * kCoopLanes;
 
 // The strong NCC as the cooperative strong update calls it, inlined at each call site (measured:
@@ -1129,28 +1137,12 @@ __device__ __forceinline__ void strong_p7(const CoopCtx &c) {
   }
 }
 
-// Phase 8 (lane 0): the refinement decisions in order, the optional Gauss-Newton plane, outputs.
-template <int kStage, bool kGN>
-__device__ __forceinline__ void strong_p8(const CoopCtx &c) {
-  if (!c.live || c.lane != 0) return;
+// The pixel's outputs after its last decision.
+__device__ __forceinline__ void strong_write(const CoopCtx &c, float4 pl_now, float cost_now) {
   const PMArgs &a = *c.a;
-  const dpe_camera &rc = a.cam[0];
   [[maybe_unused]] const long long L = (long long)a.W * a.H;
-  const int center = c.center, na = c.P->na, n = c.n;
+  const int center = c.center;
   CoopPixel &P = *c.P;
-  const float dmin = a.P.depth_min, dmax = a.P.depth_max;
-  float depth_now = P.depth_now, cost_now = P.cost_now;
-  float4 pl_now = P.pl_now;
-  for (int h = 0; h < 5; ++h) {
-    const float4 t = P.hyp[h];
-    float tc = 0.0f;
-    for (int q = 0; q < na; ++q) tc += P.vw[P.act[q]] * c.hc[(1 + h) * n + q];
-    tc /= P.wn;
-    const float db = depth_from_plane(rc, t, c.px, c.py);
-    if (db >= dmin && db <= dmax && tc < cost_now) { depth_now = db; pl_now = t; cost_now = tc; }
-  }
-  if (kGN && na > 0)
-    gn_hypothesis<kStage>(a, c.px, c.py, c.window(), P.act, na, P.vw, P.wn, &pl_now, &depth_now, &cost_now);
   G(a.rng_ctr, center, L, 215) = P.rng_ctr;
   G(a.views, center, L, 216) = P.views_new;
   store_vweight(&G(a.vweight, center, L, 217), P.vw);
@@ -1163,6 +1155,91 @@ __device__ __forceinline__ void strong_p8(const CoopCtx &c) {
     G(a.plane, center, L, 222) = pl_now;
   }
 }
+
+// Phase 8 (lane 0): the refinement decisions in order, then the outputs -- or, with the
+// Gauss-Newton hypothesis, the state phases 9-11 continue from.
+template <int kStage, bool kGN>
+__device__ __forceinline__ void strong_p8(const CoopCtx &c) {
+  if (!c.live || c.lane != 0) return;
+  const PMArgs &a = *c.a;
+  const dpe_camera &rc = a.cam[0];
+  const int na = c.P->na, n = c.n;
+  CoopPixel &P = *c.P;
+  const float dmin = a.P.depth_min, dmax = a.P.depth_max;
+  float depth_now = P.depth_now, cost_now = P.cost_now;
+  float4 pl_now = P.pl_now;
+  for (int h = 0; h < 5; ++h) {
+    const float4 t = P.hyp[h];
+    float tc = 0.0f;
+    for (int q = 0; q < na; ++q) tc += P.vw[P.act[q]] * c.hc[(1 + h) * n + q];
+    tc /= P.wn;
+    const float db = depth_from_plane(rc, t, c.px, c.py);
+    if (db >= dmin && db <= dmax && tc < cost_now) { depth_now = db; pl_now = t; cost_now = tc; }
+  }
+  if (kGN) {
+    P.pl_now = pl_now; P.depth_now = depth_now; P.cost_now = cost_now;
+    return;
+  }
+  strong_write(c, pl_now, cost_now);
+}
+
+#ifdef __CUDA_ARCH__
+// Phases 9-11, the Gauss-Newton hypothesis split over the lanes of a pixel.
+// Phase 9: lane q adds the normal equations of sampled sources q, q + 8, ...; the lanes' sums are
+// added by shuffles inside each 8-lane group (a pixel's lanes are 8 consecutive threads of one
+// warp, and every thread of the block takes part); lane 0 solves and keeps the plane in hyp[0].
+template <int kStage>
+__device__ __forceinline__ void strong_p9_gn(const CoopCtx &c) {
+  static_assert(kCoopLanes == 8 && kCoopThreads % 32 == 0, "lane groups must tile whole warps");
+  CoopPixel &P = *c.P;
+  const bool on = c.live && P.na > 0;
+  float m[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  GnFrame f{};
+  if (on) {
+    const PMArgs &a = *c.a;
+    f = gn_frame(a.cam[0], c.px, c.py, P.pl_now, P.depth_now);
+    const SmemWindow rw = c.window();
+    for (int q = c.lane; q < P.na; q += kCoopLanes)
+      gn_accumulate(a, c.px, c.py, rw, P.pl_now, f, P.act[q], (float)P.vw[P.act[q]], m);
+  }
+#pragma unroll
+  for (int k = 0; k < 9; ++k)
+#pragma unroll
+    for (int off = 1; off < kCoopLanes; off <<= 1) m[k] += __shfl_xor_sync(0xffffffffu, m[k], off, kCoopLanes);
+  if (on && c.lane == 0) {
+    float4 t;
+    const bool ok = gn_solve(*c.a, c.px, c.py, P.pl_now, f, m, &t);
+    P.flag[0] = ok ? 1 : 0;
+    if (ok) P.hyp[0] = t;
+  }
+}
+// Phase 10: the hypothesis' cost against each sampled source, split over the lanes (hc row 0).
+template <int kStage>
+__device__ __forceinline__ void strong_p10_gn(const CoopCtx &c) {
+  if (!c.live) return;
+  const CoopPixel &P = *c.P;
+  if (P.na == 0 || !P.flag[0]) return;
+  const SmemWindow rw = c.window();
+  for (int q = c.lane; q < P.na; q += kCoopLanes) c.hc[q] = coop_ncc<kStage>(*c.a, c.px, c.py, P.act[q] + 1, P.hyp[0], rw);
+}
+// Phase 11 (lane 0): the weighted cost in list order, the decision, the outputs.
+__device__ __forceinline__ void strong_p11_gn(const CoopCtx &c) {
+  if (!c.live || c.lane != 0) return;
+  const PMArgs &a = *c.a;
+  const CoopPixel &P = *c.P;
+  float4 pl_now = P.pl_now;
+  float cost_now = P.cost_now;
+  if (P.na > 0 && P.flag[0]) {
+    float tc = 0.0f;
+    for (int q = 0; q < P.na; ++q) tc += P.vw[P.act[q]] * c.hc[q];
+    tc /= P.wn;
+    const float4 t = P.hyp[0];
+    const float db = depth_from_plane(a.cam[0], t, c.px, c.py);
+    if (db >= a.P.depth_min && db <= a.P.depth_max && tc < cost_now) { pl_now = t; cost_now = tc; }
+  }
+  strong_write(c, pl_now, cost_now);
+}
+#endif
 
 // One phase for one thread (host builds of this source run the phases in lock-step over a block).
 template <int kStage, bool kGN>
@@ -1205,6 +1282,16 @@ __global__ void __launch_bounds__(kCoopThreads, DPE_STRONG_MIN_BLOCKS) k_strong_
   strong_p7<kStage>(c);
   __syncthreads();
   strong_p8<kStage, kGN>(c);
+#ifdef __CUDA_ARCH__
+  if constexpr (kGN) {
+    __syncthreads();
+    strong_p9_gn<kStage>(c);
+    __syncthreads();
+    strong_p10_gn<kStage>(c);
+    __syncthreads();
+    strong_p11_gn(c);
+  }
+#endif
 }
 
 

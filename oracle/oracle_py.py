@@ -47,6 +47,7 @@ def load() -> C.CDLL:
     lib.oracle_set_raw_moments.argtypes = [C.c_int]
     lib.oracle_set_ref_addressing.argtypes = [C.c_int]
     lib.oracle_set_serial_race.argtypes = [C.c_int]
+    lib.oracle_set_ref_homography.argtypes = [C.c_int]
     lib.oracle_ncc_strong_grad.argtypes = [C.POINTER(D.NCCQuery), C.c_void_p, C.c_void_p, C.c_void_p]
     _lib = lib
     return lib
@@ -63,6 +64,12 @@ def set_ref_addressing(on: bool) -> None:
     load().oracle_set_ref_addressing(1 if on else 0)
 
 
+def set_ref_homography(on: bool) -> None:
+    """Compose the homography in the reference's float operation order (DPE.cu:457-517) instead of
+    from camera products composed in double and rounded once (the CUDA kernels' form)."""
+    load().oracle_set_ref_homography(1 if on else 0)
+
+
 def set_serial_race(on: bool) -> None:
     """Resolve the edge-aware update's same-colour read race (Q1) as a serial raster-order run does
     (default: a snapshot taken before each colour pass, the CUDA kernels' resolution)."""
@@ -70,10 +77,12 @@ def set_serial_race(on: bool) -> None:
 
 
 def reference_arithmetic(on: bool) -> None:
-    """Raw moments and the reference's texture addressing together: the arithmetic of the reference's
-    own DPE.cu, for bit-for-bit comparison with its host build (oracle/ref_py.py)."""
+    """Raw moments, the reference's texture addressing and its float homography together: the
+    arithmetic of the reference's own DPE.cu, for bit-for-bit comparison with its host build
+    (oracle/ref_py.py)."""
     set_raw_moments(on)
     set_ref_addressing(on)
+    set_ref_homography(on)
 
 
 def philox(ctr, key) -> np.ndarray:

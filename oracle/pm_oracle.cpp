@@ -40,6 +40,9 @@ static const float kPi = 3.14159265358979323846f;
 // default samples at x itself (the CUDA kernels' addressing); oracle_set_ref_addressing(1) adds
 // the round trip, for bit-for-bit comparisons with the reference's own code compiled for the CPU.
 static bool g_ref_addressing = false;
+// The reference's float operation order for the homography (homography_ref) instead of the
+// double-composed camera part (homography_base).
+static bool g_ref_homography = false;
 
 // The same-colour read race of the edge-aware strong update (quirk Q1, DPE.cu:1279/1316): by
 // default the edge branch reads a snapshot taken before each colour pass (the CUDA kernels'
@@ -47,6 +50,14 @@ static bool g_ref_addressing = false;
 // instead -- the up-left same-colour candidate has already been updated when it is read -- which
 // is how the reference's own kernels behave when compiled for the CPU and run one thread at a time.
 static bool g_serial_race = false;
+
+// A strong window projected into a source (window_projection): its centre as an integer texel
+// (U0, V0) plus a float fraction (fu, fv), the per-tap terms, and the texture clamp relative to
+// (U0, V0).
+struct WinProj {
+  int U0, V0;
+  float fu, fv, zc, g0, g1, g3, g4, h6, h7, lox, hix, loy, hiy;
+};
 
 struct Image {
   const float *data = nullptr;
@@ -74,6 +85,20 @@ struct Image {
     const float bot = (1.0f - ax) * v01 + ax * v11;
     return (1.0f - ay) * top + ay * bot;
   }
+  // bilinear() at (U0 + x, V0 + y), with the clamp to [-1, w-1] x [-1, h-1] taken on the offsets
+  // ([lox, hix] x [loy, hiy] = the clamp shifted by (U0, V0)), which equals it on the sum.
+  float bilinear_off(const WinProj &wp, float x, float y) const {
+    const float xc = std::fmin(std::fmax(x, wp.lox), wp.hix);
+    const float yc = std::fmin(std::fmax(y, wp.loy), wp.hiy);
+    const float fx = std::floor(xc), fy = std::floor(yc);
+    const int x0 = wp.U0 + (int)fx, y0 = wp.V0 + (int)fy;
+    const float ax = xc - fx, ay = yc - fy;
+    const float v00 = texel(x0, y0), v10 = texel(x0 + 1, y0);
+    const float v01 = texel(x0, y0 + 1), v11 = texel(x0 + 1, y0 + 1);
+    const float top = (1.0f - ax) * v00 + ax * v10;
+    const float bot = (1.0f - ax) * v01 + ax * v11;
+    return (1.0f - ay) * top + ay * bot;
+  }
   double bilinear_fp64(double x, double y) const {
     const double xc = std::fmin(std::fmax(x, -1.0), (double)(w - 1));
     const double yc = std::fmin(std::fmax(y, -1.0), (double)(h - 1));
@@ -94,8 +119,9 @@ static inline void setBit(uint32_t *v, int n) { *v |= (uint32_t)(1u << n); }
 static inline void unSetBit(uint32_t *v, int n) { *v &= (uint32_t)(0xFFFFFFFEu << n); }
 
 // ----------------------------------------------------------------------------- camera geometry
-// DPE.cu:457-517
-static void homography(const dpe_camera &rc, const dpe_camera &sc, const f4 &pl, float H[9]) {
+// DPE.cu:457-517, in the reference's float operation order: the relative pose, G = Rrel - trel n^T / w,
+// then G Kr^-1 and Ks (G Kr^-1), every step in float.
+static void homography_ref(const dpe_camera &rc, const dpe_camera &sc, const f4 &pl, float H[9]) {
   float rC[3], sC[3];
   for (int k = 0; k < 3; ++k) {
     rC[k] = -(rc.R[k] * rc.t[0] + rc.R[3 + k] * rc.t[1] + rc.R[6 + k] * rc.t[2]);
@@ -121,6 +147,103 @@ static void homography(const dpe_camera &rc, const dpe_camera &sc, const f4 &pl,
     H[3 + b] = sc.K[4] * T[3 + b] + sc.K[5] * T[6 + b];
     H[6 + b] = sc.K[8] * T[6 + b];
   }
+}
+
+// The same homography H = Ks (Rrel - trel n^T / w) Kr^-1 written as A - b m^T / w with
+//   A = Ks Rrel Kr^-1,  b = Ks trel,  m = Kr^-T n = (nx / fx, ny / fy, nz - nx cx / fx - ny cy / fy),
+// Rrel = Rs Rr^T, trel = Rs (Cr - Cs), C = -R^T t.  The plane-independent A, b and the entries of
+// Kr^-1 (dm = (1/fx, 1/fy, -cx/fx, -cy/fy)) are composed in double once per call, kept in double
+// for the projection of window centres (window_projection) and rounded once to float for the
+// float homography.  Composing the camera products in float, as the reference does, moves the
+// entries of H by a few float ulps, which at source coordinates of ~2000 px places a window
+// ~1e-4 px off and on low-contrast windows moves the NCC by about as much.
+struct HomographyBase {
+  double dA[9], db[3], dm[4];
+  float A[9], b[3], m[4];
+};
+static HomographyBase homography_base(const dpe_camera &rc, const dpe_camera &sc) {
+  double rC[3], sC[3], Rr[9], Cr[3], tr[3], MK[9];
+  for (int k = 0; k < 3; ++k) {
+    rC[k] = -((double)rc.R[k] * rc.t[0] + (double)rc.R[3 + k] * rc.t[1] + (double)rc.R[6 + k] * rc.t[2]);
+    sC[k] = -((double)sc.R[k] * sc.t[0] + (double)sc.R[3 + k] * sc.t[1] + (double)sc.R[6 + k] * sc.t[2]);
+  }
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b)
+      Rr[3 * a + b] = (double)sc.R[3 * a] * rc.R[3 * b] + (double)sc.R[3 * a + 1] * rc.R[3 * b + 1] +
+                      (double)sc.R[3 * a + 2] * rc.R[3 * b + 2];
+  for (int k = 0; k < 3; ++k) Cr[k] = rC[k] - sC[k];
+  for (int a = 0; a < 3; ++a)
+    tr[a] = (double)sc.R[3 * a] * Cr[0] + (double)sc.R[3 * a + 1] * Cr[1] + (double)sc.R[3 * a + 2] * Cr[2];
+  HomographyBase h;
+  h.dm[0] = 1.0 / rc.K[0];
+  h.dm[1] = 1.0 / rc.K[4];
+  h.dm[2] = -(double)rc.K[2] / rc.K[0];
+  h.dm[3] = -(double)rc.K[5] / rc.K[4];
+  for (int a = 0; a < 3; ++a) {
+    MK[3 * a] = Rr[3 * a] * h.dm[0];
+    MK[3 * a + 1] = Rr[3 * a + 1] * h.dm[1];
+    MK[3 * a + 2] = Rr[3 * a] * h.dm[2] + Rr[3 * a + 1] * h.dm[3] + Rr[3 * a + 2];
+  }
+  for (int j = 0; j < 3; ++j) {
+    h.dA[j] = (double)sc.K[0] * MK[j] + (double)sc.K[2] * MK[6 + j];
+    h.dA[3 + j] = (double)sc.K[4] * MK[3 + j] + (double)sc.K[5] * MK[6 + j];
+    h.dA[6 + j] = (double)sc.K[8] * MK[6 + j];
+  }
+  h.db[0] = (double)sc.K[0] * tr[0] + (double)sc.K[2] * tr[2];
+  h.db[1] = (double)sc.K[4] * tr[1] + (double)sc.K[5] * tr[2];
+  h.db[2] = (double)sc.K[8] * tr[2];
+  for (int k = 0; k < 9; ++k) h.A[k] = (float)h.dA[k];
+  for (int k = 0; k < 3; ++k) h.b[k] = (float)h.db[k];
+  for (int k = 0; k < 4; ++k) h.m[k] = (float)h.dm[k];
+  return h;
+}
+static inline void homography_plane(const HomographyBase &hb, const f4 &pl, float H[9]) {
+  const float m[3] = {pl.x * hb.m[0], pl.y * hb.m[1], pl.x * hb.m[2] + pl.y * hb.m[3] + pl.z};
+  for (int i = 0; i < 3; ++i) {
+    const float bi = hb.b[i] / pl.w;
+    for (int j = 0; j < 3; ++j) H[3 * i + j] = hb.A[3 * i + j] - bi * m[j];
+  }
+}
+
+// Projection of a strong window centred on (px, py) into a source.  The centre goes through the
+// homography in double (from the double bases; the plane enters in double); it is kept as an
+// integer texel (U0, V0) plus a float fraction, and each tap p0 + (dx, dy) as a float offset:
+//   u(p0 + d) - uc = ((H00 - uc H20) dx + (H01 - uc H21) dy) / (Zc + H20 dx + H21 dy),
+// whose terms are small, so float arithmetic places the taps to ~1e-6 px.
+// false when the centre does not project inside the source (DPE.cu:709-712: cost 2)
+static bool window_projection(const HomographyBase &hb, const dpe_camera &sc, int W, int H, const f4 &pl, int px,
+                              int py, WinProj &wp) {
+  const double *A = hb.dA, *b = hb.db;
+  const double m0 = (double)pl.x * hb.dm[0], m1 = (double)pl.y * hb.dm[1];
+  const double m2 = (double)pl.x * hb.dm[2] + (double)pl.y * hb.dm[3] + (double)pl.z;
+  const double iw = 1.0 / (double)pl.w;
+  const double x = (double)px, y = (double)py;
+  const double q = (m0 * x + m1 * y + m2) * iw;
+  const double X = A[0] * x + A[1] * y + A[2] - b[0] * q;
+  const double Y = A[3] * x + A[4] * y + A[5] - b[1] * q;
+  const double Z = A[6] * x + A[7] * y + A[8] - b[2] * q;
+  const double iz = 1.0 / Z;
+  const double uc = X * iz, vc = Y * iz;
+  if (!(uc >= 0.0 && uc < (double)sc.width && vc >= 0.0 && vc < (double)sc.height)) return false;
+  const double U = std::floor(uc), V = std::floor(vc);
+  wp.U0 = (int)U;
+  wp.V0 = (int)V;
+  wp.fu = (float)(uc - U);
+  wp.fv = (float)(vc - V);
+  wp.zc = (float)Z;
+  const double bw0 = b[0] * iw, bw1 = b[1] * iw, bw2 = b[2] * iw;
+  const double h6 = A[6] - bw2 * m0, h7 = A[7] - bw2 * m1;
+  wp.g0 = (float)((A[0] - bw0 * m0) - uc * h6);
+  wp.g1 = (float)((A[1] - bw0 * m1) - uc * h7);
+  wp.g3 = (float)((A[3] - bw1 * m0) - vc * h6);
+  wp.g4 = (float)((A[4] - bw1 * m1) - vc * h7);
+  wp.h6 = (float)h6;
+  wp.h7 = (float)h7;
+  wp.lox = (float)(-1 - wp.U0);
+  wp.hix = (float)(W - 1 - wp.U0);
+  wp.loy = (float)(-1 - wp.V0);
+  wp.hiy = (float)(H - 1 - wp.V0);
+  return true;
 }
 
 // DPE.cu:519-526
@@ -260,6 +383,7 @@ struct Ctx {
   int W = 0, H = 0, N = 0, lowW = 0, lowH = 0;
   dpe_params P;
   dpe_camera cam[DPE_MAX_IMAGES];
+  HomographyBase hbase[DPE_MAX_IMAGES];  // filled by set_cameras()
   Image img[DPE_MAX_IMAGES];
   Image dep[DPE_MAX_IMAGES];
   uint32_t key[2];
@@ -276,6 +400,15 @@ struct Ctx {
   uint8_t edge_low_at(long idx) const { return (idx >= 0 && idx < (long)edge_low.size()) ? edge_low[idx] : 0; }
   uint32_t views_at(long idx) const { return (idx >= 0 && idx < (long)views.size()) ? views[idx] : 0u; }
   s2 neighbour(int center, int k) const { return neigh[(size_t)nmap[center] * DPE_NEIGHBOUR_NUM + k]; }
+  void set_cameras(const dpe_camera *cams) {
+    for (int i = 0; i < N; ++i) cam[i] = cams[i];
+    for (int i = 1; i < N; ++i) hbase[i] = homography_base(cam[0], cam[i]);
+  }
+  // Homography of a reference-camera plane into source src (DPE.cu:457-517).
+  void homography(int src, const f4 &pl, float H[9]) const {
+    if (g_ref_homography) homography_ref(cam[0], cam[src], pl, H);
+    else homography_plane(hbase[src], pl, H);
+  }
 };
 
 // ----------------------------------------------------------------------------- costs
@@ -323,19 +456,23 @@ static float window_ncc(const Ctx &c, const float H[9], const Image &src, int cx
 
 // ComputeBilateralNCCOld, DPE.cu:696-782.
 // Evaluation order: the hypothesis-invariant reference half of the window (bilateral weights,
-// weighted reference moments) is summed first, tap by tap; each source tap is then projected
-// with the numerators affine in y along a window column.  This is the same mathematics as the
+// weighted reference moments) is summed first, tap by tap; each source tap is then placed at its
+// float offset from the window centre projected in double (window_projection).  This is the same mathematics as the
 // reference's per-row loop (and the same order as the CUDA kernels); g_raw_moments selects the
 // reference's own loop order and raw moments instead.
 static float ncc_strong(const Ctx &c, int px, int py, int src, const f4 &pl) {
-  float H[9];
-  homography(c.cam[0], c.cam[src], pl, H);
-  const f2 pt = project(H, px, py);
   const dpe_camera &sc = c.cam[src];
-  if (pt.x >= sc.width || pt.x < 0.0f || pt.y >= sc.height || pt.y < 0.0f) return 2.0f;
   const float center = c.img[0].texel(px, py);
   const int r = c.P.strong_radius, inc = c.P.strong_increment;
-  if (g_raw_moments) return window_ncc(c, H, c.img[src], px, py, r, inc, center);
+  if (g_raw_moments) {
+    float H[9];
+    c.homography(src, pl, H);
+    const f2 pt = project(H, px, py);
+    if (pt.x >= sc.width || pt.x < 0.0f || pt.y >= sc.height || pt.y < 0.0f) return 2.0f;
+    return window_ncc(c, H, c.img[src], px, py, r, inc, center);
+  }
+  WinProj wp;
+  if (!window_projection(c.hbase[src], sc, c.W, c.H, pl, px, py, wp)) return 2.0f;
   float w[64], wr[64];
   float sw = 0.f, swr = 0.f, swrr = 0.f;
   int k = 0;
@@ -355,13 +492,13 @@ static float ncc_strong(const Ctx &c, int px, int py, int src, const f4 &pl) {
   float s_s = 0.f, s_ss = 0.f, s_rs = 0.f;
   k = 0;
   for (int i = -r; i <= r; i += inc) {
-    const float x = (float)(px + i);
-    const float bx = H[0] * x + H[2], by = H[3] * x + H[5], bz = H[6] * x + H[8];
+    const float dx = (float)i;
+    const float cx = wp.g0 * dx, cy = wp.g3 * dx, cz = wp.h6 * dx + wp.zc;
     for (int j = -r; j <= r; j += inc) {
-      const float y = (float)(py + j);
-      const float X = H[1] * y + bx, Y = H[4] * y + by, Z = H[7] * y + bz;
+      const float dy = (float)j;
+      const float X = wp.g1 * dy + cx, Y = wp.g4 * dy + cy, Z = wp.h7 * dy + cz;
       const float iz = 1.0f / Z;
-      const float sv = c.img[src].bilinear(X * iz, Y * iz) - center;
+      const float sv = c.img[src].bilinear_off(wp, wp.fu + X * iz, wp.fv + Y * iz) - center;
       const float ws = w[k] * sv;
       s_s += ws;
       s_ss += ws * sv;
@@ -379,7 +516,7 @@ static float ncc_strong(const Ctx &c, int px, int py, int src, const f4 &pl) {
 // ComputeBilateralNCCNew (deformable window), DPE.cu:561-694
 static float ncc_weak(const Ctx &c, int px, int py, int src, const f4 &pl) {
   float H[9];
-  homography(c.cam[0], c.cam[src], pl, H);
+  c.homography(src, pl, H);
   const f2 pt = project(H, px, py);
   const dpe_camera &sc = c.cam[src];
   if (pt.x >= sc.width || pt.x < 0.0f || pt.y >= sc.height || pt.y < 0.0f) return 2.0f;
@@ -1533,6 +1670,8 @@ void oracle_set_raw_moments(int on) { g_raw_moments = on != 0; }
 
 void oracle_set_ref_addressing(int on) { g_ref_addressing = on != 0; }
 
+void oracle_set_ref_homography(int on) { g_ref_homography = on != 0; }
+
 void oracle_set_serial_race(int on) { g_serial_race = on != 0; }
 
 // Strong NCC at explicit queries.  fp64 != 0 evaluates the cost in double precision end to end
@@ -1540,7 +1679,8 @@ void oracle_set_serial_race(int on) { g_serial_race = on != 0; }
 void oracle_ncc_strong(const dpe_ncc_query *q, int fp64, double *out) {
   Ctx c;
   c.W = q->width; c.H = q->height; c.N = q->num_images; c.P = q->params;
-  for (int i = 0; i < c.N; ++i) { c.cam[i] = q->cameras[i]; c.img[i].data = q->images[i]; c.img[i].w = c.W; c.img[i].h = c.H; }
+  c.set_cameras(q->cameras);
+  for (int i = 0; i < c.N; ++i) { c.img[i].data = q->images[i]; c.img[i].w = c.W; c.img[i].h = c.H; }
 #pragma omp parallel for schedule(static)
   for (int64_t k = 0; k < q->count; ++k) {
     const f4 pl = {q->plane[4 * k], q->plane[4 * k + 1], q->plane[4 * k + 2], q->plane[4 * k + 3]};
@@ -1635,7 +1775,8 @@ inline D4 dsqrt(const D4 &a) {
 void oracle_ncc_strong_grad(const dpe_ncc_query *q, double *cost_out, double *grad_plane, double **grad_images) {
   Ctx c;
   c.W = q->width; c.H = q->height; c.N = q->num_images; c.P = q->params;
-  for (int i = 0; i < c.N; ++i) { c.cam[i] = q->cameras[i]; c.img[i].data = q->images[i]; c.img[i].w = c.W; c.img[i].h = c.H; }
+  c.set_cameras(q->cameras);
+  for (int i = 0; i < c.N; ++i) { c.img[i].data = q->images[i]; c.img[i].w = c.W; c.img[i].h = c.H; }
   const int r = c.P.strong_radius, inc = c.P.strong_increment;
 #pragma omp parallel for schedule(static) if (!grad_images)
   for (int64_t k = 0; k < q->count; ++k) {
@@ -1753,8 +1894,8 @@ int oracle_pm_run(const dpe_problem *pr, dpe_pm_out *out, int threads) {
   c.W = pr->width; c.H = pr->height; c.N = pr->num_images; c.P = pr->params;
   c.P.num_images = c.N;
   const size_t L = (size_t)c.W * c.H;
+  c.set_cameras(pr->cameras);
   for (int i = 0; i < c.N; ++i) {
-    c.cam[i] = pr->cameras[i];
     c.img[i].data = pr->images[i]; c.img[i].w = c.W; c.img[i].h = c.H;
     if (c.P.geom_consistency) { c.dep[i].data = pr->depths[i]; c.dep[i].w = c.W; c.dep[i].h = c.H; }
   }

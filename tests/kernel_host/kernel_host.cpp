@@ -111,7 +111,7 @@ extern "C" int host_pm_run(const dpe_problem *p, dpe_pm_out *out) {
   a.P = p->params;
   a.P.num_images = N;
   for (int i = 0; i < N; ++i) a.cam[i] = p->cameras[i];
-  for (int i = 1; i < N; ++i) relative_pose(a.cam[0], a.cam[i], a.Rrel[i], a.trel[i]);
+  set_homography_bases(a);
   a.key[0] = (uint32_t)p->seed;
   a.key[1] = (uint32_t)(p->seed >> 32);
   std::vector<float *> imgs;
