@@ -20,6 +20,7 @@ on a bounded sample of the same schedule, on all host cores.
 
 `--case` runs only device-resident schedules of a chosen scene (for profilers):
     python bench.py --case c2 --levels 2 --repeat 1 [--stats] [--staging 0|1|2] [--gn]
+`--case c5` measures the batching forms on the 49-view ring workload (one JSON line).
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 """
@@ -605,6 +606,89 @@ def run_case(args):
     return 0
 
 
+def run_c5(args):
+    """The batching workload: 49 reference views of three sizes (20 at 640x480, 20 at 1600x1200, 9 at
+    3200x2400) on a 60-camera ring, each with its 10 nearest ring neighbours as sources; one
+    FIRST_INIT call per view (3 iterations, geom off).  Forms: per-view FP32 calls (plain), all 49
+    problems in one kernel sequence (batched), and batched with FP16-staged sources and the
+    Gauss-Newton hypothesis; 1 warm-up + 3 timed runs each (device time of the kernel sequences),
+    with clocks; depth agreement with plain and accuracy against ground truth; then fusion of the
+    last form's depth maps into one point cloud.  Prints one JSON line."""
+    import dpe_b200 as D
+    import scene as S
+
+    t0 = time.perf_counter()
+    ring, probs = S.c5_workload(seed=args.seed, device="cuda")
+    gen_s = time.perf_counter() - t0
+    ctx = D.Context(0)
+    p = schedule_params(0, 0, 11)
+    p.depth_min = np.float32(ring.spec.depth_min) * np.float32(0.6)  # DPE::InuputInitialization (DPE.cpp:953-954)
+    p.depth_max = np.float32(ring.spec.depth_max) * np.float32(1.2)
+    calls = [dict(images=q["images"], cameras=q["cameras"], params=p, seed=1000 + i) for i, q in enumerate(probs)]
+    mpix = sum(q["width"] * q["height"] for q in probs) / 1e6
+
+    def plain():
+        out, ms = [], 0.0
+        for c in calls:
+            r = ctx.pm_run(c["images"], c["cameras"], c["params"], seed=c["seed"])
+            ms += r["gpu_ms"]
+            out.append(r)
+        return out, ms
+
+    def batched():
+        out = ctx.pm_run_batch(calls)
+        return out, max(r["gpu_ms"] for r in out)
+
+    def depths(res):
+        return np.concatenate([r["plane"][..., 3].ravel() for r in res])
+
+    gt = np.concatenate([q["depth"].ravel() for q in probs])
+    forms, ref_res, last = {}, None, None
+    for name, fn, staging, gn in (("plain", plain, D.STAGE_FP32, 0), ("batched", batched, D.STAGE_FP32, 0),
+                                  ("batched_fp16_gn", batched, D.STAGE_FP16, 1)):
+        ctx.set_options(staging=staging, gn_refine=gn)
+        fn()
+        times, walls = [], []
+        with ClockSampler(0) as clk:
+            for _ in range(3):
+                w0 = time.perf_counter()
+                res, ms = fn()
+                walls.append(time.perf_counter() - w0)
+                times.append(ms)
+        ctx.set_options()
+        ms = statistics.median(times)
+        d = depths(res)
+        f = dict(value=round(mpix / (ms / 1e3), 4), unit=UNIT, ms=round(ms, 2), ms_samples=[round(t, 1) for t in times],
+                 wall_s=round(statistics.median(walls), 3), staging={D.STAGE_FP32: "fp32", D.STAGE_FP16: "fp16"}[staging],
+                 gauss_newton=bool(gn), depth_within_1pct_of_gt=round(float((np.abs(d - gt) <= 0.01 * gt).mean()), 4),
+                 clocks=clk.summary())
+        if ref_res is None:
+            ref_res = res
+        else:
+            dp = depths(ref_res)
+            f["depth_agreement_with_plain_0_1pct"] = round(float((np.abs(d - dp) <= 1e-3 * np.abs(dp)).mean()), 4)
+            f["vs_plain"] = round(f["value"] / forms["plain"]["value"], 3)
+        forms[name] = f
+        last = res
+    # whole-scene fusion: each view's sources are its ring neighbours that are reference views too
+    index = {q["ref"]: i for i, q in enumerate(probs)}
+    views = []
+    for q, r in zip(probs, last):
+        views.append(dict(depth=np.ascontiguousarray(r["plane"][..., 3]), normal=np.ascontiguousarray(r["plane"][..., :3]),
+                          weak=r["weak"], bgr=q["bgr"], camera=q["cameras"][0],
+                          src=[index[s] for s in q["sources"] if s in index]))
+    fu = ctx.fuse(views, D.FUSE_FP64, min_consistent=2)
+    line = dict(metric=METRIC, unit=UNIT, data="synthetic (seeded 60-camera ring scene)",
+                config=dict(workload="c5 batching: 49 reference views (20 x 640x480, 20 x 1600x1200, 9 x 3200x2400) on a "
+                                     "60-camera ring, 10 sources each, FIRST_INIT 3 iterations, then fusion min 2 views",
+                            reference_mpix=round(mpix, 3)),
+                scene_generation_s=round(gen_s, 1), forms=forms,
+                fusion=dict(points=int(fu["count"]), gpu_ms=round(fu["gpu_ms"], 2)))
+    print(json.dumps(line), flush=True)
+    ctx.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -622,6 +706,8 @@ def main():
     ap.add_argument("--staging", type=int, default=0)
     ap.add_argument("--gn", action="store_true")
     args = ap.parse_args()
+    if args.case == "c5":
+        return run_c5(args)
     if args.case:
         return run_case(args)
     if args.impl == "reference":

@@ -48,6 +48,8 @@ class SceneSpec:
     depth_max: float = 3.0
     tex_freq: float = 25.0           # base noise frequency, cycles per metre
     supersample: int = 2
+    ring: bool = False               # cameras on a full circle (360 / n_views apart) instead of an arc
+    wall_radius: Optional[float] = None  # ring scenes: a textured cylinder wall around the objects
 
 
 def preset(name: str) -> SceneSpec:
@@ -74,6 +76,11 @@ def preset(name: str) -> SceneSpec:
     if name == "c2_200":  # the c2 scene layout at 200x150 (the CPU reference's timing sample)
         return SceneSpec(width=200, height=150, n_views=10, fx=164.0625, fy=164.0625, cx=100.0, cy=75.0,
                          n_planes=6, n_spheres=2, weak_sigma=3.0, tex_freq=7.5, supersample=1)
+    if name == "c5_ring":  # 60 cameras on a ring around 5 planes + 3 spheres inside a textured wall;
+        # intrinsics at 640x480, scaled for the 1600x1200 and 3200x2400 renderings (camera_struct)
+        return SceneSpec(width=640, height=480, n_views=60, fx=525.0, fy=525.0, cx=320.0, cy=240.0,
+                         arc_radius=2.0, n_planes=6, n_spheres=3, tex_sigma=40.0, depth_min=1.0, depth_max=5.2,
+                         tex_freq=40.0, supersample=1, ring=True, wall_radius=3.0)
     raise ValueError(f"unknown scene preset {name!r}")
 
 
@@ -132,6 +139,54 @@ def _texture(p: torch.Tensor, seed: int, freq: float) -> torch.Tensor:
         amp *= 0.5
     # a single value-noise octave has a standard deviation of about 0.36 (uniform lattice, smoothstep)
     return acc / (math.sqrt(norm) * 0.36)
+
+
+def _intersect(objs, C: torch.Tensor, dw: torch.Tensor, dev):
+    """Nearest hit of the rays C + t dw (dw: (M, 3)) with the objects: (t, object index, normal);
+    t = inf and index -1 where nothing is hit."""
+    f32 = torch.float32
+    M = dw.shape[0]
+    best_t = torch.full((M,), float("inf"), device=dev)
+    best_o = torch.full((M,), -1, dtype=torch.int64, device=dev)
+    best_n = torch.zeros(M, 3, device=dev)
+    for oi, ob in enumerate(objs):
+        if ob["kind"] == "plane":
+            n = torch.tensor(ob["n"], dtype=f32, device=dev)
+            c = torch.tensor(ob["c"], dtype=f32, device=dev)
+            den = dw @ n
+            tt = ((c - C) @ n) / den
+            P = C + tt[:, None] * dw
+            rel = P - c
+            uu = rel @ torch.tensor(ob["u"], dtype=f32, device=dev)
+            vv = rel @ torch.tensor(ob["v"], dtype=f32, device=dev)
+            ok = (tt > 0) & (uu.abs() <= ob["hu"]) & (vv.abs() <= ob["hv"])
+            nn = n.expand(M, 3)
+        elif ob["kind"] == "sphere":
+            c = torch.tensor(ob["c"], dtype=f32, device=dev)
+            oc = C - c
+            a = (dw * dw).sum(1)
+            b = 2.0 * (dw @ oc)
+            cc = float(oc @ oc - ob["r"] ** 2)
+            disc = b * b - 4 * a * cc
+            ok = disc > 0
+            tt = (-b - torch.sqrt(disc.clamp_min(0))) / (2 * a)
+            ok = ok & (tt > 0)
+            P = C + tt[:, None] * dw
+            nn = (P - c) / ob["r"]
+        else:  # "wall": the inside of a vertical (y) cylinder of radius r around the origin
+            a = dw[:, 0] * dw[:, 0] + dw[:, 2] * dw[:, 2]
+            b = 2.0 * (C[0] * dw[:, 0] + C[2] * dw[:, 2])
+            cc = float(C[0] * C[0] + C[2] * C[2] - ob["r"] ** 2)
+            disc = b * b - 4 * a * cc
+            tt = (-b + torch.sqrt(disc.clamp_min(0))) / (2 * a)
+            ok = (disc > 0) & (tt > 0)
+            P = C + tt[:, None] * dw
+            nn = torch.stack([-P[:, 0], torch.zeros_like(P[:, 0]), -P[:, 2]], 1) / ob["r"]
+        upd = ok & (tt < best_t)
+        best_t = torch.where(upd, tt, best_t)
+        best_o = torch.where(upd, torch.full_like(best_o, oi), best_o)
+        best_n = torch.where(upd[:, None], nn, best_n)
+    return best_t, best_o, best_n
 
 
 def _look_at_camera(theta: float, radius: float):
@@ -209,37 +264,7 @@ def make_scene(spec: SceneSpec | str, seed: int = 1, device: str = "cpu") -> Sce
             pix = torch.stack([(us + ox).reshape(-1), (vs + oy).reshape(-1), torch.ones(H * W, device=dev)], 1)
             dcam = pix @ Kinv.T
             dw = dcam @ R  # R^T * dcam
-            best_t = torch.full((H * W,), float("inf"), device=dev)
-            best_o = torch.full((H * W,), -1, dtype=torch.int64, device=dev)
-            best_n = torch.zeros(H * W, 3, device=dev)
-            for oi, ob in enumerate(objs):
-                if ob["kind"] == "plane":
-                    n = torch.tensor(ob["n"], dtype=f32, device=dev)
-                    c = torch.tensor(ob["c"], dtype=f32, device=dev)
-                    den = dw @ n
-                    tt = ((c - C) @ n) / den
-                    P = C + tt[:, None] * dw
-                    rel = P - c
-                    uu = rel @ torch.tensor(ob["u"], dtype=f32, device=dev)
-                    vv = rel @ torch.tensor(ob["v"], dtype=f32, device=dev)
-                    ok = (tt > 0) & (uu.abs() <= ob["hu"]) & (vv.abs() <= ob["hv"])
-                    nn = n.expand(H * W, 3)
-                else:
-                    c = torch.tensor(ob["c"], dtype=f32, device=dev)
-                    oc = C - c
-                    a = (dw * dw).sum(1)
-                    b = 2.0 * (dw @ oc)
-                    cc = float(oc @ oc - ob["r"] ** 2)
-                    disc = b * b - 4 * a * cc
-                    ok = disc > 0
-                    tt = (-b - torch.sqrt(disc.clamp_min(0))) / (2 * a)
-                    ok = ok & (tt > 0)
-                    P = C + tt[:, None] * dw
-                    nn = (P - c) / ob["r"]
-                upd = ok & (tt < best_t)
-                best_t = torch.where(upd, tt, best_t)
-                best_o = torch.where(upd, torch.full_like(best_o, oi), best_o)
-                best_n = torch.where(upd[:, None], nn, best_n)
+            best_t, best_o, best_n = _intersect(objs, C, dw, dev)
             P = C + best_t[:, None] * dw
             tex = _texture(P, tex_seed, spec.tex_freq)
             sig = torch.tensor(sigmas, dtype=f32, device=dev)[best_o.clamp_min(0)]
@@ -255,29 +280,7 @@ def make_scene(spec: SceneSpec | str, seed: int = 1, device: str = "cpu") -> Sce
             # ground truth at the exact pixel centre
             pix = torch.stack([us.reshape(-1), vs.reshape(-1), torch.ones(H * W, device=dev)], 1)
             dw = (pix @ Kinv.T) @ R
-            best_t = torch.full((H * W,), float("inf"), device=dev)
-            best_n = torch.zeros(H * W, 3, device=dev)
-            for ob in objs:
-                c = torch.tensor(ob["c"], dtype=f32, device=dev)
-                if ob["kind"] == "plane":
-                    n = torch.tensor(ob["n"], dtype=f32, device=dev)
-                    tt = ((c - C) @ n) / (dw @ n)
-                    Pp = C + tt[:, None] * dw
-                    rel = Pp - c
-                    ok = (tt > 0) & ((rel @ torch.tensor(ob["u"], dtype=f32, device=dev)).abs() <= ob["hu"]) & \
-                         ((rel @ torch.tensor(ob["v"], dtype=f32, device=dev)).abs() <= ob["hv"])
-                    nn = n.expand(H * W, 3)
-                else:
-                    oc = C - c
-                    a = (dw * dw).sum(1)
-                    b = 2.0 * (dw @ oc)
-                    disc = b * b - 4 * a * float(oc @ oc - ob["r"] ** 2)
-                    tt = (-b - torch.sqrt(disc.clamp_min(0))) / (2 * a)
-                    ok = (disc > 0) & (tt > 0)
-                    nn = (C + tt[:, None] * dw - c) / ob["r"]
-                upd = ok & (tt < best_t)
-                best_t = torch.where(upd, tt, best_t)
-                best_n = torch.where(upd[:, None], nn, best_n)
+            best_t, _, best_n = _intersect(objs, C, dw, dev)
             gt_z = ((C + best_t[:, None] * dw) - C) @ R[2]
             gt_n = best_n
         val = acc_val / len(offs)
@@ -352,3 +355,128 @@ def write_dense_folder(scene: Scene, folder: str) -> None:
         f.write(f"{scene.n}\n")
         for v in range(scene.n):
             f.write(f"{v}\n{len(scene.pairs[v])} " + " ".join(f"{o} {s}" for o, s in zip(scene.pairs[v], scene.scores[v])) + "\n")
+
+
+# ---------------------------------------------------------------------------- ring scenes (C5)
+class RingScene:
+    """Cameras on a full ring around a cluster of planes and spheres inside a textured cylinder wall,
+    rendered on demand at any resolution: the intrinsics of the spec (at spec.width x spec.height)
+    are scaled as camera_struct scales them, so a rendering and its camera struct agree."""
+
+    def __init__(self, spec: SceneSpec | str, seed: int = 1, device: str = "cpu"):
+        if isinstance(spec, str):
+            spec = preset(spec)
+        assert spec.ring and spec.wall_radius, "a ring spec with a wall"
+        self.spec, self.device = spec, device
+        rng = np.random.default_rng(seed)
+        N = spec.n_views
+        self.R, self.t = [], []
+        for v in range(N):
+            R, t = _look_at_camera(2.0 * math.pi * v / N, spec.arc_radius)
+            self.R.append(R.astype(np.float32))
+            self.t.append(t.astype(np.float32))
+        objs = [dict(kind="wall", r=spec.wall_radius)]
+        for _ in range(spec.n_planes - 1):
+            c = np.array([rng.uniform(-0.5, 0.5), rng.uniform(-0.3, 0.3), rng.uniform(-0.5, 0.5)])
+            n = rng.normal(size=3)
+            n /= np.linalg.norm(n)
+            u = np.cross(np.array([0.0, 1.0, 0.0]) if abs(n[1]) < 0.9 else np.array([1.0, 0.0, 0.0]), n)
+            u /= np.linalg.norm(u)
+            objs.append(dict(kind="plane", c=c, n=n, u=u, v=np.cross(n, u), hu=rng.uniform(0.15, 0.35),
+                             hv=rng.uniform(0.12, 0.3)))
+        for _ in range(spec.n_spheres):
+            c = np.array([rng.uniform(-0.45, 0.45), rng.uniform(-0.25, 0.25), rng.uniform(-0.45, 0.45)])
+            objs.append(dict(kind="sphere", c=c, r=rng.uniform(0.1, 0.25)))
+        self.objs = objs
+        self.sigmas = np.full(len(objs), spec.tex_sigma)
+        self.tints = rng.uniform(0.85, 1.15, size=(len(objs), 3))
+        self.tex_seed = int(rng.integers(1, 2**31 - 1))
+        self._K0 = np.array([[spec.fx, 0, spec.cx], [0, spec.fy, spec.cy], [0, 0, 1]], dtype=np.float32)
+
+    @property
+    def n(self) -> int:
+        return self.spec.n_views
+
+    def camera(self, v: int, width: int, height: int) -> dict:
+        """camera_struct of ring camera v at width x height."""
+        shim = Scene(spec=self.spec, K=self._K0[None].repeat(self.n, 0), R=np.stack(self.R), t=np.stack(self.t),
+                     gray=np.zeros((0, 1, 1), np.uint8), bgr=None, depth=None, normal=None, pairs=[], scores=[])
+        return camera_struct(shim, v, width, height)
+
+    def render(self, v: int, width: int, height: int):
+        """(gray uint8 HxW, bgr uint8 HxWx3, depth float32 HxW) of ring camera v, one ray per pixel
+        centre."""
+        dev = torch.device(self.device)
+        f32 = torch.float32
+        cam = self.camera(v, width, height)
+        K = np.asarray(cam["K"], np.float64).reshape(3, 3)
+        Kinv = torch.tensor(np.linalg.inv(K), dtype=f32, device=dev)
+        R = torch.tensor(self.R[v], dtype=f32, device=dev)
+        C = torch.tensor(-self.R[v].astype(np.float64).T @ self.t[v].astype(np.float64), dtype=f32, device=dev)
+        H, W = height, width
+        vs, us = torch.meshgrid(torch.arange(H, device=dev, dtype=f32), torch.arange(W, device=dev, dtype=f32), indexing="ij")
+        pix = torch.stack([us.reshape(-1), vs.reshape(-1), torch.ones(H * W, device=dev)], 1)
+        dw = (pix @ Kinv.T) @ R
+        del pix, vs, us
+        best_t, best_o, _ = _intersect(self.objs, C, dw, dev)
+        P = C + best_t[:, None] * dw
+        del dw
+        tex = _texture(P, self.tex_seed, self.spec.tex_freq)
+        o = best_o.clamp_min(0)
+        val = self.spec.tex_mean + torch.tensor(self.sigmas, dtype=f32, device=dev)[o] * tex
+        col = val[:, None] * torch.tensor(self.tints, dtype=f32, device=dev)[o]
+        z = (P - C) @ R[2]
+        gray = torch.round(val.clamp(0, 255)).to(torch.uint8).reshape(H, W).cpu().numpy()
+        bgr = torch.round(col.clamp(0, 255)).to(torch.uint8).reshape(H, W, 3).cpu().numpy()
+        return gray, bgr, z.reshape(H, W).cpu().numpy().astype(np.float32)
+
+
+# The batching workload: 49 reference views of uneven resolution on the 60-camera ring, each with
+# its 10 nearest ring neighbours as sources (rendered at the reference view's resolution).
+C5_CLASSES = ((640, 480, 20), (1600, 1200, 20), (3200, 2400, 9))
+
+
+def c5_views(n_ring: int = 60):
+    """[(reference camera, width, height, [10 source cameras])] of the batching workload: the
+    references spread over the ring, class by class; sources nearest first."""
+    out = []
+    total = sum(c[2] for c in C5_CLASSES)
+    refs = [int(round(i * n_ring / total)) % n_ring for i in range(total)]
+    k = 0
+    for W, H, count in C5_CLASSES:
+        for _ in range(count):
+            r = refs[k]
+            k += 1
+            srcs = sorted(((r + d) % n_ring for d in (-1, 1, -2, 2, -3, 3, -4, 4, -5, 5)),
+                          key=lambda o: (min((o - r) % n_ring, (r - o) % n_ring), o))
+            out.append((r, W, H, srcs))
+    return out
+
+
+def c5_workload(seed: int = 1, device: str = "cpu", views=None):
+    """The 49 per-view problems of the batching workload: per reference view its images (reference
+    first, float32), cameras, ground-truth depth and colour.  `views` restricts it to a subset of
+    c5_views() (indices).  Each rendering is kept only until the last problem that uses it."""
+    ring = RingScene("c5_ring", seed=seed, device=device)
+    layout = c5_views(ring.n)
+    if views is not None:
+        layout = [layout[i] for i in views]
+    last = {}  # rendering -> index of the last problem that uses it
+    for i, (r, W, H, srcs) in enumerate(layout):
+        for v in [r] + srcs:
+            last[(v, W, H)] = i
+    cache = {}
+    problems = []
+    for i, (r, W, H, srcs) in enumerate(layout):
+        imgs, cams = [], []
+        for v in [r] + srcs:
+            key = (v, W, H)
+            if key not in cache:
+                cache[key] = ring.render(v, W, H)
+            imgs.append(cache[key][0].astype(np.float32))
+            cams.append(ring.camera(v, W, H))
+        _, bgr, z = cache[(r, W, H)]
+        problems.append(dict(ref=r, width=W, height=H, sources=srcs, images=imgs, cameras=cams, depth=z, bgr=bgr))
+        for key in [k for k in cache if last[k] == i]:
+            del cache[key]
+    return ring, problems
