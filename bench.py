@@ -622,6 +622,7 @@ def run_c5(args):
     gen_s = time.perf_counter() - t0
     ctx = D.Context(0)
     p = schedule_params(0, 0, 11)
+    p.use_limit = p.use_label = 0  # no edge or label maps: FIRST_INIT as ProcessProblem runs it at level 0
     p.depth_min = np.float32(ring.spec.depth_min) * np.float32(0.6)  # DPE::InuputInitialization (DPE.cpp:953-954)
     p.depth_max = np.float32(ring.spec.depth_max) * np.float32(1.2)
     calls = [dict(images=q["images"], cameras=q["cameras"], params=p, seed=1000 + i) for i, q in enumerate(probs)]
