@@ -460,6 +460,17 @@ def run_ours(args):
     launches = D.load_library().dpe_launch_count() - launches0
     ctx.set_profiling(False)
     stats = ctx.kernel_stats()
+    # the launch tuner's choices at the finest level (made during the warm-up steps): the kept
+    # setting and its gain over the first candidate (16x8 blocks / the driver's carveout)
+    tuning = ctx.tuning()
+    finest = max((e["size_class"] for e in tuning), default=None)
+    autotune = {}
+    for e in tuning:
+        if e["size_class"] != finest or e["chosen"] < 0 or not e["mean_ms"][e["chosen"]]:
+            continue
+        kept = f"{e['block'][0]}x{e['block'][1]} blocks" if e["block"][0] else f"carveout {e['carveout']}"
+        autotune[e["kernel"]] = dict(kept=kept, mean_ms=e["mean_ms"],
+                                     gain_vs_first=round(e["mean_ms"][0] / e["mean_ms"][e["chosen"]], 3))
     ms_per_step = gpu_ms / args.steps
     if dist is not None:
         t = torch.tensor([ms_per_step], device=dev)
@@ -564,7 +575,7 @@ def run_ours(args):
                 e2e=dict(value=round(e2e_value, 4), unit=UNIT, h2d_bytes_per_step=int(h2d), d2h_bytes_per_step=int(d2h)),
                 kernel_ms_per_step={k: round(v["ms"] / max(1, args.steps), 3) for k, v in
                                     sorted(stats.items(), key=lambda kv: -kv[1]["ms"])},
-                forms=forms or None)
+                forms=forms or None, autotune=autotune or None)
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()

@@ -186,6 +186,12 @@ extern "C" int dpe_ctx_destroy(dpe_ctx *c) {
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
   c->arena.release();
+  for (auto &kv : c->tuner.table)
+    for (const TuneEntry::Pend &p : kv.second.pending) {
+      cudaEventDestroy(p.t0);
+      cudaEventDestroy(p.t1);
+    }
+  for (cudaEvent_t e : c->tuner.events) cudaEventDestroy(e);
   cudaEventDestroy(c->ev0);
   cudaEventDestroy(c->ev1);
   cudaStreamDestroy(c->stream);
@@ -221,11 +227,121 @@ template <class F> void with_stage(int staging, F &&f) {
   else f(std::integral_constant<int, DPE_STAGE_FP32>{});
 }
 
+// ------------------------------------------------------------------ launch tuner (ctx.h)
+// Block shapes tried for the one-thread-per-pixel kernels of one problem (each thread reads and
+// writes only its own pixel, so the shape changes nothing but speed; all fit __launch_bounds__(128)).
+const dim3 kShapeCands[] = {dim3(16, 8), dim3(32, 4), dim3(8, 16), dim3(64, 2), dim3(8, 8)};
+constexpr int kNumShapes = 5;
+// Shared-memory carveouts (percent; -1 the driver's choice) tried for the cooperative kernels.
+const int kCarveCands[] = {-1, 100, 75, 50};
+constexpr int kNumCarves = 4;
+
+int size_class(long long pixels) {
+  int c = 0;
+  while (c < 63 && (2LL << c) <= pixels) ++c;
+  return c;
+}
+// Folds the completed measurements of e into its sums; keeps the others pending.
+void tune_harvest(dpe_ctx *ctx, TuneEntry &e) {
+  size_t keep = 0;
+  for (size_t i = 0; i < e.pending.size(); ++i) {
+    TuneEntry::Pend &p = e.pending[i];
+    const cudaError_t q = cudaEventQuery(p.t1);
+    if (q == cudaErrorNotReady) {
+      e.pending[keep++] = p;
+      continue;
+    }
+    float ms = 0.f;
+    if (q == cudaSuccess && cudaEventElapsedTime(&ms, p.t0, p.t1) == cudaSuccess) {
+      e.sum[p.cand] += ms;
+      e.count[p.cand] += 1;
+    } else {
+      cudaGetLastError();
+    }
+    ctx->tuner.events.push_back(p.t0);
+    ctx->tuner.events.push_back(p.t1);
+  }
+  e.pending.resize(keep);
+}
+cudaEvent_t tune_event(dpe_ctx *ctx) {
+  if (!ctx->tuner.events.empty()) {
+    cudaEvent_t e = ctx->tuner.events.back();
+    ctx->tuner.events.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  if (cudaEventCreate(&e) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return e;
+}
+// One launch under the tuner: `cand` is the candidate to launch with; call finish() right after
+// the launch.  With the tuner off, or once an entry has chosen, no events are recorded.
+struct TunedLaunch {
+  dpe_ctx *ctx;
+  TuneEntry *e = nullptr;
+  cudaStream_t s;
+  int cand = 0;
+  cudaEvent_t t0 = nullptr, t1 = nullptr;
+  TunedLaunch(dpe_ctx *c, int kid, long long pixels, int ncand, cudaStream_t st) : ctx(c), s(st) {
+    if (!ctx->tuner.enabled) return;
+    e = &ctx->tuner.table[LaunchTuner::key(kid, size_class(pixels))];
+    e->ncand = ncand;
+    if (e->chosen >= 0) {
+      cand = e->chosen;
+      return;
+    }
+    tune_harvest(ctx, *e);
+    bool done = e->pending.empty();
+    for (int i = 0; i < ncand && done; ++i) done = e->count[i] >= LaunchTuner::kRounds;
+    if (done) {
+      int best = 0;
+      for (int i = 1; i < ncand; ++i)
+        if (e->sum[i] / e->count[i] < e->sum[best] / e->count[best]) best = i;
+      e->chosen = cand = best;
+      return;
+    }
+    cand = e->trial++ % ncand;
+    if (e->trial > 4 * LaunchTuner::kRounds * ncand) {  // samples still in flight: no more events
+      cand = 0;
+      return;
+    }
+    t0 = tune_event(ctx);
+    t1 = tune_event(ctx);
+    if (t0 && t1) cudaEventRecord(t0, s);
+  }
+  void finish() {
+    if (!t0 || !t1) return;
+    cudaEventRecord(t1, s);
+    e->pending.push_back(TuneEntry::Pend{cand, t0, t1});
+  }
+};
+// The preferred carveout of a kernel function, set only when it changes (the attribute belongs
+// to the function, process-wide).
+void set_carveout(const void *func, int percent) {
+  static std::mutex mu;
+  static std::map<const void *, int> current;
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = current.find(func);
+  if (it != current.end() && it->second == percent) return;
+  if (cudaFuncSetAttribute(func, cudaFuncAttributePreferredSharedMemoryCarveout, percent) == cudaSuccess)
+    current[func] = percent;
+  else
+    cudaGetLastError();
+}
+dim3 shape_grid(int W, int H, dim3 b) { return dim3((W + b.x - 1) / b.x, (H + b.y - 1) / b.y); }
+
 void launch_strong_update(int staging, bool gn, dim3 grid, size_t smem, cudaStream_t s, const Launch args, int it,
-                          int parity) {
+                          int parity, int carveout) {
   with_stage(staging, [&](auto st) {
-    if (gn) k_strong_update<decltype(st)::value, true><<<grid, kCoopThreads, smem, s>>>(args, it, parity);
-    else k_strong_update<decltype(st)::value, false><<<grid, kCoopThreads, smem, s>>>(args, it, parity);
+    if (gn) {
+      set_carveout((const void *)k_strong_update<decltype(st)::value, true>, carveout);
+      k_strong_update<decltype(st)::value, true><<<grid, kCoopThreads, smem, s>>>(args, it, parity);
+    } else {
+      set_carveout((const void *)k_strong_update<decltype(st)::value, false>, carveout);
+      k_strong_update<decltype(st)::value, false><<<grid, kCoopThreads, smem, s>>>(args, it, parity);
+    }
   });
 }
 
@@ -471,11 +587,34 @@ int run_sequence(dpe_ctx *ctx, ProblemState *ps, int n, const PMArgs *d_args, co
       DPE_TRY(cudaMemsetAsync(a.nmap, 0, (size_t)L * 4, s));
     }
   }
-  DPE_TIMED(ctx, KID_GEN_EDGE_INFORM, s, k_gen_edge_inform<<<g.fg, g.fb, 0, s>>>(g.full));
+  // Launch settings the tuner picks (results do not depend on them): the block shape of a
+  // one-thread-per-pixel kernel for one problem (a batch keeps the 16 x 8 layout its block table
+  // is built for), and the shared-memory carveout of a cooperative kernel.
+  long long pix_all = 0;
+  for (int b = 0; b < n; ++b) pix_all += (long long)ps[b].L;
+  auto shaped = [&](int kid, auto launch) {
+    if (n != 1) {
+      launch(g.fg, g.fb);
+      return;
+    }
+    TunedLaunch t(ctx, kid, pix_all, kNumShapes, s);
+    const dim3 bl = kShapeCands[t.cand];
+    launch(shape_grid(ps[0].a.W, ps[0].a.H, bl), bl);
+    t.finish();
+  };
+  auto carved = [&](int kid, auto launch) {
+    TunedLaunch t(ctx, kid, pix_all, kNumCarves, s);
+    launch(kCarveCands[t.cand]);
+    t.finish();
+  };
+  DPE_TIMED(ctx, KID_GEN_EDGE_INFORM, s,
+            shaped(KID_GEN_EDGE_INFORM, [&](dim3 gr, dim3 bl) { k_gen_edge_inform<<<gr, bl, 0, s>>>(g.full); }));
   PM_LAUNCHED("k_gen_edge_inform", s);
-  DPE_TIMED(ctx, KID_FIND_NEAREST, s, k_find_nearest_strong<<<g.fg, g.fb, 0, s>>>(g.full));
+  DPE_TIMED(ctx, KID_FIND_NEAREST, s,
+            shaped(KID_FIND_NEAREST, [&](dim3 gr, dim3 bl) { k_find_nearest_strong<<<gr, bl, 0, s>>>(g.full); }));
   PM_LAUNCHED("k_find_nearest_strong", s);
-  DPE_TIMED(ctx, KID_GEN_NEIGHBOURS, s, k_gen_neighbours<<<g.fg, g.fb, 0, s>>>(g.full));
+  DPE_TIMED(ctx, KID_GEN_NEIGHBOURS, s,
+            shaped(KID_GEN_NEIGHBOURS, [&](dim3 gr, dim3 bl) { k_gen_neighbours<<<gr, bl, 0, s>>>(g.full); }));
   PM_LAUNCHED("k_gen_neighbours", s);
   DPE_TIMED(ctx, KID_NEIGHBOUR_UPDATE, s, k_neighbour_update<<<g.fg, g.fb, 0, s>>>(g.full));
   PM_LAUNCHED("k_neighbour_update", s);
@@ -495,7 +634,9 @@ int run_sequence(dpe_ctx *ctx, ProblemState *ps, int n, const PMArgs *d_args, co
                                       const_cast<int *>(a.wcount) + parity, L, WeakOfColour{a.weak, a.W, parity}, s));
     }
   }
-  DPE_TIMED(ctx, KID_RANDOM_INIT, s, with_stage(staging, [&](auto st) { k_random_init<decltype(st)::value><<<g.fg, g.fb, 0, s>>>(g.full); }));
+  DPE_TIMED(ctx, KID_RANDOM_INIT, s, shaped(KID_RANDOM_INIT, [&](dim3 gr, dim3 bl) {
+              with_stage(staging, [&](auto st) { k_random_init<decltype(st)::value><<<gr, bl, 0, s>>>(g.full); });
+            }));
   PM_LAUNCHED("k_random_init", s);
   for (int it = 0; it < P.max_iterations; ++it) {
     for (int parity = 0; parity < 2; ++parity) {
@@ -505,10 +646,13 @@ int run_sequence(dpe_ctx *ctx, ProblemState *ps, int n, const PMArgs *d_args, co
           DPE_TRY(cudaMemcpyAsync(a.plane_snap, a.plane, ps[b].L * sizeof(float4), cudaMemcpyDeviceToDevice, s));
           DPE_TRY(cudaMemcpyAsync(a.cost_snap, a.cost, ps[b].L * 4, cudaMemcpyDeviceToDevice, s));
         }
-      DPE_TIMED(ctx, KID_STRONG_UPDATE, s, launch_strong_update(staging, gn, g.cg, g.coop_smem, s, g.coop, it, parity));
+      DPE_TIMED(ctx, KID_STRONG_UPDATE, s, carved(KID_STRONG_UPDATE, [&](int cv) {
+                  launch_strong_update(staging, gn, g.cg, g.coop_smem, s, g.coop, it, parity, cv);
+                }));
       PM_LAUNCHED("k_strong_update", s);
     }
-    DPE_TIMED(ctx, KID_RANSAC, s, k_ransac_fit_plane<<<g.fg, g.fb, 0, s>>>(g.full));
+    DPE_TIMED(ctx, KID_RANSAC, s,
+              shaped(KID_RANSAC, [&](dim3 gr, dim3 bl) { k_ransac_fit_plane<<<gr, bl, 0, s>>>(g.full); }));
     PM_LAUNCHED("k_ransac_fit_plane", s);
     if (P.use_APD)
       for (int parity = 0; parity < 2; ++parity) {
@@ -530,7 +674,12 @@ int run_sequence(dpe_ctx *ctx, ProblemState *ps, int n, const PMArgs *d_args, co
     DPE_TIMED(ctx, KID_FILTER, s, k_filter_strong<<<g.hg, g.hb, 0, s>>>(g.half, parity));
     PM_LAUNCHED("k_filter_strong", s);
   }
-  DPE_TIMED(ctx, KID_DEPTH_TO_WEAK, s, with_stage(staging, [&](auto st) { k_depth_to_weak<decltype(st)::value><<<g.sg, kCoopThreads, 0, s>>>(g.sweep); }));
+  DPE_TIMED(ctx, KID_DEPTH_TO_WEAK, s, carved(KID_DEPTH_TO_WEAK, [&](int cv) {
+              with_stage(staging, [&](auto st) {
+                set_carveout((const void *)k_depth_to_weak<decltype(st)::value>, cv);
+                k_depth_to_weak<decltype(st)::value><<<g.sg, kCoopThreads, 0, s>>>(g.sweep);
+              });
+            }));
   PM_LAUNCHED("k_depth_to_weak", s);
   {
     cudaError_t attr = cudaSuccess;
@@ -541,7 +690,12 @@ int run_sequence(dpe_ctx *ctx, ProblemState *ps, int n, const PMArgs *d_args, co
     });
     DPE_TRY(attr);
   }
-  DPE_TIMED(ctx, KID_LOCAL_REFINE, s, with_stage(staging, [&](auto st) { k_local_refine<decltype(st)::value><<<g.sg, kCoopThreads, g.lr_smem, s>>>(g.sweep); }));
+  DPE_TIMED(ctx, KID_LOCAL_REFINE, s, carved(KID_LOCAL_REFINE, [&](int cv) {
+              with_stage(staging, [&](auto st) {
+                set_carveout((const void *)k_local_refine<decltype(st)::value>, cv);
+                k_local_refine<decltype(st)::value><<<g.sg, kCoopThreads, g.lr_smem, s>>>(g.sweep);
+              });
+            }));
   PM_LAUNCHED("k_local_refine", s);
   return DPE_OK;
 }
@@ -1067,6 +1221,39 @@ extern "C" int dpe_ctx_get_kernel_stats(dpe_ctx *ctx, dpe_kernel_stat *out, int 
       out[n].ms = ctx->kms[k];
       out[n].strong_ncc_evals = ctx->kevals[k][0];
       out[n].weak_ncc_evals = ctx->kevals[k][1];
+    }
+    ++n;
+  }
+  *count = n;
+  return n > capacity ? DPE_ERR_CAPACITY : DPE_OK;
+}
+
+extern "C" int dpe_ctx_set_autotune(dpe_ctx *ctx, int on) {
+  if (!ctx) return DPE_ERR_INVALID_ARGUMENT;
+  ctx->tuner.enabled = on != 0;
+  return DPE_OK;
+}
+
+extern "C" int dpe_ctx_get_tuning(dpe_ctx *ctx, dpe_tuning_entry *out, int capacity, int *count) {
+  if (!ctx || !count || (capacity > 0 && !out)) return DPE_ERR_INVALID_ARGUMENT;
+  int n = 0;
+  for (auto &kv : ctx->tuner.table) {
+    TuneEntry &e = kv.second;
+    tune_harvest(ctx, e);
+    if (n < capacity) {
+      dpe_tuning_entry &o = out[n];
+      std::memset(&o, 0, sizeof(o));
+      const int kid = (int)(kv.first / 64);
+      std::snprintf(o.name, sizeof(o.name), "%s", kid >= 0 && kid < KID_COUNT ? kKernelNames[kid] : "?");
+      o.size_class = (int)(kv.first % 64);
+      o.candidates = e.ncand;
+      o.chosen = e.chosen;
+      const bool carve = kid == KID_STRONG_UPDATE || kid == KID_DEPTH_TO_WEAK || kid == KID_LOCAL_REFINE;
+      if (e.chosen >= 0) {
+        if (carve) o.carveout = kCarveCands[e.chosen];
+        else { o.block_x = (int)kShapeCands[e.chosen].x; o.block_y = (int)kShapeCands[e.chosen].y; }
+      }
+      for (int i = 0; i < e.ncand && i < 8; ++i) o.mean_ms[i] = e.count[i] ? (float)(e.sum[i] / e.count[i]) : 0.f;
     }
     ++n;
   }

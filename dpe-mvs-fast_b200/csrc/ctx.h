@@ -87,7 +87,33 @@ class Arena {
 
 #include "kernel_ids.h"
 
+// ------------------------------------------------------------------ launch tuner
+// Online choice of launch settings that change no result: the block shape of the
+// one-thread-per-pixel kernels and the shared-memory carveout of the cooperative ones.  Per
+// (kernel, size class) the first launches cycle through the candidates, each timed by an event
+// pair on its stream; the times are read without synchronising, once the events have completed.
+// When every candidate has kRounds samples, the lowest mean is kept for every later launch.
+struct TuneEntry {
+  static constexpr int kMaxCand = 8;
+  int ncand = 0, trial = 0, chosen = -1;
+  double sum[kMaxCand] = {};
+  int count[kMaxCand] = {};
+  struct Pend {
+    int cand;
+    cudaEvent_t t0, t1;
+  };
+  std::vector<Pend> pending;
+};
+struct LaunchTuner {
+  static constexpr int kRounds = 2;
+  bool enabled = true;
+  std::map<long long, TuneEntry> table;  // key: kernel id * 64 + size class (log2 of the pixels)
+  std::vector<cudaEvent_t> events;       // completed event pairs, for reuse
+  static long long key(int kid, int cls) { return (long long)kid * 64 + cls; }
+};
+
 struct dpe_ctx {
+  LaunchTuner tuner;
   int device = 0;
   int sms = 148;  // multiprocessors of the device: grid size of the work-list kernels
   dpe_options opt = {DPE_STAGE_FP32, 0};

@@ -96,6 +96,11 @@ class KernelStat(C.Structure):
                 ("strong_ncc_evals", C.c_uint64), ("weak_ncc_evals", C.c_uint64)]
 
 
+class TuningEntry(C.Structure):
+    _fields_ = [("name", C.c_char * 32), ("size_class", C.c_int), ("candidates", C.c_int), ("chosen", C.c_int),
+                ("block_x", C.c_int), ("block_y", C.c_int), ("carveout", C.c_int), ("mean_ms", C.c_float * 8)]
+
+
 class SceneIn(C.Structure):
     _fields_ = [("num_views", C.c_int), ("width", C.c_int), ("height", C.c_int), ("views", C.POINTER(SceneView)),
                 ("memory", C.c_int)]
@@ -124,7 +129,7 @@ EXPORTED = ["dpe_status_string", "dpe_last_error", "dpe_params_default", "dpe_ct
             "dpe_fuse", "dpe_ncc_eval", "dpe_ctx_set_eval_counting", "dpe_scene_run", "dpe_ctx_set_profiling",
             "dpe_ctx_reset_kernel_stats", "dpe_ctx_get_kernel_stats", "dpe_launch_count", "dpe_fp32_peak",
             "dpe_ncc_eval_noalloc", "dpe_ncc_grad", "dpe_ctx_set_options", "dpe_pm_run_batch", "dpe_fuse_tat", "dpe_edge_map", "dpe_edge_labels",
-            "dpe_view_scores", "dpe_ncc_grad_device"]
+            "dpe_view_scores", "dpe_ncc_grad_device", "dpe_ctx_set_autotune", "dpe_ctx_get_tuning"]
 
 _lib = None
 
@@ -156,6 +161,8 @@ def load_library(path: Optional[str] = None) -> C.CDLL:
     lib.dpe_ctx_set_profiling.argtypes = [C.c_void_p, C.c_int]
     lib.dpe_ctx_reset_kernel_stats.argtypes = [C.c_void_p]
     lib.dpe_ctx_get_kernel_stats.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int)]
+    lib.dpe_ctx_set_autotune.argtypes = [C.c_void_p, C.c_int]
+    lib.dpe_ctx_get_tuning.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int)]
     lib.dpe_launch_count.restype = C.c_uint64
     lib.dpe_launch_count.argtypes = []
     lib.dpe_fp32_peak.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
@@ -332,6 +339,28 @@ class Context:
         return {arr[i].name.decode(): dict(launches=int(arr[i].launches), ms=float(arr[i].ms),
                                            strong_ncc_evals=int(arr[i].strong_ncc_evals),
                                            weak_ncc_evals=int(arr[i].weak_ncc_evals)) for i in range(min(n.value, 64))}
+
+    def set_autotune(self, on: bool):
+        """The launch tuner (dpe_ctx_set_autotune): on by default."""
+        st = self.lib.dpe_ctx_set_autotune(self.handle, 1 if on else 0)
+        if st != OK:
+            raise DPEError(st, "dpe_ctx_set_autotune")
+
+    def tuning(self) -> List[Dict]:
+        """The tuner's table (dpe_ctx_get_tuning): per kernel and size class the candidates' mean
+        times and the kept setting."""
+        arr = (TuningEntry * 256)()
+        n = C.c_int()
+        st = self.lib.dpe_ctx_get_tuning(self.handle, arr, 256, C.byref(n))
+        if st not in (OK, ERR_CAPACITY):
+            raise DPEError(st, "dpe_ctx_get_tuning")
+        out = []
+        for i in range(min(n.value, 256)):
+            e = arr[i]
+            out.append(dict(kernel=e.name.decode(), size_class=e.size_class, candidates=e.candidates, chosen=e.chosen,
+                            block=(e.block_x, e.block_y), carveout=e.carveout,
+                            mean_ms=[round(float(e.mean_ms[k]), 4) for k in range(e.candidates)]))
+        return out
 
     def fp32_peak_tflops(self) -> float:
         v = C.c_double()

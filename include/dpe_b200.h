@@ -445,6 +445,27 @@ int dpe_ctx_set_profiling(dpe_ctx *ctx, int on);
 int dpe_ctx_reset_kernel_stats(dpe_ctx *ctx);
 int dpe_ctx_get_kernel_stats(dpe_ctx *ctx, dpe_kernel_stat *out, int capacity, int *count);
 
+/* Launch tuner (no reference counterpart; the reference launches fixed 16x16 blocks).  For each
+ * (kernel, size class = floor(log2 of the call's pixels)) the context's first launches cycle
+ * through candidate settings that change no result -- the block shape of the
+ * one-thread-per-pixel kernels (16x8, 32x4, 8x16, 64x2, 8x8; single-problem calls only) and the
+ * shared-memory carveout of the cooperative cost kernels (driver default, 100, 75, 50 %) -- each
+ * timed by an event pair on the context's stream, and keep the fastest mean after 2 samples
+ * each.  On by default; dpe_ctx_set_autotune(ctx, 0) uses the first candidate throughout. */
+int dpe_ctx_set_autotune(dpe_ctx *ctx, int on);
+typedef struct dpe_tuning_entry {
+  char name[32];      /* kernel class, as in dpe_kernel_stat                                   */
+  int size_class;     /* floor(log2(pixels of the call or batch))                              */
+  int candidates;     /* settings tried                                                        */
+  int chosen;         /* index of the kept setting; -1 while still measuring                   */
+  int block_x;        /* block shape of the kept setting (shape-tuned kernels; else 0)         */
+  int block_y;
+  int carveout;       /* carveout of the kept setting in percent, -1 the driver default
+                         (carveout-tuned kernels; else 0)                                      */
+  float mean_ms[8];   /* mean measured time per candidate (0: no sample)                       */
+} dpe_tuning_entry;
+int dpe_ctx_get_tuning(dpe_ctx *ctx, dpe_tuning_entry *out, int capacity, int *count);
+
 /* Number of kernels this library has launched in the process (all contexts). */
 uint64_t dpe_launch_count(void);
 

@@ -118,7 +118,18 @@ def test_golden_pm_gpu(ctx):
     agree1 = h.rel_depth_agreement(g1["plane"][..., 3], z["plane1"][..., 3], DEPTH_REL_TOL)
     weak1 = float((g1["weak"] == z["weak1"]).mean())
     print(f"golden pm: first-init agreement {agree0:.5f}, geom refine agreement {agree1:.5f}, states {weak1:.5f}")
-    assert agree0 >= DEPTH_FRACTION
+    # the exact build reproduces both fixtures bit for bit
+    x = D.Context(0, library=D.EXACT_LIBRARY)
+    try:
+        x0 = x.pm_run(images, cams, p0, seed=seed0)
+        x1 = x.pm_run(images, cams, p1, **_pm_refine_kw(z))
+    finally:
+        x.close()
+    assert np.array_equal(x0["plane"], z["plane0"]) and np.array_equal(x1["plane"], z["plane1"])
+    # The fixture has 64 x 48 pixels: one near-tie that the default build's hardware reciprocal
+    # decides the other way spreads to ~20 pixels (0.7 %).  The 99.5 % bar is held at the measured
+    # sizes (tests/test_gpu_configs.py); here the default build must agree on 99 %.
+    assert agree0 >= 0.99
     assert (g0["weak"] == z["weak0"]).mean() >= 0.99
     # geometric refine: the statistical bar of the parity tests (FMA contraction decides near-ties)
     assert agree1 >= 0.95
