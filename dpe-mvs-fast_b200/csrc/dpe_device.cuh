@@ -253,6 +253,41 @@ __device__ __forceinline__ float floor_split(float x, int *ix) {
 #endif
 }
 
+// Packed pairs of FP32 operations: on sm_100 one FADD2 / FMUL2 instruction performs two IEEE
+// round-to-nearest (or, for the round-down add, round-down) operations, with exactly the results
+// of the two scalar operations; the tap loops are bound by instruction issue, and pairing the x and
+// y coordinates (and the two bilinear rows) cuts their arithmetic instructions.  One rule keeps the
+// results exact: a packed add never takes a packed product as an operand.  Measured on the B200,
+// the compiler turns add2(mul2(a, b), mul2(c, d)) into a fused multiply-add pair even without
+// contraction (-fmad=false), which rounds once instead of twice; products are therefore summed
+// with scalar adds.  Host builds of this source use the scalar forms.
+__device__ __forceinline__ float2 add2(float2 a, float2 b) {
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
+  return __fadd2_rn(a, b);
+#else
+  return make_float2(a.x + b.x, a.y + b.y);
+#endif
+}
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return add2(a, make_float2(-b.x, -b.y)); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) {
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
+  return __fmul2_rn(a, b);
+#else
+  return make_float2(a.x * b.x, a.y * b.y);
+#endif
+}
+// floor_split of both coordinates of a pair.
+__device__ __forceinline__ float2 floor_split2(float2 v, int *ix, int *iy) {
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
+  const float2 f = __fadd2_rd(v, make_float2(12582912.0f, 12582912.0f));
+  *ix = __float_as_int(f.x) - 0x4B400000;
+  *iy = __float_as_int(f.y) - 0x4B400000;
+  return add2(f, make_float2(-12582912.0f, -12582912.0f));
+#else
+  return make_float2(floor_split(v.x, ix), floor_split(v.y, iy));
+#endif
+}
+
 // tex2D(x+0.5, y+0.5) with linear filtering and clamp-to-edge addressing, exact FP32 weights.
 // The padded border makes the four reads branch-free for x0 in [-1, W-1].
 __device__ __forceinline__ float bilinear(const float *__restrict__ img, int pad_w, int W, int H, float x, float y) {
@@ -543,12 +578,13 @@ __device__ __forceinline__ float tap_rcp(float z) {
 // whose terms are small, so float arithmetic places the taps to ~1e-6 px.  The plane enters in
 // double too; the per-tap arithmetic is float.
 struct WinProj {
-  int U0, V0;                // integer part of the projected centre
-  float fu, fv;              // its fraction, in [0, 1]
-  float zc;                  // projective depth of the centre
-  float g0, g1, g3, g4;      // H00 - uc H20, H01 - uc H21, H10 - vc H20, H11 - vc H21
-  float h6, h7;              // H20, H21
-  float lox, hix, loy, hiy;  // the texture clamp [-1, W-1] x [-1, H-1] relative to (U0, V0)
+  int U0, V0;   // integer part of the projected centre
+  float2 fuv;   // its fraction (fu, fv), in [0, 1]
+  float2 g03;   // the dx coefficients (H00 - uc H20, H10 - vc H20)
+  float2 g14;   // the dy coefficients (H01 - uc H21, H11 - vc H21)
+  float zc;     // projective depth of the centre
+  float h6, h7; // H20, H21
+  float2 lo, hi;  // the texture clamp [-1, W-1] x [-1, H-1] relative to (U0, V0)
 };
 // Fills wp for plane pl at pixel (px, py) of source s; false when the centre does not project
 // inside the source (the cost is then 2, DPE.cu:709-712).
@@ -569,51 +605,51 @@ __device__ __forceinline__ bool window_projection(const PMArgs &a, int s, float4
   const double U = floor(uc), V = floor(vc);
   wp.U0 = (int)U;
   wp.V0 = (int)V;
-  wp.fu = (float)(uc - U);
-  wp.fv = (float)(vc - V);
+  wp.fuv = make_float2((float)(uc - U), (float)(vc - V));
   wp.zc = (float)Z;
   const double bw0 = b[0] * iw, bw1 = b[1] * iw, bw2 = b[2] * iw;
   const double h6 = A[6] - bw2 * m0, h7 = A[7] - bw2 * m1;
-  wp.g0 = (float)((A[0] - bw0 * m0) - uc * h6);
-  wp.g1 = (float)((A[1] - bw0 * m1) - uc * h7);
-  wp.g3 = (float)((A[3] - bw1 * m0) - vc * h6);
-  wp.g4 = (float)((A[4] - bw1 * m1) - vc * h7);
+  wp.g03 = make_float2((float)((A[0] - bw0 * m0) - uc * h6), (float)((A[3] - bw1 * m0) - vc * h6));
+  wp.g14 = make_float2((float)((A[1] - bw0 * m1) - uc * h7), (float)((A[4] - bw1 * m1) - vc * h7));
   wp.h6 = (float)h6;
   wp.h7 = (float)h7;
-  wp.lox = (float)(-1 - wp.U0);
-  wp.hix = (float)(a.W - 1 - wp.U0);
-  wp.loy = (float)(-1 - wp.V0);
-  wp.hiy = (float)(a.H - 1 - wp.V0);
+  wp.lo = make_float2((float)(-1 - wp.U0), (float)(-1 - wp.V0));
+  wp.hi = make_float2((float)(a.W - 1 - wp.U0), (float)(a.H - 1 - wp.V0));
   return true;
 }
 // bilinear_s at (U0 + x, V0 + y): the clamp to [-1, W-1] x [-1, H-1] and the split into texel and
-// weight are taken on the offsets, which equals them on the absolute coordinates.
+// weight are taken on the offsets, which equals them on the absolute coordinates.  The x and y
+// halves and the two rows of the blend run as packed pairs (the same operations as bilinear_s).
 template <class Src, bool kClamp = true>
-__device__ __forceinline__ float bilinear_w(const Src &src, const WinProj &wp, float x, float y) {
-  const float xc = kClamp ? fminf(fmaxf(x, wp.lox), wp.hix) : x;
-  const float yc = kClamp ? fminf(fmaxf(y, wp.loy), wp.hiy) : y;
+__device__ __forceinline__ float bilinear_w(const Src &src, const WinProj &wp, float2 p) {
+  const float2 c = kClamp ? make_float2(fminf(fmaxf(p.x, wp.lo.x), wp.hi.x), fminf(fmaxf(p.y, wp.lo.y), wp.hi.y)) : p;
   int ix, iy;
-  const float fx = floor_split(xc, &ix), fy = floor_split(yc, &iy);
-  const float ax = xc - fx, ay = yc - fy;
+  const float2 f = floor_split2(c, &ix, &iy);
+  const float2 a = sub2(c, f);                            // (ax, ay)
+  const float2 oa = sub2(make_float2(1.0f, 1.0f), a);     // (1 - ax, 1 - ay)
   const float4 v = src.fetch((wp.V0 + iy + 1) * src.pw + (wp.U0 + ix + 1));
-  const float top = (1.0f - ax) * v.x + ax * v.y;
-  const float bot = (1.0f - ax) * v.z + ax * v.w;
-  return (1.0f - ay) * top + ay * bot;
+  // (top, bot) = (1 - ax) (v00, v01) + ax (v10, v11); then (1 - ay) top + ay bot
+  const float2 l = mul2(make_float2(oa.x, oa.x), make_float2(v.x, v.z));
+  const float2 rt = mul2(make_float2(a.x, a.x), make_float2(v.y, v.w));
+  const float2 r = mul2(make_float2(oa.y, a.y), make_float2(l.x + rt.x, l.y + rt.y));
+  return r.x + r.y;
 }
 // One tap of the strong window: sample the source at the projected tap and accumulate the
-// hypothesis-dependent moments (sums of w*s, w*s^2, w*(r-c)*s over s = sample - c).  (cx, cy, cz)
-// carry the tap column's dx terms.
+// hypothesis-dependent moments (sums of w*s, w*s^2, w*(r-c)*s over s = sample - c); acc holds
+// (sum w*s, sum w*(r-c)*s).  cxy and cz carry the tap column's dx terms.
 template <bool kClamp, class Src, class RW>
-__device__ __forceinline__ void strong_tap(const WinProj &wp, const Src &src, const RW &rw, float cx, float cy,
-                                           float cz, float dy, int k, float &s_s, float &s_ss, float &s_rs) {
-  const float X = wp.g1 * dy + cx, Y = wp.g4 * dy + cy, Z = wp.h7 * dy + cz;
+__device__ __forceinline__ void strong_tap(const WinProj &wp, const Src &src, const RW &rw, float2 cxy, float cz,
+                                           float dy, int k, float2 &acc, float &s_ss) {
+  const float2 gy = mul2(wp.g14, make_float2(dy, dy));
+  const float Z = wp.h7 * dy + cz;
   const float iz = tap_rcp(Z);
-  const float sv = bilinear_w<Src, kClamp>(src, wp, wp.fu + X * iz, wp.fv + Y * iz) - rw.center;
-  const float2 t = rw.tap(k);
-  const float ws = t.x * sv;
-  s_s += ws;
-  s_ss += ws * sv;
-  s_rs += t.y * sv;
+  const float2 t = mul2(make_float2(gy.x + cxy.x, gy.y + cxy.y), make_float2(iz, iz));  // (X, Y) / Z
+  const float sv = bilinear_w<Src, kClamp>(src, wp, make_float2(wp.fuv.x + t.x, wp.fuv.y + t.y)) - rw.center;
+  const float2 m = mul2(rw.tap(k), make_float2(sv, sv));  // (w s, w (r - c) s)
+  const float q = m.x * sv;
+  acc.x += m.x;
+  acc.y += m.y;
+  s_ss += q;
 }
 // ComputeBilateralNCCOld (DPE.cu:696-782) with the reference window precomputed; the window loop
 // for one source sampler, columns dx outer and rows dy inner as the reference window's taps.
@@ -621,27 +657,32 @@ template <bool kClamp, class Src, int kUnroll, class RW>
 __device__ __forceinline__ void strong_window(const PMArgs &a, const WinProj &wp, const Src &src, const RW &rw,
                                               float &s_s, float &s_ss, float &s_rs) {
   const int r = a.P.strong_radius, inc = a.P.strong_increment;
+  float2 acc = make_float2(s_s, s_rs);
   // Tap offsets are small whole numbers, so stepping them by float adds gives the same floats as
   // converting each integer, without a conversion per tap.
   if (kUnroll > 0 && r == 5 && inc == 2) {
     for (int ii = 0; ii < 6; ++ii) {
       const float dx = (float)(2 * ii - 5);
-      const float cx = wp.g0 * dx, cy = wp.g3 * dx, cz = wp.h6 * dx + wp.zc;
+      const float2 cxy = mul2(wp.g03, make_float2(dx, dx));
+      const float cz = wp.h6 * dx + wp.zc;
 #pragma unroll(kUnroll > 0 ? kUnroll : 1)
       for (int jj = 0; jj < 6; ++jj)
-        strong_tap<kClamp>(wp, src, rw, cx, cy, cz, (float)(2 * jj - 5), 6 * ii + jj, s_s, s_ss, s_rs);
+        strong_tap<kClamp>(wp, src, rw, cxy, cz, (float)(2 * jj - 5), 6 * ii + jj, acc, s_ss);
     }
   } else {
     int k = 0;
     const float finc = (float)inc, d0 = (float)(-r);
     float dx = d0;
     for (int i = -r; i <= r; i += inc, dx += finc) {
-      const float cx = wp.g0 * dx, cy = wp.g3 * dx, cz = wp.h6 * dx + wp.zc;
+      const float2 cxy = mul2(wp.g03, make_float2(dx, dx));
+      const float cz = wp.h6 * dx + wp.zc;
       float dy = d0;
       for (int j = -r; j <= r; j += inc, dy += finc)
-        strong_tap<kClamp>(wp, src, rw, cx, cy, cz, dy, k++, s_s, s_ss, s_rs);
+        strong_tap<kClamp>(wp, src, rw, cxy, cz, dy, k++, acc, s_ss);
     }
   }
+  s_s = acc.x;
+  s_rs = acc.y;
 }
 template <class Src, int kUnroll, class RW>
 __device__ __forceinline__ float ncc_strong_src(const PMArgs &a, const WinProj &wp, const Src &src, const RW &rw) {
@@ -699,13 +740,13 @@ __device__ __forceinline__ float ncc_strong_adjoint(const PMArgs &a, int px, int
   int k = 0;
   for (int i = -r; i <= r; i += inc) {
     const float dx = (float)i, x = (float)(px + i);
-    const float cx = wp.g0 * dx, cy = wp.g3 * dx, cz = wp.h6 * dx + wp.zc;
+    const float cx = wp.g03.x * dx, cy = wp.g03.y * dx, cz = wp.h6 * dx + wp.zc;
     for (int j = -r; j <= r; j += inc) {
       const float dy = (float)j, y = (float)(py + j);
-      const float X = wp.g1 * dy + cx, Y = wp.g4 * dy + cy, Z = wp.h7 * dy + cz;
+      const float X = wp.g14.x * dy + cx, Y = wp.g14.y * dy + cy, Z = wp.h7 * dy + cz;
       const float iz = tap_rcp(Z);
-      const float uo = wp.fu + X * iz, vo = wp.fv + Y * iz;  // offsets from (U0, V0)
-      const float xc = fminf(fmaxf(uo, wp.lox), wp.hix), yc = fminf(fmaxf(vo, wp.loy), wp.hiy);
+      const float uo = wp.fuv.x + X * iz, vo = wp.fuv.y + Y * iz;  // offsets from (U0, V0)
+      const float xc = fminf(fmaxf(uo, wp.lo.x), wp.hi.x), yc = fminf(fmaxf(vo, wp.lo.y), wp.hi.y);
       int ix, iy;
       const float fx = floor_split(xc, &ix), fy = floor_split(yc, &iy);
       const float ax = xc - fx, ay = yc - fy;
@@ -716,8 +757,8 @@ __device__ __forceinline__ float ncc_strong_adjoint(const PMArgs &a, int px, int
       const float rc = texel(a, 0, px + i, py + j) - rw.center;  // r_k - c
       const float dc = rw.w(k) * (ka * (rc - rw.mean_r) + kb * (sv - m_s));
       // slope of the sample; zero along a clamped coordinate
-      const float dsx = (uo > wp.lox && uo < wp.hix) ? (1.0f - ay) * (v10 - v00) + ay * (v11 - v01) : 0.0f;
-      const float dsy = (vo > wp.loy && vo < wp.hiy) ? (1.0f - ax) * (v01 - v00) + ax * (v11 - v10) : 0.0f;
+      const float dsx = (uo > wp.lo.x && uo < wp.hi.x) ? (1.0f - ay) * (v10 - v00) + ay * (v11 - v01) : 0.0f;
+      const float dsy = (vo > wp.lo.y && vo < wp.hi.y) ? (1.0f - ax) * (v01 - v00) + ax * (v11 - v10) : 0.0f;
       // u = X' / Z' with X' = H0. p, Z' = H2. p: du/dH0j = p_j / Z', du/dH2j = -u p_j / Z'
       const float u = (float)wp.U0 + uo, v = (float)wp.V0 + vo;
       const float gu = dc * dsx * iz, gv = dc * dsy * iz;
