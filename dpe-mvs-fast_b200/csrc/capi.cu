@@ -587,13 +587,16 @@ int run_sequence(dpe_ctx *ctx, ProblemState *ps, int n, const PMArgs *d_args, co
       DPE_TRY(cudaMemsetAsync(a.nmap, 0, (size_t)L * 4, s));
     }
   }
-  // Launch settings the tuner picks (results do not depend on them): the block shape of a
-  // one-thread-per-pixel kernel for one problem (a batch keeps the 16 x 8 layout its block table
-  // is built for), and the shared-memory carveout of a cooperative kernel.
+  // Launch settings the tuner picks (results do not depend on them): the block shape of the random
+  // initialisation for one problem (a batch keeps the 16 x 8 layout its block table is built for)
+  // and the shared-memory carveout of the strong update.  These two do the same work in every
+  // launch of a size class, so launches with different settings compare; the kernels whose work
+  // follows a view's weak pixels (GenNeighbours, the nearest-strong search, the plane fit,
+  // DepthToWeak, LocalRefine) keep hand-measured settings, since their samples would compare views.
   long long pix_all = 0;
   for (int b = 0; b < n; ++b) pix_all += (long long)ps[b].L;
   auto shaped = [&](int kid, auto launch) {
-    if (n != 1) {
+    if (n != 1 || kid != KID_RANDOM_INIT) {
       launch(g.fg, g.fb);
       return;
     }
@@ -603,6 +606,10 @@ int run_sequence(dpe_ctx *ctx, ProblemState *ps, int n, const PMArgs *d_args, co
     t.finish();
   };
   auto carved = [&](int kid, auto launch) {
+    if (kid != KID_STRONG_UPDATE) {
+      launch(-1);
+      return;
+    }
     TunedLaunch t(ctx, kid, pix_all, kNumCarves, s);
     launch(kCarveCands[t.cand]);
     t.finish();

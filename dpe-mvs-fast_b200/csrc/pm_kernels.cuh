@@ -199,9 +199,16 @@ __device__ __forceinline__ void find_nearest_strong_pixel(const PMArgs &a, int p
   }
   a.nearest[center] = res;
 }
+// Resident blocks requested for the one-thread-per-pixel searches (nearest strong point,
+// GenNeighbours, the plane fit): measured on the 10-view 1600x1200 schedule with fixed 16x8
+// blocks, 6 blocks (80 registers) make GenNeighbours 9 % faster than its unbounded 104 registers
+// (4 blocks) and 4 % faster than 8 blocks (64 registers, more stack traffic).
+#ifndef DPE_LATENCY_MIN_BLOCKS
+#define DPE_LATENCY_MIN_BLOCKS 6
+#endif
 // One thread per pixel of a 2D grid: the tiles keep the rays of neighbouring pixels together
 // (measured faster than a work list over the WEAK pixels).
-__global__ void __launch_bounds__(128) k_find_nearest_strong(const Launch lc) {
+__global__ void __launch_bounds__(128, DPE_LATENCY_MIN_BLOCKS) k_find_nearest_strong(const Launch lc) {
   const Blk B = resolve<kGridFull>(lc);
   const PMArgs &a = *B.a;
   int px, py;
@@ -506,7 +513,7 @@ __device__ __forceinline__ void gen_neighbours_pixel(const PMArgs &a, int px, in
 }
 // One thread per pixel of a 2D grid: the tiles keep the rays of neighbouring pixels together
 // (measured faster than a work list over the WEAK pixels).
-__global__ void __launch_bounds__(128) k_gen_neighbours(const Launch lc) {
+__global__ void __launch_bounds__(128, DPE_LATENCY_MIN_BLOCKS) k_gen_neighbours(const Launch lc) {
   const Blk B = resolve<kGridFull>(lc);
   const PMArgs &a = *B.a;
   int px, py;
@@ -1433,7 +1440,7 @@ __device__ __forceinline__ void ransac_fit_plane_pixel(const PMArgs &a, int px, 
 }
 // One thread per pixel of a 2D grid: the tiles keep the rays of neighbouring pixels together
 // (measured faster than a work list over the WEAK pixels).
-__global__ void __launch_bounds__(128) k_ransac_fit_plane(const Launch lc) {
+__global__ void __launch_bounds__(128, DPE_LATENCY_MIN_BLOCKS) k_ransac_fit_plane(const Launch lc) {
   const Blk B = resolve<kGridFull>(lc);
   const PMArgs &a = *B.a;
   int px, py;
@@ -1498,7 +1505,13 @@ __global__ void __launch_bounds__(128) k_weak_prepare(const Launch lc, int parit
 // sources the pixel sampled.  Unevaluated candidates keep the fused form's initial costs (0, and 2
 // for the first candidate's first source: quirk Q2).
 template <bool kRandom, int kStage>
-__global__ void __launch_bounds__(128) k_weak_eval(const Launch lc, int parity) {
+// Resident blocks requested for the deformable evaluation (__launch_bounds__): measured on the
+// 10-view 1600x1200 schedule, 8 blocks (64 registers, a few spills) make it 21 % faster than the
+// unbounded 96 registers and 5 blocks: it waits on its gathers, and more warps hide them.
+#ifndef DPE_WEAK_MIN_BLOCKS
+#define DPE_WEAK_MIN_BLOCKS 8
+#endif
+__global__ void __launch_bounds__(128, DPE_WEAK_MIN_BLOCKS) k_weak_eval(const Launch lc, int parity) {
   const Blk B = resolve<kGridList>(lc);
   const PMArgs &a = *B.a;
   const int n = a.N - 1;

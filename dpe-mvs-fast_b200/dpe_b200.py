@@ -309,6 +309,9 @@ class Context:
         if st != OK:
             raise DPEError(st, "dpe_ctx_create")
         self.handle = h
+        # DPE_AUTOTUNE=0 turns the launch tuner off for every context (fixed default settings)
+        if os.environ.get("DPE_AUTOTUNE") == "0" and hasattr(self.lib, "dpe_ctx_set_autotune"):
+            self.lib.dpe_ctx_set_autotune(self.handle, 0)
 
     def close(self):
         if getattr(self, "handle", None):

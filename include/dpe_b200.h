@@ -447,11 +447,12 @@ int dpe_ctx_get_kernel_stats(dpe_ctx *ctx, dpe_kernel_stat *out, int capacity, i
 
 /* Launch tuner (no reference counterpart; the reference launches fixed 16x16 blocks).  For each
  * (kernel, size class = floor(log2 of the call's pixels)) the context's first launches cycle
- * through candidate settings that change no result -- the block shape of the
- * one-thread-per-pixel kernels (16x8, 32x4, 8x16, 64x2, 8x8; single-problem calls only) and the
- * shared-memory carveout of the cooperative cost kernels (driver default, 100, 75, 50 %) -- each
- * timed by an event pair on the context's stream, and keep the fastest mean after 2 samples
- * each.  On by default; dpe_ctx_set_autotune(ctx, 0) uses the first candidate throughout. */
+ * through candidate settings that change no result -- the block shape of the random
+ * initialisation (16x8, 32x4, 8x16, 64x2, 8x8; single-problem calls only) and the shared-memory
+ * carveout of the strong update (driver default, 100, 75, 50 %), the two kernels whose launches
+ * of one size class do the same work -- each timed by an event pair on the context's stream, and
+ * keep the fastest mean after 2 samples each.  On by default; dpe_ctx_set_autotune(ctx, 0) uses
+ * the first candidate throughout. */
 int dpe_ctx_set_autotune(dpe_ctx *ctx, int on);
 typedef struct dpe_tuning_entry {
   char name[32];      /* kernel class, as in dpe_kernel_stat                                   */
