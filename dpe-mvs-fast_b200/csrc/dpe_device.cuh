@@ -352,15 +352,19 @@ struct SrcBF16 {
 // identity.
 template <class Src, bool kClamp = true>
 __device__ __forceinline__ float bilinear_s(const Src &src, int W, int H, float x, float y) {
-  const float xc = kClamp ? fminf(fmaxf(x, -1.0f), (float)(W - 1)) : x;
-  const float yc = kClamp ? fminf(fmaxf(y, -1.0f), (float)(H - 1)) : y;
+  const float2 c = kClamp ? make_float2(fminf(fmaxf(x, -1.0f), (float)(W - 1)), fminf(fmaxf(y, -1.0f), (float)(H - 1)))
+                          : make_float2(x, y);
   int ix, iy;
-  const float fx = floor_split(xc, &ix), fy = floor_split(yc, &iy);
-  const float ax = xc - fx, ay = yc - fy;
+  const float2 f = floor_split2(c, &ix, &iy);
+  const float2 a = sub2(c, f);                            // (ax, ay)
+  const float2 oa = sub2(make_float2(1.0f, 1.0f), a);     // (1 - ax, 1 - ay)
   const float4 v = src.fetch((iy + 1) * src.pw + (ix + 1));
-  const float top = (1.0f - ax) * v.x + ax * v.y;
-  const float bot = (1.0f - ax) * v.z + ax * v.w;
-  return (1.0f - ay) * top + ay * bot;
+  // (top, bot) = (1 - ax) (v00, v01) + ax (v10, v11); then (1 - ay) top + ay bot; products are
+  // summed with scalar adds (see add2)
+  const float2 l = mul2(make_float2(oa.x, oa.x), make_float2(v.x, v.z));
+  const float2 rt = mul2(make_float2(a.x, a.x), make_float2(v.y, v.w));
+  const float2 r = mul2(make_float2(oa.y, a.y), make_float2(l.x + rt.x, l.y + rt.y));
+  return r.x + r.y;
 }
 __device__ __forceinline__ SrcF32 src_f32(const PMArgs &a, int s) {
   return SrcF32{a.img[s], a.pad_w, (long long)a.pad_w * (a.H + 2)};
@@ -484,12 +488,14 @@ __device__ __forceinline__ float2 project(const float H[9], int x, int y) {
 // the IEEE quotients X / Z and Y / Z.
 __device__ __forceinline__ float tap_rcp(float z);
 __device__ __forceinline__ float2 project_tap(const float H[9], float fx, float fy) {
-  const float X = H[0] * fx + H[1] * fy + H[2];
-  const float Y = H[3] * fx + H[4] * fy + H[5];
+  const float2 px = mul2(make_float2(H[0], H[3]), make_float2(fx, fx));
+  const float2 py = mul2(make_float2(H[1], H[4]), make_float2(fy, fy));
+  const float X = px.x + py.x + H[2];
+  const float Y = px.y + py.y + H[5];
   const float Z = H[6] * fx + H[7] * fy + H[8];
 #if defined(__CUDA_ARCH__) && !defined(DPE_EXACT)
   const float iz = tap_rcp(Z);
-  return make_float2(X * iz, Y * iz);
+  return mul2(make_float2(X, Y), make_float2(iz, iz));
 #else
   return make_float2(X / Z, Y / Z);
 #endif
@@ -849,8 +855,8 @@ __device__ __forceinline__ float window_ncc_tab(const PMArgs &a, const float H[9
     for (int j = -radius; j <= radius; j += inc, y += finc) {
       const float2 sp = project_tap(H, x, y);
       const float sv = bilinear_s(src, a.W, a.H, sp.x, sp.y) - ref_center;
-      const float2 e = tab[t++];
-      r_s += e.x * sv; r_ss += e.x * sv * sv; r_rs += e.y * sv;
+      const float2 m = mul2(tab[t++], make_float2(sv, sv));  // (w s, w (r - c) s)
+      r_s += m.x; r_ss += m.x * sv; r_rs += m.y;
     }
     s_s += r_s; s_ss += r_ss; s_rs += r_rs;
   }
