@@ -15,7 +15,8 @@ of the fused points.  The scene's working set (10 x 1600 x 1200 images, states a
 is far larger than the 126 MB L2, so no flush is needed between steps.
 
 `--impl reference` times the reference's own DPE.cu / DPE.cpp compiled for the host CPU
-(oracle/_ref/libref.so; the reference's CUDA build is not run on the shared GPUs),
+(oracle/_ref/libref.so; its CUDA build reads past the ends of its device buffers and an
+uninitialised radius array, so it is not run on the GPU),
 on a bounded sample of the same schedule, on all host cores.
 
 `--case` runs only device-resident schedules of a chosen scene (for profilers):
