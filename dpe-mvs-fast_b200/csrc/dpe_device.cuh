@@ -38,17 +38,20 @@ constexpr int kMaxWin = 6;  // taps per window side for radius 5 / step 2 (DPE.c
 #define DPE_SWEEP_MIN_BLOCKS 8
 #endif
 // Unrolling of a window column's taps (the reference window, radius 5 / step 2, has 6 per column)
-// in the kernels that sweep one plane family over all sources: measured, unrolling by 3 speeds
-// DepthToWeak, LocalRefine and the random initialisation by 8-15 %, and slows the strong update,
-// whose registers are bounded for occupancy, by 25 %.
+// in the kernels that sweep one plane family over all sources (DepthToWeak, LocalRefine, the
+// random initialisation).  Measured on the 10-view 1600x1200 schedule with the packed tap
+// arithmetic: the whole column (6) makes DepthToWeak 6 % and LocalRefine 7 % faster than 3, and 2
+// is slower than 3.
 #ifndef DPE_SWEEP_UNROLL
-#define DPE_SWEEP_UNROLL 3
+#define DPE_SWEEP_UNROLL 6
 #endif
 constexpr int kSweepUnroll = DPE_SWEEP_UNROLL;
-// taps of a window column unrolled in the strong update's cost evaluations (0: rolled loop;
-// measured: unrolling by 3 or 6 makes the cooperative strong update 35-40 % slower)
+// taps of a window column unrolled in the strong update's cost evaluations (0: rolled loop).
+// Measured on the 10-view 1600x1200 schedule with the packed tap arithmetic: unrolling by 2 makes
+// the cooperative strong update 5 % faster (the next tap's gathers issue before this tap's blend);
+// by 3 or 6 it was 35-40 % slower with the scalar taps (registers, under the 8-block bound).
 #ifndef DPE_STRONG_UNROLL
-#define DPE_STRONG_UNROLL 0
+#define DPE_STRONG_UNROLL 2
 #endif
 constexpr int kStrongUnroll = DPE_STRONG_UNROLL;
 
