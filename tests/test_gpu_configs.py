@@ -91,11 +91,11 @@ def test_c2_finest_geom_call_matches_oracle(ctx, xctx, c2_scene):
           f"{agree:.5f}, well-matched ({conf.mean():.3f} of pixels) {conf_agree:.5f}, states "
           f"{(g['weak'] == o['weak']).mean():.5f}; within 1% of GT gpu {acc_g:.4f} oracle {acc_o:.4f}")
     assert _identical(x, o)
-    # the default build's statistical bar on the geometric path (FMA contraction decides near-ties
-    # among equally good hypotheses; see test_gpu_parity.test_pm_refine_geom_matches_oracle)
+    # the default build on the geometric path: the north-star bar on all pixels, plus the
+    # statistical bars (see test_gpu_parity.test_pm_refine_geom_matches_oracle)
     assert conf_agree >= 0.98
     assert abs(acc_g - acc_o) <= 0.01
-    assert agree >= 0.95
+    assert agree >= DEPTH_FRACTION
 
 
 def test_c2_fusion_bit_exact_fp64(ctx, c2_scene):

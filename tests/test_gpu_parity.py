@@ -102,12 +102,11 @@ def test_pm_refine_geom_matches_oracle(ctx, weak_scene):
     g = ctx.pm_run(images, cams, p, **kw)
     o = O.pm_run(images, cams, p, **kw)
     agree, weak_agree = _compare_calls(g, o, "refine-iter (geom)")
-    # With the geometric term on a near-textureless scene many hypotheses tie, and the GPU's FMA
-    # contraction alone changes which of the equally good ones wins: the same kernel source built
-    # for the host matches the oracle bit for bit without contraction (test_kernel_host.py) and
-    # agrees on 97.5 % of pixels with it (98.9 % after one iteration).  So on this path the bar is
-    # statistical: well-matched pixels agree within 0.1 % on >= 98 %, and both runs are equally
-    # accurate against the ground truth.
+    # With the geometric term on a near-textureless scene many hypotheses tie, and any change of
+    # rounding can change which of the equally good ones wins (built with FMA contraction, the
+    # kernels agreed with the oracle on 97.5 % here).  The default build no longer contracts; the
+    # tap reciprocal is its only difference from the oracle, and it is held to the north-star bar
+    # of 99.5 % of all pixels, besides the statistical bars on well-matched pixels and accuracy.
     dg, do = g["plane"][..., 3], o["plane"][..., 3]
     conf = np.isfinite(o["costs"]) & (o["costs"] < 0.3) & (o["weak"] == D.STRONG) & (g["weak"] == D.STRONG)
     conf_agree = h.rel_depth_agreement(dg[conf], do[conf], DEPTH_REL_TOL)
@@ -118,7 +117,7 @@ def test_pm_refine_geom_matches_oracle(ctx, weak_scene):
           f"gpu {acc_g:.4f} oracle {acc_o:.4f}")
     assert conf_agree >= 0.98
     assert abs(acc_g - acc_o) <= 0.01
-    assert agree >= 0.95
+    assert agree >= DEPTH_FRACTION
     assert weak_agree >= 0.99
 
 
