@@ -309,7 +309,13 @@ struct TunedLaunch {
     }
     t0 = tune_event(ctx);
     t1 = tune_event(ctx);
-    if (t0 && t1) cudaEventRecord(t0, s);
+    if (t0 && t1) {
+      cudaEventRecord(t0, s);
+      return;
+    }
+    if (t0) ctx->tuner.events.push_back(t0);  // no pair: this launch goes unmeasured
+    if (t1) ctx->tuner.events.push_back(t1);
+    t0 = t1 = nullptr;
   }
   void finish() {
     if (!t0 || !t1) return;
