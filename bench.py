@@ -529,6 +529,16 @@ def run_ours(args):
                                staging={D.STAGE_FP32: "fp32", D.STAGE_FP16: "fp16"}[staging],
                                gauss_newton=bool(gn), points=int(r["points"]), clocks=fclocks.summary())
 
+    # the same forms on the batching workload (C5), one process only; a failure there leaves the
+    # rest of the line intact
+    forms_c5 = None
+    if not args.no_forms and world == 1:
+        try:
+            c5 = measure_c5(ctx, 1)
+            forms_c5 = dict(workload=c5["config"]["workload"], reference_mpix=c5["config"]["reference_mpix"],
+                            fusion=c5["fusion"], **c5["forms"])
+        except Exception as e:  # noqa: BLE001 -- reported in the line
+            forms_c5 = dict(error=repr(e)[:300])
     traffic = load_traffic_table()
     rooflines = kernel_rooflines(stats, counted, args.steps, fp32_peak, traffic, L)
     dname = max(rooflines, key=lambda k: rooflines[k]["ms_per_step"])
@@ -576,7 +586,7 @@ def run_ours(args):
                 e2e=dict(value=round(e2e_value, 4), unit=UNIT, h2d_bytes_per_step=int(h2d), d2h_bytes_per_step=int(d2h)),
                 kernel_ms_per_step={k: round(v["ms"] / max(1, args.steps), 3) for k, v in
                                     sorted(stats.items(), key=lambda kv: -kv[1]["ms"])},
-                forms=forms or None, autotune=autotune or None)
+                forms=forms or None, forms_c5=forms_c5, autotune=autotune or None)
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
@@ -627,12 +637,21 @@ def run_c5(args):
     with clocks; depth agreement with plain and accuracy against ground truth; then fusion of the
     last form's depth maps into one point cloud.  Prints one JSON line."""
     import dpe_b200 as D
+
+    ctx = D.Context(0)
+    print(json.dumps(measure_c5(ctx, args.seed)), flush=True)
+    ctx.close()
+    return 0
+
+
+def measure_c5(ctx, seed: int) -> dict:
+    """The forms of the batching workload (run_c5) on context ctx; returns the line's fields."""
+    import dpe_b200 as D
     import scene as S
 
     t0 = time.perf_counter()
-    ring, probs = S.c5_workload(seed=args.seed, device="cuda")
+    ring, probs = S.c5_workload(seed=seed, device="cuda")
     gen_s = time.perf_counter() - t0
-    ctx = D.Context(0)
     p = schedule_params(0, 0, 11)
     p.use_limit = p.use_label = 0  # no edge or label maps: FIRST_INIT as ProcessProblem runs it at level 0
     p.depth_min = np.float32(ring.spec.depth_min) * np.float32(0.6)  # DPE::InuputInitialization (DPE.cpp:953-954)
@@ -697,9 +716,7 @@ def run_c5(args):
                             reference_mpix=round(mpix, 3)),
                 scene_generation_s=round(gen_s, 1), forms=forms,
                 fusion=dict(points=int(fu["count"]), gpu_ms=round(fu["gpu_ms"], 2)))
-    print(json.dumps(line), flush=True)
-    ctx.close()
-    return 0
+    return line
 
 
 def main():
