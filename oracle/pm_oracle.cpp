@@ -5,7 +5,8 @@
 // CPU (oracle/_ref, built by oracle/Makefile behind the stand-ins of oracle/refshim) produce the
 // same bits as this restatement on the first-init, weak-texture and geometric paths when the
 // switches below select the reference's arithmetic (oracle_set_raw_moments,
-// oracle_set_ref_addressing, oracle_set_serial_race); tests/test_ref_oracle.py holds that.
+// oracle_set_ref_addressing, oracle_set_ref_homography, oracle_set_serial_race);
+// tests/test_ref_oracle.py holds that.
 // Each function cites the reference lines it restates.  Semantics are FP32 without fast-math
 // (the reference build uses --use_fast_math, CMakeLists.txt:26; that rounding is not restated).
 // Red/black passes run in the reference's colour order; pixels of one colour are independent and
@@ -15,6 +16,9 @@
 //     reads a snapshot of costs/planes taken before the colour pass (oracle_set_serial_race
 //     selects the serial raster-order reading instead);
 //   * NCC moments are shifted by the window centre (oracle_set_raw_moments selects the raw ones);
+//   * the homography's camera part is composed in double once per call, and each strong window's
+//     centre is projected in double with its taps as float offsets (oracle_set_ref_homography
+//     selects the reference's per-hypothesis float composition and float projection);
 //   * texture reads are exact bilinear with clamp-to-edge addressing at x itself (the hardware
 //     path uses 8-bit interpolation weights; oracle_set_ref_addressing adds the rounding of the
 //     reference's tex2D(x + 0.5, y + 0.5) coordinate);
